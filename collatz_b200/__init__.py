@@ -1,0 +1,412 @@
+"""collatz_b200 -- B200-native Collatz verifier (Python mirror of the C ABI).
+
+The compute path is the CUDA library libcollatz_b200.so (include/collatz.h);
+this module only marshals arguments through ctypes.  There is no CPU
+fallback: if the library or a usable sm_100 device is missing, calls raise.
+
+Reference interface mirrored (vigleik0/collatz, collatz_cudav7.cu):
+  run_case(...)        main() on one stdin 6-tuple            (cu:95-183)
+  launchkernel(...)    one batch of Step-1 pairs of a bucket  (cu:565-649)
+  step1_pairs(...)     the leaves of search1                  (cu:497-563)
+New entry modes: verify_range, verify_batch, trajectory, plans and the server.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcollatz_b200.so")
+
+OK = 0
+E_ARG, E_CUDA, E_NOMEM, E_LIMIT, E_DEVICE, E_TIMEOUT, E_STATE, E_ADMISSION, E_NODEV = \
+    -1, -2, -3, -4, -5, -6, -7, -8, -9
+RANGE_NO_MOD9 = 0x1
+VARIANT_AUTO = 0xFFFFFFFF
+BV_WORDS = (1 << 19) + 32
+
+
+class CollatzError(RuntimeError):
+    def __init__(self, status: int, msg: str = ""):
+        super().__init__(f"collatz status {status}: {msg}")
+        self.status = status
+
+
+class Config(C.Structure):
+    _fields_ = [("maxbits", C.c_uint32), ("range_k", C.c_uint32), ("device", C.c_int32),
+                ("variant", C.c_uint32), ("iter_cap", C.c_uint32), ("reserved", C.c_uint32 * 11)]
+
+
+class Case(C.Structure):
+    _fields_ = [("base", C.c_uint64 * 2), ("sigfig", C.c_uint32), ("threepower", C.c_uint32),
+                ("number", C.c_uint64 * 2), ("doubleeven", C.c_uint32), ("numevens", C.c_uint32)]
+
+
+class CaseResultC(C.Structure):
+    _fields_ = [("hash", C.c_uint32), ("spot_checks", C.c_uint32), ("launches", C.c_uint64),
+                ("seeds_checked", C.c_uint64), ("pairs", C.c_uint64), ("cpu_pairs", C.c_uint64),
+                ("n_overflow", C.c_uint64), ("overflow_seeds", C.POINTER(C.c_uint32)),
+                ("overflow_cap", C.c_uint64), ("max_excursion", C.c_uint32 * 4),
+                ("max_excursion_seed", C.c_uint32 * 4), ("max_stopping_time", C.c_uint64),
+                ("max_stopping_time_seed", C.c_uint32 * 4), ("errors", C.c_uint32),
+                ("reserved", C.c_uint32), ("device_ms", C.c_double)]
+
+
+class Range(C.Structure):
+    _fields_ = [("offset", C.c_uint64 * 2), ("size", C.c_uint64), ("k", C.c_uint32),
+                ("flags", C.c_uint32)]
+
+
+class RangeResultC(C.Structure):
+    _fields_ = [("seeds_checked", C.c_uint64), ("failures", C.c_uint64), ("widened", C.c_uint64),
+                ("max_excursion", C.c_uint32 * 8), ("max_excursion_seed", C.c_uint32 * 4),
+                ("max_stopping_time", C.c_uint64), ("max_stopping_time_seed", C.c_uint32 * 4),
+                ("errors", C.c_uint32), ("status", C.c_int32), ("device_ms", C.c_double)]
+
+
+def _limbs(arr) -> int:
+    return sum(int(w) << (32 * i) for i, w in enumerate(arr))
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads libcollatz_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run collatz_b200/build.py")
+        L = C.CDLL(LIB_PATH)
+        P = C.c_void_p
+        sigs = {
+            "collatz_config_default": (None, [C.POINTER(Config)]),
+            "collatz_create": (C.c_int, [C.POINTER(Config), C.POINTER(P)]),
+            "collatz_destroy": (None, [P]),
+            "collatz_status_string": (C.c_char_p, [C.c_int]),
+            "collatz_last_error": (C.c_char_p, [P]),
+            "collatz_set_stream": (C.c_int, [P, P]),
+            "collatz_device_info": (C.c_int, [P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+            "collatz_run_case": (C.c_int, [P, C.POINTER(Case), C.POINTER(CaseResultC)]),
+            "collatz_verify_pairs": (C.c_int, [P, C.c_uint32, P, C.c_uint32, C.POINTER(CaseResultC)]),
+            "collatz_step1_pairs": (C.c_int, [C.c_uint32, C.POINTER(Case), P, C.c_uint64,
+                                              C.POINTER(C.c_uint64)]),
+            "collatz_case_tables": (C.c_int, [P, P, P]),
+            "collatz_range_sieve": (C.c_int, [P, C.c_uint32, P, C.POINTER(C.c_uint64)]),
+            "collatz_verify_range": (C.c_int, [P, C.POINTER(Range), C.POINTER(RangeResultC)]),
+            "collatz_verify_batch": (C.c_int, [P, P, C.c_uint32, P]),
+            "collatz_plan_create": (C.c_int, [P, P, C.c_uint32, C.POINTER(P)]),
+            "collatz_plan_launch": (C.c_int, [P]),
+            "collatz_plan_results": (C.c_int, [P, P]),
+            "collatz_plan_destroy": (None, [P]),
+            "collatz_trajectory": (C.c_int, [P, P, C.c_uint32, P, P, P]),
+            "collatz_variant_count": (C.c_int, [C.c_int]),
+            "collatz_set_variant": (C.c_int, [P, C.c_int, C.c_int]),
+        }
+        for name, (res, args) in sigs.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def status_string(s: int) -> str:
+    return lib().collatz_status_string(s).decode()
+
+
+# ----------------------------------------------------------------------------
+# results
+# ----------------------------------------------------------------------------
+
+@dataclass
+class CaseResult:
+    hash: int
+    launches: int
+    spot_checks: int
+    seeds_checked: int
+    pairs: int
+    cpu_pairs: int
+    n_overflow: int
+    overflow: list
+    max_excursion: int
+    max_excursion_seed: int
+    max_stopping_time: int
+    max_stopping_time_seed: int
+    errors: int
+    device_ms: float
+
+    def summary_line(self) -> str:
+        """The reference's stderr line (cu:181-182)."""
+        return (f"Number of kernel launches = {self.launches}. Spot checks = {self.spot_checks}. "
+                f"Complete hash = {self.hash:X}.")
+
+
+@dataclass
+class RangeResult:
+    seeds_checked: int
+    failures: int
+    widened: int
+    max_excursion: int
+    max_excursion_seed: int
+    max_stopping_time: int
+    max_stopping_time_seed: int
+    errors: int = 0
+    status: int = 0
+    device_ms: float = 0.0
+
+
+def _case_result(r: CaseResultC, ovbuf, cap) -> CaseResult:
+    n = min(r.n_overflow, cap)
+    ov = [_limbs(ovbuf[4 * i:4 * i + 4]) for i in range(n)] if ovbuf is not None else []
+    return CaseResult(r.hash, r.launches, r.spot_checks, r.seeds_checked, r.pairs, r.cpu_pairs,
+                      r.n_overflow, ov, _limbs(r.max_excursion), _limbs(r.max_excursion_seed),
+                      r.max_stopping_time, _limbs(r.max_stopping_time_seed), r.errors, r.device_ms)
+
+
+def _range_result(r: RangeResultC) -> RangeResult:
+    return RangeResult(r.seeds_checked, r.failures, r.widened, _limbs(r.max_excursion),
+                       _limbs(r.max_excursion_seed), r.max_stopping_time,
+                       _limbs(r.max_stopping_time_seed), r.errors, r.status, r.device_ms)
+
+
+def make_case(base, sigfig, threepower, number, doubleeven, numevens) -> Case:
+    c = Case()
+    c.base[0], c.base[1] = base & (2**64 - 1), base >> 64
+    c.sigfig, c.threepower = sigfig, threepower
+    c.number[0], c.number[1] = number & (2**64 - 1), number >> 64
+    c.doubleeven, c.numevens = doubleeven, numevens
+    return c
+
+
+def make_range(offset: int, size: int, k: int = 0, mod9: bool = True) -> Range:
+    r = Range()
+    r.offset[0], r.offset[1] = offset & (2**64 - 1), offset >> 64
+    r.size, r.k, r.flags = size, k, 0 if mod9 else RANGE_NO_MOD9
+    return r
+
+
+def pack_pairs(pairs) -> "C.Array":
+    """[(base, number)] -> npairs x 8 uint32 (cu:521-528 layout)."""
+    buf = (C.c_uint32 * (8 * len(pairs)))()
+    for i, (b, m) in enumerate(pairs):
+        for j in range(4):
+            buf[8 * i + j] = (b >> (32 * j)) & 0xFFFFFFFF
+            buf[8 * i + 4 + j] = (m >> (32 * j)) & 0xFFFFFFFF
+    return buf
+
+
+def step1_pairs(maxbits: int, base, sigfig, threepower, number, doubleeven, numevens, cap=None):
+    """Step-1 leaves [(bigindex, base, number)] (host only, no device)."""
+    c = make_case(base, sigfig, threepower, number, doubleeven, numevens)
+    cnt = C.c_uint64()
+    rc = lib().collatz_step1_pairs(maxbits, C.byref(c), None, 0, C.byref(cnt))
+    if rc:
+        raise CollatzError(rc, "step1_pairs")
+    n = cnt.value if cap is None else min(cap, cnt.value)
+    buf = (C.c_uint32 * (8 * max(1, n)))()
+    rc = lib().collatz_step1_pairs(maxbits, C.byref(c), buf, n, C.byref(cnt))
+    if rc:
+        raise CollatzError(rc, "step1_pairs")
+    out = []
+    for i in range(n):
+        w = buf[8 * i:8 * i + 8]
+        out.append((w[3], w[0] | (w[1] << 32) | (w[2] << 64), _limbs(w[4:8])))
+    return out
+
+
+class Verifier:
+    """One device context (tables resident in HBM)."""
+
+    def __init__(self, maxbits: int = 45, range_k: int = 24, device: int = 0,
+                 variant: int | None = None, iter_cap: int = 0):
+        cfg = Config()
+        lib().collatz_config_default(C.byref(cfg))
+        cfg.maxbits, cfg.range_k, cfg.device = maxbits, range_k, device
+        cfg.iter_cap = iter_cap
+        if variant is not None:
+            cfg.variant = variant
+        h = C.c_void_p()
+        rc = lib().collatz_create(C.byref(cfg), C.byref(h))
+        if rc:
+            raise CollatzError(rc, status_string(rc))
+        self._h = h
+        self.maxbits = maxbits
+        self.range_k = range_k
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().collatz_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc: int, what: str):
+        if rc:
+            raise CollatzError(rc, f"{what}: {status_string(rc)}: "
+                                   f"{lib().collatz_last_error(self._h).decode()}")
+
+    @property
+    def handle(self):
+        return self._h
+
+    def device_info(self):
+        sm, clk = C.c_int(), C.c_int()
+        self._check(lib().collatz_device_info(self._h, C.byref(sm), C.byref(clk)), "device_info")
+        return sm.value, clk.value
+
+    def set_stream(self, stream_handle: int | None):
+        self._check(lib().collatz_set_stream(self._h, C.c_void_p(stream_handle or 0)), "set_stream")
+
+    def set_variant(self, mode: int, variant: int):
+        self._check(lib().collatz_set_variant(self._h, mode, variant), "set_variant")
+
+    # ---- cases mode ----
+    def run_case(self, base, sigfig, threepower, number, doubleeven, numevens,
+                 overflow_cap: int = 1 << 16, check: bool = True) -> CaseResult:
+        c = make_case(base, sigfig, threepower, number, doubleeven, numevens)
+        r = CaseResultC()
+        ov = (C.c_uint32 * (4 * overflow_cap))()
+        r.overflow_seeds = C.cast(ov, C.POINTER(C.c_uint32))
+        r.overflow_cap = overflow_cap
+        rc = lib().collatz_run_case(self._h, C.byref(c), C.byref(r))
+        if check:
+            self._check(rc, "run_case")
+        return _case_result(r, ov, overflow_cap)
+
+    def launchkernel(self, bigindex: int, pairs, overflow_cap: int = 1 << 16,
+                     check: bool = True) -> CaseResult:
+        """One batch of pairs [(base, number)] or a packed uint32 buffer."""
+        if isinstance(pairs, (list, tuple)):
+            buf, n = pack_pairs(pairs), len(pairs)
+        else:
+            buf, n = pairs, len(pairs) // 8
+        r = CaseResultC()
+        ov = (C.c_uint32 * (4 * overflow_cap))()
+        r.overflow_seeds = C.cast(ov, C.POINTER(C.c_uint32))
+        r.overflow_cap = overflow_cap
+        rc = lib().collatz_verify_pairs(self._h, bigindex, buf, n, C.byref(r))
+        if check:
+            self._check(rc, "verify_pairs")
+        return _case_result(r, ov, overflow_cap)
+
+    verify_pairs = launchkernel
+
+    def case_tables(self) -> tuple[bytes, bytes]:
+        bv = (C.c_uint32 * (16 * BV_WORDS))()
+        m9 = (C.c_uint32 * (9 * 32))()
+        self._check(lib().collatz_case_tables(self._h, bv, m9), "case_tables")
+        return bytes(bv), bytes(m9)
+
+    # ---- range mode ----
+    def range_sieve(self, k: int) -> tuple[int, bytes]:
+        cnt = C.c_uint64()
+        buf = (C.c_uint8 * ((1 << k) // 8))()
+        self._check(lib().collatz_range_sieve(self._h, k, buf, C.byref(cnt)), "range_sieve")
+        return cnt.value, bytes(buf)
+
+    def verify_range(self, offset: int, size: int, k: int = 0, mod9: bool = True,
+                     check: bool = True) -> RangeResult:
+        r = make_range(offset, size, k, mod9)
+        out = RangeResultC()
+        rc = lib().collatz_verify_range(self._h, C.byref(r), C.byref(out))
+        if check:
+            self._check(rc, "verify_range")
+        return _range_result(out)
+
+    def verify_batch(self, reqs, check: bool = True) -> list[RangeResult]:
+        """reqs: [(offset, size)] or [(offset, size, k, mod9)]."""
+        n = len(reqs)
+        arr = (Range * n)()
+        for i, q in enumerate(reqs):
+            arr[i] = make_range(*q)
+        out = (RangeResultC * n)()
+        rc = lib().collatz_verify_batch(self._h, arr, n, out)
+        if check:
+            self._check(rc, "verify_batch")
+        return [_range_result(out[i]) for i in range(n)]
+
+    def plan(self, reqs) -> "Plan":
+        return Plan(self, reqs)
+
+    # ---- trajectory queries ----
+    def trajectory(self, seeds) -> list[tuple[int, int, int]]:
+        """[(status, stopping_time, excursion)] per seed (< 2^256)."""
+        n = len(seeds)
+        arr = (C.c_uint32 * (8 * max(1, n)))()
+        for i, s in enumerate(seeds):
+            if s < 0 or s >> 256:
+                raise ValueError("seeds must be in [0, 2^256)")
+            for j in range(8):
+                arr[8 * i + j] = (s >> (32 * j)) & 0xFFFFFFFF
+        st = (C.c_uint64 * max(1, n))()
+        exc = (C.c_uint32 * (16 * max(1, n)))()
+        status = (C.c_uint32 * max(1, n))()
+        self._check(lib().collatz_trajectory(self._h, arr, n, st, exc, status), "trajectory")
+        return [(status[i], st[i], _limbs(exc[16 * i:16 * i + 16])) for i in range(n)]
+
+
+class Plan:
+    """Lowered range requests + a captured CUDA graph, relaunchable."""
+
+    def __init__(self, v: Verifier, reqs):
+        self.v = v
+        self.n = len(reqs)
+        arr = (Range * self.n)()
+        for i, q in enumerate(reqs):
+            arr[i] = make_range(*q)
+        h = C.c_void_p()
+        v._check(lib().collatz_plan_create(v.handle, arr, self.n, C.byref(h)), "plan_create")
+        self._h = h
+
+    def launch(self):
+        self.v._check(lib().collatz_plan_launch(self._h), "plan_launch")
+
+    def results(self, check: bool = True) -> list[RangeResult]:
+        out = (RangeResultC * self.n)()
+        rc = lib().collatz_plan_results(self._h, out)
+        if check:
+            self.v._check(rc, "plan_results")
+        return [_range_result(out[i]) for i in range(self.n)]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().collatz_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def combine_range_results(parts: list[RangeResult]) -> RangeResult:
+    """Merges results of disjoint sub-ranges (sum, max with the smaller seed on ties)."""
+    out = RangeResult(0, 0, 0, 0, 0, 0, 0)
+    have = False
+    for p in parts:
+        out.seeds_checked += p.seeds_checked
+        out.failures += p.failures
+        out.widened += p.widened
+        out.errors |= p.errors
+        if p.seeds_checked == 0:
+            continue
+        if not have or (p.max_excursion, -p.max_excursion_seed) > (out.max_excursion, -out.max_excursion_seed):
+            out.max_excursion, out.max_excursion_seed = p.max_excursion, p.max_excursion_seed
+        if not have or (p.max_stopping_time, -p.max_stopping_time_seed) > \
+                (out.max_stopping_time, -out.max_stopping_time_seed):
+            out.max_stopping_time, out.max_stopping_time_seed = p.max_stopping_time, p.max_stopping_time_seed
+        have = True
+    return out

@@ -1,0 +1,848 @@
+// api.cu -- the C ABI of include/collatz.h: context, cases mode (host
+// Step 1 feeding the GPU), range plans (lowered work lists + captured CUDA
+// graphs), trajectory queries.
+#include <algorithm>
+#include <atomic>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <thread>
+
+#include "runtime.h"
+
+using namespace cz;
+
+static const size_t BV_WORDS_HOST = (1u << 19) + 32u;
+
+#define CK(c, expr)                                                  \
+  do {                                                               \
+    cudaError_t e_ = (expr);                                         \
+    if (e_ != cudaSuccess) return cz::set_cuda_error((c), e_, #expr); \
+  } while (0)
+
+namespace cz {
+
+int set_cuda_error(collatz_ctx* c, cudaError_t e, const char* where) {
+  if (c) c->err = std::string(where) + ": " + cudaGetErrorString(e);
+  cudaGetLastError();
+  return COLLATZ_E_CUDA;
+}
+
+static u128 u128_of(const uint64_t* x) { return ((u128)x[1] << 64) | x[0]; }
+
+static void limbs4(u128 x, uint32_t* w) {
+  for (int i = 0; i < 4; i++) w[i] = (uint32_t)(x >> (32 * i));
+}
+
+static int grid_for(collatz_ctx* c, int mode, int variant) {
+  int bps = 0;
+  cudaError_t e = mode == 0 ? cases_occupancy(variant, &bps) : range_occupancy(variant, &bps);
+  if (e != cudaSuccess || bps <= 0) bps = 1;
+  return bps * c->sm_count;
+}
+
+void rec_to_range_result(const ReqRec& r, collatz_range_result* out) {
+  std::memset(out, 0, sizeof *out);
+  out->seeds_checked = r.seeds;
+  out->failures = r.failures;
+  out->widened = r.widened;
+  if (r.valid & 2u) {
+    std::memcpy(out->max_excursion, r.E, sizeof r.E);
+    std::memcpy(out->max_excursion_seed, r.E_seed, sizeof r.E_seed);
+  }
+  if (r.valid & 1u) {
+    out->max_stopping_time = r.st;
+    std::memcpy(out->max_stopping_time_seed, r.st_seed, sizeof r.st_seed);
+  }
+  out->errors = r.errors;
+  out->status = r.errors ? COLLATZ_E_DEVICE : COLLATZ_OK;
+}
+
+// ---------------------------------------------------------------------
+// Range tables and lowering of requests into work segments.
+// ---------------------------------------------------------------------
+
+int get_range_tables(collatz_ctx* c, uint32_t k, RangeTables** out) {
+  auto it = c->rt.find(k);
+  if (it != c->rt.end()) {
+    *out = &it->second;
+    return COLLATZ_OK;
+  }
+  RangeTables T;
+  cudaError_t e = build_range_table(&T.dev, k, true, c->own_stream);
+  if (e != cudaSuccess) {
+    free_range_table(&T.dev);
+    return set_cuda_error(c, e, "build_range_table");
+  }
+  if (T.dev.violations) {
+    c->err = "range sieve validation failed for k=" + std::to_string(k);
+    free_range_table(&T.dev);
+    return COLLATZ_E_DEVICE;
+  }
+  if (k <= 28 && T.dev.count) {
+    std::vector<RangeEntry> h(T.dev.count);
+    e = cudaMemcpy(h.data(), T.dev.table, sizeof(RangeEntry) * T.dev.count, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return set_cuda_error(c, e, "range table copy");
+    T.residues.resize(T.dev.count);
+    for (size_t i = 0; i < h.size(); i++) T.residues[i] = (uint64_t)h[i].r_lo | ((uint64_t)(h[i].meta & 0xFF) << 32);
+  }
+  auto ins = c->rt.emplace(k, std::move(T));
+  *out = &ins.first->second;
+  return COLLATZ_OK;
+}
+
+// index of the first survivor >= r
+static int lower_bound_res(collatz_ctx* c, const RangeTables& T, uint64_t r, uint32_t* out) {
+  if (r >= (1ull << T.dev.k)) {
+    *out = (uint32_t)T.dev.count;
+    return COLLATZ_OK;
+  }
+  if (!T.residues.empty() || T.dev.count == 0) {
+    *out = (uint32_t)(std::lower_bound(T.residues.begin(), T.residues.end(), r) - T.residues.begin());
+    return COLLATZ_OK;
+  }
+  uint64_t lo = 0, hi = T.dev.count;  // binary search with single-entry reads
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) / 2;
+    RangeEntry e;
+    cudaError_t err = cudaMemcpy(&e, T.dev.table + mid, sizeof e, cudaMemcpyDeviceToHost);
+    if (err != cudaSuccess) return set_cuda_error(c, err, "lower_bound");
+    const uint64_t rr = (uint64_t)e.r_lo | ((uint64_t)(e.meta & 0xFF) << 32);
+    if (rr < r) lo = mid + 1; else hi = mid;
+  }
+  *out = (uint32_t)lo;
+  return COLLATZ_OK;
+}
+
+int lower_range(collatz_ctx* c, const collatz_range& r, uint32_t req, const RangeTables& T,
+                std::vector<RangeSeg>& segs, unsigned long long& items) {
+  const uint32_t k = T.dev.k;
+  const u128 O = u128_of(r.offset), S = r.size, E = O + S;
+  if (r.size > (1ull << 48) || E > ((u128)1 << 96) || E < O) return COLLATZ_E_LIMIT;
+  const uint32_t mod9 = (r.flags & COLLATZ_RANGE_NO_MOD9) ? 0u : 1u;
+  const u128 K = (u128)1 << k;
+  if (S == 0) return COLLATZ_OK;
+  if (O < K) {  // integers below 2^k: no residue sieve
+    const uint64_t d_lo = (uint64_t)O, d_hi = (uint64_t)std::min(E, K);
+    RangeSeg g{};
+    g.item_begin = items;
+    g.q_lo = d_lo;
+    g.d_hi = d_hi;
+    g.req = req;
+    g.kind = 1;
+    g.mod9 = mod9;
+    segs.push_back(g);
+    items += (d_hi - d_lo + DENSE_ITEM - 1) / DENSE_ITEM;
+  }
+  const u128 lo = std::max(O, K);
+  if (lo >= E) return COLLATZ_OK;
+  const u128 qa = lo >> k, qb = (E - 1) >> k;
+  uint32_t sa, sb;
+  int rc = lower_bound_res(c, T, (uint64_t)(lo & (K - 1)), &sa);
+  if (rc) return rc;
+  rc = lower_bound_res(c, T, (uint64_t)((E - 1) & (K - 1)) + 1, &sb);
+  if (rc) return rc;
+  const uint32_t ns = (uint32_t)T.dev.count;
+  auto add = [&](u128 q, u128 nq, uint32_t s_lo, uint32_t s_hi) {
+    if (s_lo >= s_hi || nq == 0) return;
+    const uint32_t ipq = (s_hi - s_lo + RANGE_ITEM - 1) / RANGE_ITEM;
+    while (nq > 0) {
+      const uint32_t take = (uint32_t)std::min(nq, (u128)0x7FFFFFFF);
+      RangeSeg g{};
+      g.item_begin = items;
+      g.q_lo = (uint64_t)q;
+      g.q_hi = (uint32_t)(q >> 64);
+      g.nq = take;
+      g.s_lo = s_lo;
+      g.s_hi = s_hi;
+      g.ipq = ipq;
+      g.req = req;
+      g.kind = 0;
+      g.mod9 = mod9;
+      segs.push_back(g);
+      items += (unsigned long long)take * ipq;
+      q += take;
+      nq -= take;
+    }
+  };
+  if (qa == qb) {
+    add(qa, 1, sa, sb);
+  } else {
+    add(qa, 1, sa, ns);
+    add(qa + 1, qb - qa - 1, 0, ns);
+    add(qb, 1, 0, sb);
+  }
+  return COLLATZ_OK;
+}
+
+}  // namespace cz
+
+// =====================================================================
+// Context.
+// =====================================================================
+
+extern "C" void collatz_config_default(collatz_config* cfg) {
+  if (!cfg) return;
+  std::memset(cfg, 0, sizeof *cfg);
+  cfg->maxbits = 45;
+  cfg->range_k = 24;
+  cfg->device = 0;
+  cfg->variant = COLLATZ_VARIANT_AUTO;
+  cfg->iter_cap = 0;
+}
+
+extern "C" const char* collatz_status_string(int s) {
+  switch (s) {
+    case COLLATZ_OK: return "ok";
+    case COLLATZ_E_ARG: return "invalid argument";
+    case COLLATZ_E_CUDA: return "CUDA error";
+    case COLLATZ_E_NOMEM: return "out of memory";
+    case COLLATZ_E_LIMIT: return "request beyond limits";
+    case COLLATZ_E_DEVICE: return "device reported an error";
+    case COLLATZ_E_TIMEOUT: return "timed out";
+    case COLLATZ_E_STATE: return "invalid state";
+    case COLLATZ_E_ADMISSION: return "refused by device-memory admission";
+    case COLLATZ_E_NODEV: return "no usable CUDA device";
+    default: return "unknown status";
+  }
+}
+
+extern "C" const char* collatz_last_error(const collatz_ctx* c) { return c ? c->err.c_str() : ""; }
+
+extern "C" int collatz_create(const collatz_config* cfg, collatz_ctx** out) {
+  if (!cfg || !out) return COLLATZ_E_ARG;
+  *out = nullptr;
+  if (cfg->maxbits < 16 || cfg->maxbits > 96) return COLLATZ_E_ARG;
+  if (cfg->range_k < 8 || cfg->range_k > 34) return COLLATZ_E_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return COLLATZ_E_NODEV;
+  }
+  if (cfg->device < 0 || cfg->device >= ndev) return COLLATZ_E_ARG;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess) return COLLATZ_E_NODEV;
+  if (prop.major != 10 || prop.minor != 0) return COLLATZ_E_NODEV;  // kernels are built for sm_100a only
+  collatz_ctx* c = new collatz_ctx();
+  c->cfg = *cfg;
+  c->device = cfg->device;
+  c->sm_count = prop.multiProcessorCount;
+  int clk = 0;
+  cudaDeviceGetAttribute(&clk, cudaDevAttrClockRate, c->device);
+  c->sm_clock_khz = clk;
+  if (cfg->iter_cap) c->iter_cap = cfg->iter_cap;
+  if (cfg->variant != COLLATZ_VARIANT_AUTO) {
+    if ((int)cfg->variant >= range_variants()) {
+      delete c;
+      return COLLATZ_E_ARG;
+    }
+    c->range_variant = (int)cfg->variant;
+  }
+  int rc = COLLATZ_OK;
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);
+  for (int i = 0; i < 4 && e == cudaSuccess; i++) e = cudaEventCreate(&c->ev[i]);
+  if (e == cudaSuccess) e = build_case_tables(&c->ct, cfg->maxbits, c->own_stream);
+  if (e != cudaSuccess) {
+    rc = set_cuda_error(c, e, "collatz_create");
+    collatz_destroy(c);
+    return rc;
+  }
+  c->stream = c->own_stream;
+  *out = c;
+  return COLLATZ_OK;
+}
+
+extern "C" void collatz_destroy(collatz_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->own_stream) cudaStreamSynchronize(c->own_stream);
+  if (c->stream && c->stream != c->own_stream) cudaStreamSynchronize(c->stream);
+  free_case_tables(&c->ct);
+  for (auto& kv : c->rt) free_range_table(&kv.second.dev);
+  DevBuf* bufs[] = {&c->d_rec, &c->d_counter, &c->d_overflow, &c->d_ovcount, &c->d_pairs[0], &c->d_pairs[1],
+                    &c->d_segs, &c->d_widen, &c->d_widen2, &c->d_wcount, &c->t_seeds, &c->t_st, &c->t_exc,
+                    &c->t_status, &c->t_idx[0], &c->t_idx[1], &c->t_cnt};
+  for (DevBuf* b : bufs) b->release();
+  c->h_rec.release();
+  c->h_pairs.release();
+  for (auto& ev : c->ev)
+    if (ev) cudaEventDestroy(ev);
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  delete c;
+}
+
+extern "C" int collatz_set_stream(collatz_ctx* c, void* s) {
+  if (!c) return COLLATZ_E_ARG;
+  std::lock_guard<std::recursive_mutex> g(c->mu);
+  c->stream = s ? (cudaStream_t)s : c->own_stream;
+  return COLLATZ_OK;
+}
+
+extern "C" int collatz_device_info(const collatz_ctx* c, int* sm_count, int* sm_clock_khz) {
+  if (!c) return COLLATZ_E_ARG;
+  if (sm_count) *sm_count = c->sm_count;
+  if (sm_clock_khz) *sm_clock_khz = c->sm_clock_khz;
+  return COLLATZ_OK;
+}
+
+extern "C" int collatz_variant_count(int mode) { return mode == 0 ? cases_variants() : range_variants(); }
+
+extern "C" int collatz_set_variant(collatz_ctx* c, int mode, int v) {
+  if (!c || v < 0 || v >= collatz_variant_count(mode)) return COLLATZ_E_ARG;
+  std::lock_guard<std::recursive_mutex> g(c->mu);
+  if (mode == 0) c->cases_variant = v; else c->range_variant = v;
+  return COLLATZ_OK;
+}
+
+// =====================================================================
+// Cases mode.
+// =====================================================================
+
+static int case_prepare(collatz_ctx* c) {
+  CK(c, c->d_rec.ensure(sizeof(ReqRec)));
+  CK(c, c->d_counter.ensure(sizeof(uint32_t) * 4));
+  CK(c, c->d_overflow.ensure(sizeof(uint32_t) * 4 * OVERFLOW_CAP));
+  CK(c, c->d_ovcount.ensure(sizeof(unsigned long long)));
+  CK(c, c->h_rec.ensure(sizeof(ReqRec) + 64));
+  CK(c, cudaMemsetAsync(c->d_rec.p, 0, sizeof(ReqRec), c->stream));
+  CK(c, cudaMemsetAsync(c->d_ovcount.p, 0, sizeof(unsigned long long), c->stream));
+  return COLLATZ_OK;
+}
+
+static CasesArgs case_args(collatz_ctx* c, const uint32_t* d_pairs, uint32_t npairs, int bigindex) {
+  CasesArgs a;
+  a.pairs = d_pairs;
+  a.npairs = npairs;
+  a.bigindex = bigindex;
+  a.bv = c->ct.bv;
+  a.mod9 = c->ct.mod9;
+  a.magic = c->ct.magic;
+  a.pow3 = c->ct.pow3;
+  a.mbi = c->ct.mbi;
+  a.tpo = c->ct.tpo;
+  a.pair_counter = c->d_counter.as<uint32_t>();
+  a.rec = c->d_rec.as<ReqRec>();
+  a.overflow = c->d_overflow.as<uint32_t>();
+  a.overflow_cap = OVERFLOW_CAP;
+  a.overflow_count = c->d_ovcount.as<unsigned long long>();
+  a.iter_cap = c->iter_cap;
+  return a;
+}
+
+// Copies the record and the overflow list back (after the stream is idle).
+static int case_finish(collatz_ctx* c, collatz_case_result* out) {
+  ReqRec r;
+  unsigned long long nov = 0;
+  CK(c, cudaMemcpy(&r, c->d_rec.p, sizeof r, cudaMemcpyDeviceToHost));
+  CK(c, cudaMemcpy(&nov, c->d_ovcount.p, sizeof nov, cudaMemcpyDeviceToHost));
+  out->hash = r.hash;
+  out->spot_checks = 0;
+  out->seeds_checked = r.seeds;
+  out->n_overflow = nov;
+  out->errors = r.errors;
+  if (r.valid & 2u) {
+    std::memcpy(out->max_excursion, r.E, sizeof out->max_excursion);
+    std::memcpy(out->max_excursion_seed, r.E_seed, sizeof out->max_excursion_seed);
+  } else {
+    std::memset(out->max_excursion, 0, sizeof out->max_excursion);
+    std::memset(out->max_excursion_seed, 0, sizeof out->max_excursion_seed);
+  }
+  if (r.valid & 1u) {
+    out->max_stopping_time = r.st;
+    std::memcpy(out->max_stopping_time_seed, r.st_seed, sizeof out->max_stopping_time_seed);
+  } else {
+    out->max_stopping_time = 0;
+    std::memset(out->max_stopping_time_seed, 0, sizeof out->max_stopping_time_seed);
+  }
+  const uint64_t have = std::min<uint64_t>(nov, OVERFLOW_CAP);
+  if (out->overflow_seeds && out->overflow_cap && have) {
+    std::vector<uint32_t> ov(4 * have);
+    CK(c, cudaMemcpy(ov.data(), c->d_overflow.p, 16 * have, cudaMemcpyDeviceToHost));
+    std::vector<u128> seeds(have);
+    for (uint64_t i = 0; i < have; i++)
+      seeds[i] = (u128)ov[4 * i] | ((u128)ov[4 * i + 1] << 32) | ((u128)ov[4 * i + 2] << 64);
+    std::sort(seeds.begin(), seeds.end());
+    const uint64_t n = std::min<uint64_t>(have, out->overflow_cap);
+    for (uint64_t i = 0; i < n; i++) limbs4(seeds[i], out->overflow_seeds + 4 * i);
+  }
+  if (r.errors) {
+    c->err = "device error bits 0x" + std::to_string(r.errors);
+    return COLLATZ_E_DEVICE;
+  }
+  return COLLATZ_OK;
+}
+
+extern "C" int collatz_verify_pairs(collatz_ctx* c, uint32_t bigindex, const uint32_t* pairs, uint32_t npairs,
+                                    collatz_case_result* out) {
+  if (!c || !out || (npairs && !pairs)) return COLLATZ_E_ARG;
+  if (c->ct.tpo + bigindex >= POW3_COUNT) return COLLATZ_E_ARG;
+  std::lock_guard<std::recursive_mutex> g(c->mu);
+  uint32_t* ovbuf = out->overflow_seeds;
+  const uint64_t ovcap = out->overflow_cap;
+  std::memset(out, 0, sizeof *out);
+  out->overflow_seeds = ovbuf;
+  out->overflow_cap = ovcap;
+  CK(c, cudaSetDevice(c->device));
+  int rc = case_prepare(c);
+  if (rc) return rc;
+  if (npairs) {
+    CK(c, c->d_pairs[0].ensure(32ull * npairs));
+    CK(c, cudaMemcpyAsync(c->d_pairs[0].p, pairs, 32ull * npairs, cudaMemcpyHostToDevice, c->stream));
+    CK(c, cudaMemsetAsync(c->d_counter.p, 0, sizeof(uint32_t), c->stream));
+    CasesArgs a = case_args(c, c->d_pairs[0].as<uint32_t>(), npairs, (int)bigindex);
+    CK(c, cudaEventRecord(c->ev[0], c->stream));
+    CK(c, launch_cases(a, c->cases_variant, grid_for(c, 0, c->cases_variant), c->stream));
+    CK(c, cudaEventRecord(c->ev[1], c->stream));
+  }
+  CK(c, cudaStreamSynchronize(c->stream));
+  if (npairs) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    out->device_ms = ms;
+    if (bigindex < 16) {
+      out->pairs = npairs;
+      out->launches = 1;  // launchkernel returns 1 for a non-empty batch (cu:648)
+    } else {
+      out->cpu_pairs = npairs;
+    }
+  }
+  return case_finish(c, out);
+}
+
+extern "C" int collatz_step1_pairs(uint32_t maxbits, const collatz_case* cs, uint32_t* pairs, uint64_t cap,
+                                   uint64_t* count) {
+  if (!cs || !count || (cap && !pairs) || maxbits < 16 || maxbits > 96) return COLLATZ_E_ARG;
+  const uint32_t mbi = maxbits - 10, tpo = mbi * 306 / 485 + 1;
+  if (cs->sigfig > mbi || cs->threepower >= 128) return COLLATZ_E_ARG;
+  Step1 s1(mbi, tpo);
+  Step1Node root{u128_of(cs->base), cs->sigfig, cs->threepower, u128_of(cs->number), cs->doubleeven, cs->numevens};
+  uint64_t n = 0;
+  s1.leaves(root, [&](uint32_t bi, u128 b, u128 num) {
+    if (n < cap) pack_pair(pairs + 8 * n, b, num, bi);
+    n++;
+  });
+  *count = n;
+  return COLLATZ_OK;
+}
+
+namespace {
+
+// Host Step 1 on all cores feeding batches of pairs to the GPU.
+struct CasePipeline {
+  std::mutex mu;
+  std::condition_variable cv_free, cv_full;
+  std::deque<int> free_bufs;
+  std::deque<std::pair<int, uint32_t>> full;
+  int workers_left = 0;
+  uint32_t* host = nullptr;  // nbuf x CASE_BATCH pairs (pinned)
+
+  int acquire() {
+    std::unique_lock<std::mutex> l(mu);
+    cv_free.wait(l, [&] { return !free_bufs.empty(); });
+    const int b = free_bufs.front();
+    free_bufs.pop_front();
+    return b;
+  }
+  void submit(int b, uint32_t n) {
+    {
+      std::lock_guard<std::mutex> l(mu);
+      full.emplace_back(b, n);
+    }
+    cv_full.notify_one();
+  }
+  void release(int b) {
+    {
+      std::lock_guard<std::mutex> l(mu);
+      free_bufs.push_back(b);
+    }
+    cv_free.notify_one();
+  }
+};
+
+struct CaseWorker {
+  CasePipeline* P;
+  int buf = -1;
+  uint32_t n = 0;
+  uint64_t counts[17] = {};  // [16] = bigindex >= 16
+  static void leaf(void* vctx, uint32_t bi, u128 base, u128 number) {
+    CaseWorker* w = (CaseWorker*)vctx;
+    if (w->buf < 0) w->buf = w->P->acquire();
+    pack_pair(w->P->host + (size_t)w->buf * CASE_BATCH * 8 + 8ull * w->n, base, number, bi);
+    w->counts[bi < 16 ? bi : 16]++;
+    if (++w->n == CASE_BATCH) {
+      w->P->submit(w->buf, w->n);
+      w->buf = -1;
+      w->n = 0;
+    }
+  }
+};
+
+}  // namespace
+
+extern "C" int collatz_run_case(collatz_ctx* c, const collatz_case* cs, collatz_case_result* out) {
+  if (!c || !cs || !out) return COLLATZ_E_ARG;
+  if (cs->sigfig > c->ct.mbi || cs->threepower >= 128) return COLLATZ_E_ARG;  // cu:515 is never reached
+  std::lock_guard<std::recursive_mutex> g(c->mu);
+  uint32_t* ovbuf = out->overflow_seeds;
+  const uint64_t ovcap = out->overflow_cap;
+  std::memset(out, 0, sizeof *out);
+  out->overflow_seeds = ovbuf;
+  out->overflow_cap = ovcap;
+  CK(c, cudaSetDevice(c->device));
+  int rc = case_prepare(c);
+  if (rc) return rc;
+
+  Step1 s1(c->ct.mbi, c->ct.tpo);
+  const Step1Node root{u128_of(cs->base), cs->sigfig, cs->threepower, u128_of(cs->number), cs->doubleeven,
+                       cs->numevens};
+  unsigned hw = std::thread::hardware_concurrency();
+  const int nthreads = (int)std::max(1u, std::min(hw ? hw : 1u, 64u));
+  // split the tree until there are enough independent subtrees
+  std::vector<Step1Node> roots;
+  uint32_t cut = cs->sigfig;
+  for (;;) {
+    roots.clear();
+    s1.split(root, cut, roots);
+    if (roots.size() >= (size_t)8 * nthreads || cut >= c->ct.mbi) break;
+    cut = std::min(c->ct.mbi, cut + 2);
+  }
+
+  const int nbuf = 2 * nthreads + 4;
+  CK(c, c->h_pairs.ensure((size_t)nbuf * CASE_BATCH * 32));
+  CK(c, c->d_pairs[0].ensure((size_t)CASE_BATCH * 32));
+  CK(c, c->d_pairs[1].ensure((size_t)CASE_BATCH * 32));
+  CasePipeline P;
+  P.host = c->h_pairs.as<uint32_t>();
+  for (int i = 0; i < nbuf; i++) P.free_bufs.push_back(i);
+  P.workers_left = nthreads;
+  std::atomic<size_t> next_root{0};
+  std::vector<CaseWorker> ws(nthreads);
+  std::vector<std::thread> th;
+  for (int t = 0; t < nthreads; t++) {
+    ws[t].P = &P;
+    th.emplace_back([&, t] {
+      CaseWorker& w = ws[t];
+      for (;;) {
+        const size_t i = next_root.fetch_add(1);
+        if (i >= roots.size()) break;
+        s1.leaves_fn(roots[i], &CaseWorker::leaf, &w);
+      }
+      if (w.buf >= 0 && w.n) P.submit(w.buf, w.n);
+      else if (w.buf >= 0) P.release(w.buf);
+      {
+        std::lock_guard<std::mutex> l(P.mu);
+        P.workers_left--;
+      }
+      P.cv_full.notify_one();
+    });
+  }
+
+  // consumer: H2D on the copy stream, kernel on the compute stream
+  cudaEvent_t copied[2], kdone[2];
+  for (int i = 0; i < 2; i++) {
+    cudaEventCreateWithFlags(&copied[i], cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&kdone[i], cudaEventDisableTiming);
+  }
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> timing;
+  uint64_t batches = 0;
+  cudaError_t err = cudaSuccess;
+  for (;;) {
+    std::pair<int, uint32_t> job;
+    {
+      std::unique_lock<std::mutex> l(P.mu);
+      P.cv_full.wait(l, [&] { return !P.full.empty() || P.workers_left == 0; });
+      if (P.full.empty()) break;
+      job = P.full.front();
+      P.full.pop_front();
+    }
+    const int slot = (int)(batches & 1);
+    if (err == cudaSuccess) {
+      if (batches >= 2) err = cudaStreamWaitEvent(c->copy_stream, kdone[slot], 0);
+      if (!err)
+        err = cudaMemcpyAsync(c->d_pairs[slot].p, P.host + (size_t)job.first * CASE_BATCH * 8, 32ull * job.second,
+                              cudaMemcpyHostToDevice, c->copy_stream);
+      if (!err) err = cudaEventRecord(copied[slot], c->copy_stream);
+      if (!err) err = cudaStreamWaitEvent(c->stream, copied[slot], 0);
+      if (!err) err = cudaMemsetAsync(c->d_counter.p, 0, sizeof(uint32_t), c->stream);
+      cudaEvent_t e0, e1;
+      cudaEventCreate(&e0);
+      cudaEventCreate(&e1);
+      timing.emplace_back(e0, e1);
+      if (!err) err = cudaEventRecord(e0, c->stream);
+      if (!err) {
+        CasesArgs a = case_args(c, c->d_pairs[slot].as<uint32_t>(), job.second, -1);
+        err = launch_cases(a, c->cases_variant, grid_for(c, 0, c->cases_variant), c->stream);
+      }
+      if (!err) err = cudaEventRecord(e1, c->stream);
+      if (!err) err = cudaEventRecord(kdone[slot], c->stream);
+      if (!err) err = cudaEventSynchronize(copied[slot]);
+    }
+    P.release(job.first);
+    batches++;
+  }
+  for (auto& t : th) t.join();
+  if (err == cudaSuccess) err = cudaStreamSynchronize(c->stream);
+  double ms = 0;
+  for (auto& ev : timing) {
+    float x = 0;
+    if (err == cudaSuccess) cudaEventElapsedTime(&x, ev.first, ev.second);
+    ms += x;
+    cudaEventDestroy(ev.first);
+    cudaEventDestroy(ev.second);
+  }
+  for (int i = 0; i < 2; i++) {
+    cudaEventDestroy(copied[i]);
+    cudaEventDestroy(kdone[i]);
+  }
+  if (err != cudaSuccess) return set_cuda_error(c, err, "collatz_run_case");
+  uint64_t counts[17] = {};
+  for (auto& w : ws)
+    for (int i = 0; i < 17; i++) counts[i] += w.counts[i];
+  for (int b = 0; b < 16; b++) {
+    out->pairs += counts[b];
+    out->launches += (counts[b] + (1u << 16) - 1) >> 16;  // full buckets + final flush (cu:532-534, 177-179)
+  }
+  out->cpu_pairs = counts[16];
+  out->device_ms = ms;
+  return case_finish(c, out);
+}
+
+// =====================================================================
+// Range plans.
+// =====================================================================
+
+struct collatz_plan {
+  collatz_ctx* c = nullptr;
+  uint32_t n = 0;
+  RangeTables* T = nullptr;
+  std::vector<RangeSeg> segs;
+  unsigned long long items = 0;
+  DevBuf d_segs, d_recs, d_cursor, d_widen, d_widen2, d_wcount;
+  HostBuf h_recs;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  float last_ms = 0;
+};
+
+static int plan_build(collatz_ctx* c, const collatz_range* r, uint32_t n, collatz_plan* p) {
+  const uint32_t k = r[0].k ? r[0].k : c->cfg.range_k;
+  for (uint32_t i = 0; i < n; i++)
+    if ((r[i].k ? r[i].k : c->cfg.range_k) != k) return COLLATZ_E_ARG;  // one sieve per launch
+  if (k < 8 || k > 34) return COLLATZ_E_ARG;
+  int rc = get_range_tables(c, k, &p->T);
+  if (rc) return rc;
+  for (uint32_t i = 0; i < n; i++) {
+    rc = lower_range(c, r[i], i, *p->T, p->segs, p->items);
+    if (rc) return rc;
+  }
+  if (p->segs.empty()) {  // keep the kernel's segment search well-defined
+    RangeSeg g{};
+    g.kind = 1;
+    p->segs.push_back(g);
+  }
+  p->n = n;
+  CK(c, p->d_segs.ensure(sizeof(RangeSeg) * p->segs.size()));
+  CK(c, cudaMemcpy(p->d_segs.p, p->segs.data(), sizeof(RangeSeg) * p->segs.size(), cudaMemcpyHostToDevice));
+  CK(c, p->d_recs.ensure(sizeof(ReqRec) * std::max(1u, n)));
+  CK(c, p->h_recs.ensure(sizeof(ReqRec) * std::max(1u, n)));
+  CK(c, p->d_cursor.ensure(sizeof(unsigned long long)));
+  CK(c, p->d_widen.ensure(sizeof(WidenEntry) * WIDEN_CAP));
+  CK(c, p->d_widen2.ensure(sizeof(WidenEntry) * WIDEN_CAP));
+  CK(c, p->d_wcount.ensure(sizeof(uint32_t) * 2));
+
+  RangeArgs a;
+  a.table = p->T->dev.table;
+  a.k = k;
+  a.segs = p->d_segs.as<RangeSeg>();
+  a.nsegs = (uint32_t)p->segs.size();
+  a.item_cursor = p->d_cursor.as<unsigned long long>();
+  a.item_limit = p->items;
+  a.recs = p->d_recs.as<ReqRec>();
+  a.widen = p->d_widen.as<WidenEntry>();
+  a.widen_cap = WIDEN_CAP;
+  a.widen_count = p->d_wcount.as<uint32_t>();
+  a.iter_cap = c->iter_cap;
+  const uint32_t grid = (uint32_t)grid_for(c, 1, c->range_variant);
+  cudaStream_t s = c->own_stream;
+  CK(c, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = cudaMemsetAsync(p->d_recs.p, 0, sizeof(ReqRec) * std::max(1u, n), s);
+  if (!e) e = cudaMemsetAsync(p->d_cursor.p, 0, sizeof(unsigned long long), s);
+  if (!e) e = cudaMemsetAsync(p->d_wcount.p, 0, sizeof(uint32_t) * 2, s);
+  if (!e) e = launch_range(a, c->range_variant, grid, s);
+  if (!e)
+    e = launch_range_wide(p->d_widen.as<WidenEntry>(), p->d_wcount.as<uint32_t>(), WIDEN_CAP, 6, a.recs,
+                          p->d_widen2.as<WidenEntry>(), WIDEN_CAP, p->d_wcount.as<uint32_t>() + 1, c->iter_cap, s);
+  if (!e)
+    e = launch_range_wide(p->d_widen2.as<WidenEntry>(), p->d_wcount.as<uint32_t>() + 1, WIDEN_CAP, 8, a.recs,
+                          nullptr, 0, nullptr, c->iter_cap, s);
+  if (!e) e = cudaMemcpyAsync(p->h_recs.p, p->d_recs.p, sizeof(ReqRec) * std::max(1u, n), cudaMemcpyDeviceToHost, s);
+  cudaError_t e2 = cudaStreamEndCapture(s, &p->graph);
+  if (e) return set_cuda_error(c, e, "plan capture");
+  if (e2) return set_cuda_error(c, e2, "cudaStreamEndCapture");
+  CK(c, cudaGraphInstantiate(&p->exec, p->graph, 0));
+  return COLLATZ_OK;
+}
+
+extern "C" int collatz_plan_create(collatz_ctx* c, const collatz_range* r, uint32_t n, collatz_plan** out) {
+  if (!c || !r || !n || !out) return COLLATZ_E_ARG;
+  std::lock_guard<std::recursive_mutex> g(c->mu);
+  CK(c, cudaSetDevice(c->device));
+  collatz_plan* p = new collatz_plan();
+  p->c = c;
+  int rc = plan_build(c, r, n, p);
+  if (rc) {
+    collatz_plan_destroy(p);
+    return rc;
+  }
+  *out = p;
+  return COLLATZ_OK;
+}
+
+extern "C" int collatz_plan_launch(collatz_plan* p) {
+  if (!p || !p->exec) return COLLATZ_E_ARG;
+  collatz_ctx* c = p->c;
+  std::lock_guard<std::recursive_mutex> g(c->mu);
+  CK(c, cudaEventRecord(c->ev[2], c->stream));
+  CK(c, cudaGraphLaunch(p->exec, c->stream));
+  CK(c, cudaEventRecord(c->ev[3], c->stream));
+  return COLLATZ_OK;
+}
+
+extern "C" int collatz_plan_results(collatz_plan* p, collatz_range_result* out) {
+  if (!p || !out) return COLLATZ_E_ARG;
+  collatz_ctx* c = p->c;
+  std::lock_guard<std::recursive_mutex> g(c->mu);
+  CK(c, cudaStreamSynchronize(c->stream));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);
+  const ReqRec* h = p->h_recs.as<ReqRec>();
+  int status = COLLATZ_OK;
+  for (uint32_t i = 0; i < p->n; i++) {
+    rec_to_range_result(h[i], &out[i]);
+    out[i].device_ms = ms;
+    if (out[i].status) status = out[i].status;
+  }
+  return status;
+}
+
+extern "C" void collatz_plan_destroy(collatz_plan* p) {
+  if (!p) return;
+  if (p->exec) cudaGraphExecDestroy(p->exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  p->d_segs.release();
+  p->d_recs.release();
+  p->d_cursor.release();
+  p->d_widen.release();
+  p->d_widen2.release();
+  p->d_wcount.release();
+  p->h_recs.release();
+  delete p;
+}
+
+extern "C" int collatz_verify_batch(collatz_ctx* c, const collatz_range* r, uint32_t n, collatz_range_result* out) {
+  if (!c || !r || !n || !out) return COLLATZ_E_ARG;
+  collatz_plan* p = nullptr;
+  int rc = collatz_plan_create(c, r, n, &p);
+  if (rc) return rc;
+  rc = collatz_plan_launch(p);
+  if (!rc) rc = collatz_plan_results(p, out);
+  collatz_plan_destroy(p);
+  return rc;
+}
+
+extern "C" int collatz_verify_range(collatz_ctx* c, const collatz_range* r, collatz_range_result* out) {
+  return collatz_verify_batch(c, r, 1, out);
+}
+
+// =====================================================================
+// Trajectory queries.
+// =====================================================================
+
+extern "C" int collatz_trajectory(collatz_ctx* c, const uint32_t* seeds, uint32_t n, uint64_t* st, uint32_t* exc,
+                                  uint32_t* status) {
+  if (!c || (n && (!seeds || !st || !exc || !status))) return COLLATZ_E_ARG;
+  if (n == 0) return COLLATZ_OK;
+  std::lock_guard<std::recursive_mutex> g(c->mu);
+  CK(c, cudaSetDevice(c->device));
+  static const int classes[5] = {4, 6, 8, 12, 16};
+  std::vector<std::vector<uint32_t>> lists(5);
+  for (uint32_t i = 0; i < n; i++) {
+    uint32_t bl = 0;
+    for (int j = 7; j >= 0; j--)
+      if (seeds[8ull * i + j]) {
+        bl = 32u * j + (32u - __builtin_clz(seeds[8ull * i + j]));
+        break;
+      }
+    int cl = bl <= 96 ? 0 : bl <= 160 ? 1 : bl <= 224 ? 2 : bl <= 352 ? 3 : 4;
+    lists[cl].push_back(i);
+  }
+  CK(c, c->t_seeds.ensure(32ull * n));
+  CK(c, c->t_st.ensure(8ull * n));
+  CK(c, c->t_exc.ensure(64ull * n));
+  CK(c, c->t_status.ensure(4ull * n));
+  CK(c, c->t_idx[0].ensure(4ull * n));
+  CK(c, c->t_idx[1].ensure(4ull * n));
+  CK(c, c->t_cnt.ensure(16));
+  CK(c, cudaMemcpyAsync(c->t_seeds.p, seeds, 32ull * n, cudaMemcpyHostToDevice, c->stream));
+  std::vector<uint32_t> carry;
+  for (int ci = 0; ci < 5; ci++) {
+    std::vector<uint32_t>& L = lists[ci];
+    L.insert(L.end(), carry.begin(), carry.end());
+    carry.clear();
+    if (L.empty()) continue;
+    CK(c, cudaMemcpyAsync(c->t_idx[0].p, L.data(), 4ull * L.size(), cudaMemcpyHostToDevice, c->stream));
+    CK(c, cudaMemsetAsync(c->t_cnt.p, 0, 16, c->stream));
+    TrajArgs a;
+    a.seeds = c->t_seeds.as<uint32_t>();
+    a.nseeds = n;
+    a.index = c->t_idx[0].as<uint32_t>();
+    a.nindex = (uint32_t)L.size();
+    a.st = c->t_st.as<unsigned long long>();
+    a.exc = c->t_exc.as<uint32_t>();
+    a.status = c->t_status.as<uint32_t>();
+    a.next = ci < 4 ? c->t_idx[1].as<uint32_t>() : nullptr;
+    a.next_count = c->t_cnt.as<uint32_t>();
+    a.cursor = c->t_cnt.as<uint32_t>() + 1;
+    a.iter_cap = c->iter_cap;
+    const uint32_t grid = std::min<uint32_t>((uint32_t)(L.size() + 127) / 128, (uint32_t)c->sm_count * 8);
+    CK(c, launch_traj(a, classes[ci], grid, c->stream));
+    if (ci < 4) {
+      uint32_t cnt = 0;
+      CK(c, cudaMemcpyAsync(&cnt, c->t_cnt.p, 4, cudaMemcpyDeviceToHost, c->stream));
+      CK(c, cudaStreamSynchronize(c->stream));
+      if (cnt) {
+        carry.resize(cnt);
+        CK(c, cudaMemcpy(carry.data(), c->t_idx[1].p, 4ull * cnt, cudaMemcpyDeviceToHost));
+      }
+    }
+  }
+  CK(c, cudaMemcpyAsync(st, c->t_st.p, 8ull * n, cudaMemcpyDeviceToHost, c->stream));
+  CK(c, cudaMemcpyAsync(exc, c->t_exc.p, 64ull * n, cudaMemcpyDeviceToHost, c->stream));
+  CK(c, cudaMemcpyAsync(status, c->t_status.p, 4ull * n, cudaMemcpyDeviceToHost, c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  return COLLATZ_OK;
+}
+
+extern "C" int collatz_case_tables(collatz_ctx* c, uint32_t* bv, uint32_t* mod9) {
+  if (!c || !bv || !mod9) return COLLATZ_E_ARG;
+  std::lock_guard<std::recursive_mutex> g(c->mu);
+  CK(c, cudaSetDevice(c->device));
+  CK(c, cudaMemcpy(bv, c->ct.bv, sizeof(uint32_t) * 16 * BV_WORDS_HOST, cudaMemcpyDeviceToHost));
+  CK(c, cudaMemcpy(mod9, c->ct.mod9, sizeof(uint32_t) * 9 * 32, cudaMemcpyDeviceToHost));
+  return COLLATZ_OK;
+}
+
+extern "C" int collatz_range_sieve(collatz_ctx* c, uint32_t k, uint8_t* bits, uint64_t* count) {
+  if (!c || k < 8 || k > 34) return COLLATZ_E_ARG;
+  std::lock_guard<std::recursive_mutex> g(c->mu);
+  CK(c, cudaSetDevice(c->device));
+  RangeTables* T = nullptr;
+  int rc = get_range_tables(c, k, &T);
+  if (rc) return rc;
+  if (count) *count = T->dev.count;
+  if (bits) CK(c, cudaMemcpy(bits, T->dev.bits, (1ull << k) / 8, cudaMemcpyDeviceToHost));
+  return COLLATZ_OK;
+}

@@ -1,0 +1,343 @@
+// cases.cu -- reference-compatible Step 2 + Step 3 (collatz_cudav7.cu
+// compute_kernel, cu:185-411; search2/search3, cu:654-715) for batches of
+// Step-1 pairs.
+//
+// Design (B200): persistent warps.  A warp takes one pair at a time, reads
+// the 33 look-ahead words of BV_f with one coalesced load per lane, ANDs
+// the mod-9 row, and ranks the surviving high-bit values with popc + a warp
+// scan into a per-warp queue in shared memory.  Lanes pull seeds from the
+// queue as they finish, so a pair with 500 survivors no longer serialises
+// in one thread (the reference runs one pair per thread).  Each lane runs
+// the reference's checkpoint structure exactly -- [odd run <= 8, overflow
+// test, even run <= 31] x 2, XOR the low limb, stop when v < n -- so the
+// XOR hash, the seed count and the overflow list are identical; the order
+// of work does not matter because every output is an XOR, a sum or a max.
+// Stopping time and maximum excursion are tracked on the side.
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "kernels.h"
+#include "tables.h"
+
+namespace cz {
+
+constexpr u32 CQ = 1024;  // queue entries per warp (>= 31 + 570 survivors of one pair)
+constexpr u32 CR = 32;    // pair slots per warp (a queue of < 32 entries spans < 32 pairs)
+constexpr u32 CWARPS = 8;
+
+struct CasesWarp {
+  unsigned short q[CQ];   // (slot << 10) | a
+  u32 ring[CR][12];       // base0..2, number0..3, 3^f limbs 0..3, flags
+  u32 lane[32][8];        // per lane: [0] st, [1..3] seed, [4..7] seed-local max E
+  u32 thr[4];             // excursion threshold (lower bound of the running max)
+};
+
+template <int ITERS, int REFILL_MIN>
+__global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
+  __shared__ CasesWarp S[CWARPS];
+  __shared__ u32 s_pow3[9];
+  const u32 lane = lane_id();
+  CasesWarp& W = S[threadIdx.x >> 5];
+  if (threadIdx.x < 9) {
+    u32 p = 1;
+    for (u32 i = 0; i < threadIdx.x; i++) p *= 3;
+    s_pow3[threadIdx.x] = p;  // THREEPOWERSU16, cu:61
+  }
+  if (lane < 4) W.thr[lane] = 0;
+  __syncthreads();
+
+  const u32 mbi = A.mbi;
+  // warp-uniform state
+  u32 qhead = 0, qcount = 0, ring_seq = 0;
+  bool exhausted = false;
+  u32 thr_st = 0, thr3 = 0, thr2 = 0;
+  ull warp_seeds = 0;
+  // lane state
+  bool active = false;
+  u32 v0 = 0, v1 = 0, v2 = 0, v3 = 0, n0 = 0, n1 = 0, n2 = 0;
+  u32 st = 0, iters = 0, hash = 0;
+  u32 found = 0, ovf = 0, cpu = 0, evalid = 0, pend = 0;
+
+  for (;;) {
+    // ---- offers of finished seeds, one lane at a time (bounded locks) ----
+    {
+      u32 pm = __ballot_sync(FULL, pend != 0);
+      while (pm) {
+        const u32 leader = __ffs(pm) - 1;
+        if (lane == leader) {
+          u32 seed[4] = {W.lane[lane][1], W.lane[lane][2], W.lane[lane][3], 0};
+          if (pend & 1u) rec_offer_st(A.rec, W.lane[lane][0], seed);
+          if (pend & 2u) rec_offer_e<4>(A.rec, &W.lane[lane][4], seed);
+          pend = 0;
+        }
+        pm &= pm - 1;
+      }
+      __syncwarp();
+    }
+
+    // ---- refill the queue and hand seeds to idle lanes ----
+    const u32 idle = __ballot_sync(FULL, !active);
+    const u32 nidle = __popc(idle);
+    if (nidle >= (u32)REFILL_MIN || nidle == 32u) {
+      while (qcount < nidle && !exhausted) {
+        u32 p = 0;
+        if (lane == 0) p = atomicAdd(A.pair_counter, 1u);
+        p = __shfl_sync(FULL, p, 0);
+        if (p >= A.npairs) {
+          exhausted = true;
+          break;
+        }
+        // thresholds: refreshed once per pair
+        {
+          ull sk = 0, ek = 0;
+          if (lane == 0) {
+            sk = *(volatile ull*)&A.rec->st_key;
+            ek = *(volatile ull*)&A.rec->e_key;
+          }
+          sk = __shfl_sync(FULL, sk, 0);
+          ek = __shfl_sync(FULL, ek, 0);
+          thr_st = (u32)sk;
+          u32 t[4];
+          key_decode<4>(ek, t);
+          if (lane < 4) W.thr[lane] = t[lane];
+          thr3 = t[3];
+          thr2 = t[2];
+        }
+        // Step 2 (cu:198-235): sieve words for this pair
+        const u32* P = A.pairs + 8ull * p;
+        const u32 pw = (lane < 8) ? P[lane] : 0u;
+        const u32 b0 = __shfl_sync(FULL, pw, 0), b1 = __shfl_sync(FULL, pw, 1);
+        const u32 b2 = __shfl_sync(FULL, pw, 2), b3 = __shfl_sync(FULL, pw, 3);
+        const u32 m0 = __shfl_sync(FULL, pw, 4);
+        u32 bi = (A.bigindex >= 0) ? (u32)A.bigindex : b3;
+        u32 f = A.tpo + bi;
+        if (f >= POW3_COUNT) f = POW3_COUNT - 1;
+        const u32 red = ((b0 % 9u) + 4u * (b1 % 9u) + 7u * (b2 % 9u)) % 9u;  // 2^32 = 4, 2^64 = 7 (mod 9)
+        u32 word = A.mod9[red * 32u + lane];
+        if (bi < 16u) {
+          const u32 idx = (A.magic[bi] * m0) & ((1u << 24) - 1);
+          const u32* row = A.bv + (size_t)bi * BV_WORDS + (idx >> 5);
+          const u32 lo = row[lane];
+          u32 hi = __shfl_down_sync(FULL, lo, 1);
+          if (lane == 31) hi = row[32];
+          word &= __funnelshift_r(lo, hi, idx & 31u);
+        }
+        u32 total;
+        const u32 excl = warp_excl_scan(__popc(word), &total);
+        if (total) {
+          const u32 slot = ring_seq & (CR - 1);
+          ring_seq++;
+          const u32 rv = __shfl_sync(FULL, pw, lane < 3 ? lane : lane + 1);  // base0..2, number0..3
+          if (lane < 7) W.ring[slot][lane] = rv;
+          if (lane >= 7 && lane < 11) W.ring[slot][lane] = A.pow3[4u * f + (lane - 7)];
+          if (lane == 11) W.ring[slot][11] = (bi >= 16u) ? 1u : 0u;
+          u32 pos = qhead + qcount + excl;
+          while (word) {
+            const u32 j = ctz32(word);
+            word &= word - 1;
+            W.q[pos & (CQ - 1)] = (unsigned short)((slot << 10) | (lane * 32u + j));
+            pos++;
+          }
+          qcount += total;
+          warp_seeds += total;
+        }
+        __syncwarp();
+      }
+      const u32 take = min(nidle, qcount);
+      if (!active) {
+        const u32 rank = __popc(idle & lanemask_lt());
+        if (rank < take) {
+          const u32 e = W.q[(qhead + rank) & (CQ - 1)];
+          const u32* R = W.ring[e >> 10];
+          const u32 a = e & 1023u;
+          // seed n = base | a << (N-A)  (cu:241-260)
+          n0 = R[0];
+          n1 = R[1];
+          n2 = R[2];
+          {
+            const u32 li = mbi >> 5, sh = mbi & 31u;
+            const u32 lo = a << sh, hi = sh ? (a >> (32u - sh)) : 0u;
+            if (li == 0) {
+              n0 |= lo;
+              n1 |= hi;
+            } else if (li == 1) {
+              n1 |= lo;
+              n2 |= hi;
+            } else {
+              n2 |= lo;
+            }
+          }
+          // v = number + a * 3^f  (cu:262-278)
+          u64 t = (u64)a * R[7] + R[3];
+          v0 = (u32)t;
+          t = (u64)a * R[8] + R[4] + (t >> 32);
+          v1 = (u32)t;
+          t = (u64)a * R[9] + R[5] + (t >> 32);
+          v2 = (u32)t;
+          v3 = a * R[10] + R[6] + (u32)(t >> 32);
+          cpu = R[11];
+          st = mbi;
+          iters = 0;
+          found = 0;
+          ovf = 0;
+          evalid = 0;
+          if (n2 == 0 && n1 == 0 && n0 < 3u) {
+            // v < n can never hold: the reference would loop forever
+            atomicOr(&A.rec->errors, ERR_SEED_SMALL);
+          } else {
+            active = true;
+            // E candidate T^(N-A)(n) = v - 1
+            const u32 x0 = v0 - 1, x1 = v1 - (v0 == 0), x2 = v2 - ((v0 | v1) == 0), x3 = v3 - ((v0 | v1 | v2) == 0);
+            const bool ge = !lt96(x1, x2, x3, W.thr[1], W.thr[2], W.thr[3]) &&
+                            !((x3 == W.thr[3]) & (x2 == W.thr[2]) & (x1 == W.thr[1]) & (x0 < W.thr[0]));
+            if (ge) {
+              W.lane[lane][4] = x0;
+              W.lane[lane][5] = x1;
+              W.lane[lane][6] = x2;
+              W.lane[lane][7] = x3;
+              evalid = 1;
+            }
+          }
+        }
+      }
+      qhead = (qhead + take) & (CQ - 1);
+      qcount -= take;
+      if (take == 0 && exhausted && nidle == 32u) break;
+    }
+
+    // ---- Step 3 (cu:280-405) ----
+    if (active) {
+      const u64 thr_top = ((u64)thr3 << 32) | thr2;
+#pragma unroll 1
+      for (int it = 0; it < ITERS; it++) {
+#pragma unroll
+        for (int half = 0; half < 2; half++) {
+          // odd run
+          const u32 a = ctz32(v0 | (1u << 8));
+          odd_run4(v0, v1, v2, v3, a, s_pow3[a]);
+          if (!found) st += a;
+          if (v3 >= 16u) {  // v >= 2^100 (cu:295, 334); search3 tests > on the second (cu:702)
+            const bool o = !(half == 1 && cpu && v3 == 16u && (v0 | v1 | v2) == 0u);
+            if (o) {
+              const ull i = atomicAdd(A.overflow_count, 1ull);
+              if (i < A.overflow_cap) {
+                A.overflow[4 * i + 0] = n0;
+                A.overflow[4 * i + 1] = n1;
+                A.overflow[4 * i + 2] = n2;
+                A.overflow[4 * i + 3] = 0;
+              }
+              ovf = 1;
+              v0 = 2;
+              v1 = v2 = v3 = 0;
+            }
+          }
+          if (!found && !ovf && (((u64)v3 << 32) | v2) >= thr_top) {
+            // rare: exact excursion candidate x = v - 1 against the seed max / threshold
+            const u32 x0 = v0 - 1, x1 = v1 - (v0 == 0), x2 = v2 - ((v0 | v1) == 0), x3 = v3 - ((v0 | v1 | v2) == 0);
+            const u32* ref = evalid ? &W.lane[lane][4] : W.thr;
+            const bool ge = !lt96(x1, x2, x3, ref[1], ref[2], ref[3]) &&
+                            !((x3 == ref[3]) & (x2 == ref[2]) & (x1 == ref[1]) & (x0 < ref[0]));
+            if (ge) {
+              W.lane[lane][4] = x0;
+              W.lane[lane][5] = x1;
+              W.lane[lane][6] = x2;
+              W.lane[lane][7] = x3;
+              evalid = 1;
+            }
+          }
+          // even run
+          v0 -= 1;
+          const u32 b = ctz32(v0 | 0x80000000u);
+          const u32 w0 = __funnelshift_r(v0, v1, b), w1 = __funnelshift_r(v1, v2, b);
+          const u32 w2 = __funnelshift_r(v2, v3, b), w3 = v3 >> b;
+          if (!found && !ovf) {
+            if (b != 0 && w3 == 0 && w2 <= n2 && lt96(w0, w1, w2, n0, n1, n2)) {
+              // first descent inside this run: smallest i with (v-1) >> i < n
+              u32 i = 1;
+              for (; i < b; i++) {
+                const u32 y0 = __funnelshift_r(v0, v1, i), y1 = __funnelshift_r(v1, v2, i);
+                const u32 y2 = __funnelshift_r(v2, v3, i), y3 = v3 >> i;
+                if (y3 == 0 && lt96(y0, y1, y2, n0, n1, n2)) break;
+              }
+              st += i;
+              found = 1;
+            } else {
+              st += b;
+            }
+          }
+          v0 = w0 + 1;
+          v1 = w1;
+          v2 = w2;
+          v3 = w3;
+          if (v0 == 0 && b != 0) {  // carry of the +1 (cu:310-318)
+            v1 += 1;
+            if (v1 == 0) {
+              v2 += 1;
+              if (v2 == 0) v3 += 1;
+            }
+          }
+        }
+        hash ^= v0;  // cu:359
+        iters++;
+        const bool done = (v3 == 0) && lt96(v0, v1, v2, n0, n1, n2);  // cu:362-365
+        if (done || iters >= A.iter_cap) {
+          if (!done) {
+            atomicOr(&A.rec->errors, ERR_ITER_CAP);
+            atomicAdd(&A.rec->failures, 1ull);
+          } else if (!ovf) {
+            W.lane[lane][1] = n0;
+            W.lane[lane][2] = n1;
+            W.lane[lane][3] = n2;
+            if (st >= thr_st) {
+              W.lane[lane][0] = st;
+              pend |= 1u;
+            }
+            if (evalid) pend |= 2u;
+          }
+          active = false;
+          break;
+        }
+      }
+    }
+  }
+
+  // ---- warp totals ----
+#pragma unroll
+  for (u32 d = 16; d; d >>= 1) hash ^= __shfl_xor_sync(FULL, hash, d);
+  if (lane == 0) {
+    atomicXor(&A.rec->hash, hash);
+    atomicAdd(&A.rec->seeds, warp_seeds);
+  }
+}
+
+// ------------------------------------------------------------------
+// Host launcher.
+// ------------------------------------------------------------------
+
+template <int I, int R>
+static cudaError_t launch_cases_t(const CasesArgs& a, u32 grid, cudaStream_t st) {
+  k_cases<I, R><<<grid, CWARPS * 32, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+int cases_variants() { return 4; }
+
+cudaError_t launch_cases(const CasesArgs& a, int variant, u32 grid, cudaStream_t st) {
+  switch (variant) {
+    case 0: return launch_cases_t<1, 1>(a, grid, st);
+    case 1: return launch_cases_t<2, 4>(a, grid, st);
+    case 2: return launch_cases_t<2, 8>(a, grid, st);
+    default: return launch_cases_t<4, 8>(a, grid, st);
+  }
+}
+
+cudaError_t cases_occupancy(int variant, int* blocks_per_sm) {
+  switch (variant) {
+    case 0: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_cases<1, 1>, CWARPS * 32, 0);
+    case 1: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_cases<2, 4>, CWARPS * 32, 0);
+    case 2: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_cases<2, 8>, CWARPS * 32, 0);
+    default: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_cases<4, 8>, CWARPS * 32, 0);
+  }
+}
+
+}  // namespace cz

@@ -1,0 +1,96 @@
+// kernels.h -- argument blocks and launchers of the hot-path kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "rec.h"
+#include "tables.h"
+
+namespace cz {
+
+// ---------------- cases mode (cases.cu) ----------------
+struct CasesArgs {
+  const uint32_t* pairs;   // npairs x 8 words: base limbs 0..3, number limbs 0..3 (cu:521-528)
+  uint32_t npairs;
+  int bigindex;            // >= 0: bucket of every pair; < 0: per pair in base limb 3
+  const uint32_t* bv;      // CaseTables
+  const uint32_t* mod9;
+  const uint32_t* magic;
+  const uint32_t* pow3;
+  uint32_t mbi, tpo;
+  uint32_t* pair_counter;  // scratch, zero before launch
+  ReqRec* rec;
+  uint32_t* overflow;      // overflow seeds, 4 words each
+  uint32_t overflow_cap;
+  unsigned long long* overflow_count;
+  uint32_t iter_cap;       // checkpoints per seed before ERR_ITER_CAP
+};
+int cases_variants();
+cudaError_t launch_cases(const CasesArgs& a, int variant, uint32_t grid, cudaStream_t st);
+cudaError_t cases_occupancy(int variant, int* blocks_per_sm);
+
+// ---------------- range mode (range.cu) ----------------
+constexpr uint32_t RANGE_ITEM = 256;    // survivor-table entries per work item
+constexpr uint32_t DENSE_ITEM = 1024;   // consecutive integers per dense work item
+
+// A run of work items of one request.  kind 0: survivor entries
+// [s_lo, s_hi) of blocks q .. q+nq-1 (seeds n = q 2^k + r);
+// kind 1: integers [d_lo, d_hi) iterated without the residue sieve.
+struct RangeSeg {
+  unsigned long long item_begin;  // global index of the first item
+  unsigned long long q_lo;        // kind 0: first block, low 64 bits; kind 1: d_lo
+  unsigned long long d_hi;        // kind 1: end (exclusive)
+  uint32_t q_hi;                  // kind 0: first block, bits 64..95
+  uint32_t nq;                    // kind 0: number of blocks
+  uint32_t s_lo, s_hi;            // kind 0: survivor index range
+  uint32_t ipq;                   // kind 0: items per block
+  uint32_t req;                   // request index (ReqRec)
+  uint32_t kind;
+  uint32_t mod9;                  // 1: apply the mod-9 sieve
+};
+static_assert(sizeof(RangeSeg) == 56, "RangeSeg");
+
+struct WidenEntry {  // a seed to re-run with wider limbs
+  uint32_t req, n0, n1, n2;
+};
+
+struct RangeArgs {
+  const RangeEntry* table;        // survivor table of the 2^k sieve
+  uint32_t k;
+  const RangeSeg* segs;
+  uint32_t nsegs;
+  unsigned long long* item_cursor;  // scratch: next item to claim
+  unsigned long long item_limit;    // items >= limit are not claimed in this launch
+  ReqRec* recs;
+  WidenEntry* widen;
+  uint32_t widen_cap;
+  uint32_t* widen_count;
+  uint32_t iter_cap;              // odd/even run pairs per seed before ERR_ITER_CAP
+};
+int range_variants();
+cudaError_t launch_range(const RangeArgs& a, int variant, uint32_t grid, cudaStream_t st);
+cudaError_t range_occupancy(int variant, int* blocks_per_sm);
+// Seeds of a widen list re-run from scratch with 6 (then 8) limbs; the
+// list length is read on the device (*count, at most cap), so the pass can
+// sit in a captured graph right behind the range kernel.
+cudaError_t launch_range_wide(const WidenEntry* list, const uint32_t* count, uint32_t cap, int limbs,
+                              ReqRec* recs, WidenEntry* next, uint32_t next_cap, uint32_t* next_count,
+                              uint32_t iter_cap, cudaStream_t st);
+
+// ---------------- trajectory queries (traj.cu) ----------------
+struct TrajArgs {
+  const uint32_t* seeds;       // nseeds x 8 limbs
+  uint32_t nseeds;
+  const uint32_t* index;       // optional: seeds to process (nullptr = all)
+  uint32_t nindex;
+  unsigned long long* st;      // out: stopping time
+  uint32_t* exc;               // out: 16 limbs each
+  uint32_t* status;            // out: 0 ok, 1 trivial, 2 overflow, 3 iteration cap
+  uint32_t* next;              // seeds that need more limbs
+  uint32_t* next_count;
+  uint32_t* cursor;            // scratch
+  uint32_t iter_cap;
+};
+cudaError_t launch_traj(const TrajArgs& a, int limbs, uint32_t grid, cudaStream_t st);
+
+}  // namespace cz

@@ -1,0 +1,100 @@
+// runtime.h -- host runtime shared by api.cu and server.cpp.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/collatz.h"
+#include "kernels.h"
+#include "rec.h"
+#include "step1.h"
+#include "tables.h"
+
+namespace cz {
+
+// Device buffer that only grows.
+struct DevBuf {
+  void* p = nullptr;
+  size_t n = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= n) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e == cudaSuccess) n = bytes;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  template <class T>
+  T* as() const {
+    return reinterpret_cast<T*>(p);
+  }
+};
+
+// Pinned host buffer that only grows.
+struct HostBuf {
+  void* p = nullptr;
+  size_t n = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= n) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    n = 0;
+    cudaError_t e = cudaMallocHost(&p, bytes);
+    if (e == cudaSuccess) n = bytes;
+    return e;
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    n = 0;
+  }
+  template <class T>
+  T* as() const {
+    return reinterpret_cast<T*>(p);
+  }
+};
+
+constexpr uint32_t WIDEN_CAP = 1u << 16;
+constexpr uint32_t OVERFLOW_CAP = 1u << 16;
+constexpr uint32_t CASE_BATCH = 1u << 20;  // pairs per device batch in run_case
+
+struct RangeTables {
+  RangeTable dev;
+  std::vector<uint64_t> residues;  // host copy for k <= 28 (partial-block bounds)
+};
+
+}  // namespace cz
+
+struct collatz_ctx {
+  collatz_config cfg;
+  int device = 0, sm_count = 0, sm_clock_khz = 0;
+  cudaStream_t own_stream = nullptr, stream = nullptr, copy_stream = nullptr;
+  cz::CaseTables ct;
+  std::map<uint32_t, cz::RangeTables> rt;
+  int cases_variant = 1, range_variant = 2;
+  uint32_t iter_cap = 1u << 16;
+  // scratch for the synchronous calls
+  cz::DevBuf d_rec, d_counter, d_overflow, d_ovcount, d_pairs[2], d_segs, d_widen, d_widen2, d_wcount;
+  cz::HostBuf h_rec, h_pairs;
+  cz::DevBuf t_seeds, t_st, t_exc, t_status, t_idx[2], t_cnt;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  std::recursive_mutex mu;
+  std::string err;
+};
+
+namespace cz {
+int set_cuda_error(collatz_ctx* c, cudaError_t e, const char* where);
+int get_range_tables(collatz_ctx* c, uint32_t k, RangeTables** out);
+int lower_range(collatz_ctx* c, const collatz_range& r, uint32_t req, const RangeTables& T,
+                std::vector<RangeSeg>& segs, unsigned long long& items);
+void rec_to_range_result(const ReqRec& r, collatz_range_result* out);
+}  // namespace cz

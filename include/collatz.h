@@ -1,0 +1,193 @@
+/*
+ * collatz.h -- C ABI of collatz_b200, a B200-native (sm_100a) Collatz
+ * convergence verifier with the inputs and outputs of the reference
+ * program collatz_cudav7.cu (vigleik0/collatz).
+ *
+ * Conventions: every entry point returns an int status (COLLATZ_OK = 0,
+ * negative on error) and never throws.  The caller owns every host buffer;
+ * the library owns its device memory (sieve tables, scratch).  Numbers
+ * wider than 64 bits are little-endian arrays of uint64_t (u128 fields) or
+ * uint32_t limbs.  A context is used by one host thread at a time (calls
+ * on one context are serialised internally); the server object is the
+ * thread-safe front end.
+ *
+ * Definitions (T is the reference's shortcut map, main.rs:13):
+ *   T(n) = (3n+1)/2 for odd n, n/2 for even n.
+ *   stopping time  sigma(n) = least k >= 1 with T^k(n) < n.
+ *   excursion      E(n) = max over 0 <= k <= sigma(n) of T^k(n).
+ * In cases mode Step 1 carries no per-seed history, so E is the maximum
+ * over N-A <= k <= sigma(n); sigma still counts from n.  Ties in either
+ * maximum go to the smaller seed.
+ */
+#ifndef COLLATZ_B200_H
+#define COLLATZ_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define COLLATZ_ABI_VERSION 1
+
+enum collatz_status_code {
+  COLLATZ_OK = 0,
+  COLLATZ_E_ARG = -1,       /* invalid argument */
+  COLLATZ_E_CUDA = -2,      /* CUDA runtime error (see collatz_last_error) */
+  COLLATZ_E_NOMEM = -3,     /* host or device allocation failed */
+  COLLATZ_E_LIMIT = -4,     /* request beyond a documented size limit */
+  COLLATZ_E_DEVICE = -5,    /* a kernel reported an error bit (see result.errors) */
+  COLLATZ_E_TIMEOUT = -6,   /* poll timed out */
+  COLLATZ_E_STATE = -7,     /* object in the wrong state (e.g. server stopped) */
+  COLLATZ_E_ADMISSION = -8, /* request refused: not enough free device memory */
+  COLLATZ_E_NODEV = -9      /* no CUDA device / the kernels are not loadable */
+};
+
+/* device error bits reported in result.errors */
+#define COLLATZ_ERR_LOCK 0x1u        /* a result lock spin hit its limit */
+#define COLLATZ_ERR_ITER_CAP 0x2u    /* a seed exceeded the per-seed iteration cap */
+#define COLLATZ_ERR_WIDEN_FULL 0x4u  /* widening list full */
+#define COLLATZ_ERR_SEED_SMALL 0x8u  /* cases mode: a seed < 3 (never descends) */
+
+typedef struct collatz_ctx collatz_ctx;
+
+typedef struct {
+  uint32_t maxbits;     /* N = MAXBITS (collatz_cudav7.cu:43); 16..96; default 45 */
+  uint32_t range_k;     /* default residue-sieve exponent of range requests; default 24 */
+  int32_t device;       /* CUDA device ordinal; default 0 */
+  uint32_t variant;     /* kernel variant, COLLATZ_VARIANT_AUTO = tuned default */
+  uint32_t iter_cap;    /* per-seed loop cap in checkpoints / run pairs (0 = default 1<<16) */
+  uint32_t reserved[11];
+} collatz_config;
+#define COLLATZ_VARIANT_AUTO 0xFFFFFFFFu
+
+void collatz_config_default(collatz_config *cfg);
+/* Builds the reference's sieve tables for cfg->maxbits on the device
+ * (replaces precompute, cu:423-495, and the uploads of cu:133-171). */
+int collatz_create(const collatz_config *cfg, collatz_ctx **out);
+void collatz_destroy(collatz_ctx *ctx);
+const char *collatz_status_string(int status);
+const char *collatz_last_error(const collatz_ctx *ctx);
+/* Work is issued on this CUDA stream (cudaStream_t; NULL = the library's
+ * own stream). */
+int collatz_set_stream(collatz_ctx *ctx, void *cuda_stream);
+int collatz_device_info(const collatz_ctx *ctx, int *sm_count, int *sm_clock_khz);
+
+/* ------------------------------------------------------------------ */
+/* Cases mode: the reference's verification run (Algorithm 1).         */
+/* ------------------------------------------------------------------ */
+
+/* One stdin line of the reference: "base sigfig threepower number
+ * doubleeven numevens" (cu:96-101, 174), the format of cases_*. */
+typedef struct {
+  uint64_t base[2];
+  uint32_t sigfig;
+  uint32_t threepower;
+  uint64_t number[2];
+  uint32_t doubleeven;
+  uint32_t numevens;
+} collatz_case;
+
+typedef struct {
+  uint32_t hash;            /* "Complete hash" (cu:182) */
+  uint32_t spot_checks;     /* always 0: the product never recomputes on the CPU */
+  uint64_t launches;        /* the reference's "Number of kernel launches" (cu:181) */
+  uint64_t seeds_checked;   /* surviving seeds iterated */
+  uint64_t pairs;           /* Step-1 leaves with bigindex < 16 */
+  uint64_t cpu_pairs;       /* Step-1 leaves with bigindex >= 16 (cu:517-519), run on the GPU */
+  uint64_t n_overflow;      /* seeds whose value reached 2^100 (the reference prints them) */
+  uint32_t *overflow_seeds; /* caller buffer: 4 uint32_t limbs per seed, sorted ascending; may be NULL */
+  uint64_t overflow_cap;    /* capacity of overflow_seeds, in seeds */
+  uint32_t max_excursion[4];
+  uint32_t max_excursion_seed[4];
+  uint64_t max_stopping_time;
+  uint32_t max_stopping_time_seed[4];
+  uint32_t errors;          /* COLLATZ_ERR_* bits */
+  uint32_t reserved;
+  double device_ms;         /* device time of the Step 2/3 kernels */
+} collatz_case_result;
+
+/* Whole run from one 6-tuple (replaces main, cu:95-183): host Step 1
+ * (search1, cu:497-563) on all host threads feeding the GPU. */
+int collatz_run_case(collatz_ctx *ctx, const collatz_case *c, collatz_case_result *out);
+
+/* One batch of Step-1 pairs of one bucket (replaces launchkernel,
+ * cu:565-649, and compute_kernel, cu:185-411).  pairs: npairs x 8 uint32
+ * (base limbs 0..3, number limbs 0..3; base limb 3 is ignored as in
+ * cu:201).  bigindex = threepower - THREEPOWEROFFSET; bigindex >= 16 runs
+ * search2/search3 semantics (cu:654-715).  The result accumulates nothing
+ * across calls. */
+int collatz_verify_pairs(collatz_ctx *ctx, uint32_t bigindex, const uint32_t *pairs, uint32_t npairs,
+                         collatz_case_result *out);
+
+/* Step-1 leaves of a case (search1, cu:497-563) for N = maxbits, in the
+ * reference's order, without Steps 2-3: each pair as 8 uint32 with base
+ * limb 3 = bigindex.  *count receives the number of leaves (pairs are
+ * written up to cap).  Host-only: needs no device. */
+int collatz_step1_pairs(uint32_t maxbits, const collatz_case *c, uint32_t *pairs, uint64_t cap,
+                        uint64_t *count);
+
+/* Copies the device-built tables back: bv = 16 x (2^19 + 32) uint32 (the
+ * reference's flat d_flat, cu:138-152), mod9 = 9 x 32 uint32 (cu:159-171). */
+int collatz_case_tables(collatz_ctx *ctx, uint32_t *bv, uint32_t *mod9);
+
+/* ------------------------------------------------------------------ */
+/* Range mode and trajectory queries (new entry modes).                */
+/* ------------------------------------------------------------------ */
+
+/* Seeds n in [offset, offset + size) with n >= 2 and, with the sieves on,
+ * n mod 9 in {0,1,3,6,7} and (for n >= 2^k) n mod 2^k a survivor of the
+ * k-step descent sieve.  offset + size <= 2^96, size <= 2^48, k in 8..34. */
+typedef struct {
+  uint64_t offset[2];
+  uint64_t size;
+  uint32_t k;      /* 0 = the context's range_k */
+  uint32_t flags;  /* COLLATZ_RANGE_NO_MOD9 */
+} collatz_range;
+#define COLLATZ_RANGE_NO_MOD9 0x1u
+
+typedef struct {
+  uint64_t seeds_checked;
+  uint64_t failures;         /* seeds that did not finish within 256-bit values or the iteration cap */
+  uint64_t widened;          /* seeds re-run with 192/256-bit values */
+  uint32_t max_excursion[8]; /* 256-bit */
+  uint32_t max_excursion_seed[4];
+  uint64_t max_stopping_time;
+  uint32_t max_stopping_time_seed[4];
+  uint32_t errors;           /* COLLATZ_ERR_* bits */
+  int32_t status;
+  double device_ms;
+} collatz_range_result;
+
+int collatz_verify_range(collatz_ctx *ctx, const collatz_range *r, collatz_range_result *out);
+/* Many requests in one persistent launch (device work queue). */
+int collatz_verify_batch(collatz_ctx *ctx, const collatz_range *r, uint32_t n, collatz_range_result *out);
+
+/* Device-resident form for timing: a plan holds the lowered work list on
+ * the device and a captured CUDA graph (reset, kernel, widening passes). */
+typedef struct collatz_plan collatz_plan;
+int collatz_plan_create(collatz_ctx *ctx, const collatz_range *r, uint32_t n, collatz_plan **out);
+int collatz_plan_launch(collatz_plan *p);   /* enqueue on the context stream, no sync */
+int collatz_plan_results(collatz_plan *p, collatz_range_result *out); /* sync + copy back */
+void collatz_plan_destroy(collatz_plan *p);
+
+/* Copies the range-mode residue sieve for k back: bits (2^k / 8 bytes,
+ * bit r set iff r mod 2^k survives) and the survivor count. */
+int collatz_range_sieve(collatz_ctx *ctx, uint32_t k, uint8_t *bits, uint64_t *count);
+
+/* Per-seed stopping time and excursion.  seeds: n x 8 uint32 limbs
+ * (seeds < 2^256).  stopping_time[i]; excursion: 16 limbs (512 bits) per
+ * seed; status[i]: 0 ok, 1 seed < 2 (no stopping time), 2 value left 512
+ * bits, 3 iteration cap. */
+int collatz_trajectory(collatz_ctx *ctx, const uint32_t *seeds, uint32_t n, uint64_t *stopping_time,
+                       uint32_t *excursion, uint32_t *status);
+
+/* Kernel variants for the autotuner. */
+int collatz_variant_count(int mode); /* mode 0 cases, 1 range */
+int collatz_set_variant(collatz_ctx *ctx, int mode, int variant);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* COLLATZ_B200_H */

@@ -1,0 +1,101 @@
+"""Range mode and batches on the GPU against the oracle (oracle/collatz_oracle.c:
+orc_range, the reference's run-length loop of search3, cu:684-715, with exact
+stopping time and excursion)."""
+import os
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+NT = max(1, min(32, os.cpu_count() or 1))
+
+CASES = [
+    # (offset, size, k, mod9)
+    (1 << 40, 1 << 22, 16, True),
+    (1 << 40, 1 << 22, 24, True),
+    ((1 << 60) + (5 << 24), 1 << 21, 24, True),
+    ((1 << 40) + 12345, 300001, 20, True),      # unaligned both ends, within one block
+    ((1 << 40) - 77777, 3 << 20, 20, True),     # unaligned, spans blocks
+    (0, 1 << 20, 16, True),                     # seeds below 2^k: unsieved (dense) region
+    (1000, 5000, 12, False),                    # no mod-9 sieve
+    ((1 << 64) - (1 << 20), 1 << 21, 24, True),  # crosses 2^64
+    ((1 << 90) + 3, 1 << 17, 16, True),         # 91-bit seeds
+]
+
+
+def _cmp(g, o):
+    assert g.errors == 0 and g.failures == 0
+    assert g.seeds_checked == o.seeds
+    assert (g.max_stopping_time, g.max_stopping_time_seed) == (o.max_st, o.max_st_seed)
+    assert (g.max_excursion, g.max_excursion_seed) == (o.max_exc, o.max_exc_seed)
+
+
+@pytest.mark.parametrize("k", [8, 12, 16, 20, 24])
+def test_range_sieve_matches_oracle(verifier, k):
+    from oracle import oracle as O
+    n, bits = verifier(26).range_sieve(k)
+    on, obits = O.range_sieve(k)
+    assert n == on
+    assert bits == obits
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: f"o{c[0]:x}-s{c[1]}-k{c[2]}-m{int(c[3])}")
+def test_range_matches_oracle(verifier, case):
+    from oracle import oracle as O
+    off, size, k, mod9 = case
+    g = verifier(26).verify_range(off, size, k, mod9)
+    o = O.range_verify(off, size, k, mod9, method=1, nthreads=NT)
+    _cmp(g, o)
+
+
+def test_batch_equals_alone(verifier):
+    """Each request's result is the same alone and in a mixed batch."""
+    v = verifier(26)
+    reqs = [((1 << 40) + i * (1 << 24) + 9 * i, (1 << 18) + 1000 * i, 24, True) for i in range(12)]
+    reqs.append((1 << 50, 1 << 23, 24, True))
+    reqs.append((17, 40000, 24, True))
+    mixed = v.verify_batch(reqs)
+    for q, m in zip(reqs, mixed):
+        assert _key(v.verify_range(*q)) == _key(m)
+
+
+def _key(r):
+    return (r.seeds_checked, r.failures, r.max_stopping_time, r.max_stopping_time_seed, r.max_excursion,
+            r.max_excursion_seed, r.errors)
+
+
+def test_plan_relaunch_is_deterministic(verifier):
+    v = verifier(26)
+    p = v.plan([(1 << 44, 1 << 24, 24, True), ((1 << 52) + 1, 1 << 22, 24, True)])
+    p.launch()
+    a = p.results()
+    p.launch()
+    b = p.results()
+    for x, y in zip(a, b):
+        assert (x.seeds_checked, x.max_excursion, x.max_excursion_seed, x.max_stopping_time,
+                x.max_stopping_time_seed) == (y.seeds_checked, y.max_excursion, y.max_excursion_seed,
+                                              y.max_stopping_time, y.max_stopping_time_seed)
+    p.close()
+
+
+def test_shards_combine(verifier):
+    """Disjoint shards (the multi-GPU split) combine to the whole range."""
+    import collatz_b200 as cb
+    v = verifier(26)
+    off, size = (1 << 41) + 3, 5 << 22
+    whole = v.verify_range(off, size, 24)
+    parts = [v.verify_range(off + i * (size // 4), size // 4, 24) for i in range(4)]
+    c = cb.combine_range_results(parts)
+    assert (c.seeds_checked, c.max_excursion, c.max_excursion_seed, c.max_stopping_time,
+            c.max_stopping_time_seed) == (whole.seeds_checked, whole.max_excursion,
+                                          whole.max_excursion_seed, whole.max_stopping_time,
+                                          whole.max_stopping_time_seed)
+
+
+def test_limits_rejected(verifier):
+    import collatz_b200 as cb
+    v = verifier(26)
+    with pytest.raises(cb.CollatzError):
+        v.verify_range((1 << 96) - 10, 100, 24)
+    with pytest.raises(cb.CollatzError):
+        v.verify_range(1 << 40, 1 << 49, 24)

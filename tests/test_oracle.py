@@ -1,0 +1,158 @@
+"""The CPU oracle pinned against the reference's own outputs (golden fixtures
+from collatz_cudav7.cu built through the CPU shim) and against brute force."""
+import hashlib
+import random
+
+import pytest
+
+from conftest import load_golden
+
+RUNS = load_golden("cases_runs.json")["runs"]
+TABLES = load_golden("tables.json")["tables"]
+
+
+def T_step(n):
+    return (3 * n + 1) // 2 if n & 1 else n // 2
+
+
+def brute(n):
+    """(stopping time, excursion) by single steps."""
+    x, E, k = n, n, 0
+    while True:
+        x = T_step(x)
+        k += 1
+        E = max(E, x)
+        if x < n:
+            return k, E
+
+
+@pytest.mark.parametrize("t", [t for t in TABLES if t["N"] in (26, 45)], ids=lambda t: f"N{t['N']}")
+def test_oracle_tables_match_reference(oracle_tables, t):
+    T = oracle_tables(t["N"])
+    assert hashlib.sha256(T.bv_bytes()).hexdigest() == t["bv_sha256"]
+    assert hashlib.sha256(T.mod9_bytes()).hexdigest() == t["mod9_sha256"]
+
+
+@pytest.mark.parametrize("n", [26, 45])
+def test_oracle_pairs_match_reference(oracle_tables, n):
+    fx = load_golden(f"pairs_N{n}.json")
+    T = oracle_tables(n)
+    for b in fx["batches"]:
+        pairs = [(int(x), int(y)) for x, y in b["pairs"]]
+        o = T.pairs_result(b["bigindex"], pairs)
+        assert f"{o.hash:X}" == b["hash"]
+        assert o.seeds == b["seeds"]
+        assert sorted(o.overflow) == sorted(int(x) for x in b["overflow"])
+    for d in fx["search2"]:
+        o = T.pairs_result(d["bigindex"], [(int(d["base"]), int(d["number"]))], cpu_sem=True)
+        assert f"{o.hash:X}" == d["hash"]
+
+
+@pytest.mark.parametrize("run", [r for r in RUNS if r["N"] <= 30 or (r["N"] == 36 and r["tuple"][1] >= 10)
+                                 or r["tuple"][1] >= 20],
+                         ids=lambda r: f"N{r['N']}-" + "_".join(map(str, r["tuple"])))
+def test_oracle_runs_match_reference(oracle_tables, run):
+    o = oracle_tables(run["N"]).run_case(*run["tuple"])
+    assert f"{o.hash:X}" == run["hash"]
+    assert o.launches == run["launches"]
+    assert o.seeds == run["seeds"]
+    assert sorted(o.overflow) == sorted(int(x) for x in run["overflow"])
+
+
+def test_oracle_case_maxima_brute(oracle_tables):
+    """sigma counts from n; E is the maximum over k >= N - A (Step 1 carries
+    no history) -- equal to the brute-force maximum whenever the peak comes
+    after step N - A."""
+    o = oracle_tables(26).run_case(3, 2, 2, 9, 1, 0)
+    st, _ = brute(o.max_st_seed)
+    assert st == o.max_st
+    n = o.max_exc_seed
+    x, E = n, 0
+    for k in range(1, brute(n)[0] + 1):
+        x = T_step(x)
+        if k >= 16:
+            E = max(E, x)
+    assert E == o.max_exc
+
+
+def test_step1_leaves_match_product(oracle_tables):
+    """The product's host Step 1 (collatz_step1_pairs) visits the same leaves
+    in the same order as the oracle's restatement of search1."""
+    import collatz_b200 as cb
+    from oracle import oracle as O
+    for n, tup in ((26, (3, 2, 2, 9, 1, 0)), (36, (27, 10, 8, 183, 0, 0)), (45, (27, 25, 18, 335, 0, 1))):
+        assert cb.step1_pairs(n, *tup) == O.leaves(n, tup)
+
+
+@pytest.mark.parametrize("k", [8, 10, 12, 14, 16, 18, 20])
+def test_range_sieve_valid_from_2k(k):
+    """Every removed residue r descends within its tau steps from 2^k + r,
+    hence (T^tau affine with slope < 1 on the class) for every n >= 2^k."""
+    from oracle import oracle as O
+    assert O.range_sieve_validate(k) == 0
+
+
+def test_range_sieve_bruteforce():
+    from oracle import oracle as O
+    k = 12
+    n, bits = O.range_sieve(k)
+    cnt = 0
+    for r in range(1 << k):
+        x, f, ok = r, 0, True
+        for j in range(1, k + 1):
+            if x & 1:
+                f += 1
+            x = T_step(x)
+            if 3 ** f < 2 ** j:
+                ok = False
+                break
+        assert ok == bool((bits[r >> 3] >> (r & 7)) & 1)
+        cnt += ok
+    assert cnt == n
+
+
+@pytest.mark.parametrize("case", [((1 << 20) + 7, 3000, 12), (2, 4000, 16), ((1 << 33) + 11, 5000, 16)])
+def test_range_oracle_bruteforce(case):
+    from oracle import oracle as O
+    off, size, k = case
+    o = O.range_verify(off, size, k, True, method=0)
+    _, bits = O.range_sieve(k)
+    best_st, best_e, seeds = (-1, 0), (-1, 0), 0
+    for n in range(off, off + size):
+        if n < 2 or n % 9 not in (0, 1, 3, 6, 7):
+            continue
+        if n >= (1 << k):
+            r = n % (1 << k)
+            if not (bits[r >> 3] >> (r & 7)) & 1:
+                continue
+        seeds += 1
+        st, E = brute(n)
+        best_st = max(best_st, (st, -n))
+        best_e = max(best_e, (E, -n))
+    assert o.seeds == seeds
+    assert (o.max_st, o.max_st_seed) == (best_st[0], -best_st[1])
+    assert (o.max_exc, o.max_exc_seed) == (best_e[0], -best_e[1])
+
+
+@pytest.mark.parametrize("case", [(1 << 40, 1 << 20, 24), ((1 << 60) + 3, 1 << 18, 16), (0, 1 << 16, 12),
+                                  ((1 << 90) + 5, 1 << 14, 16)])
+def test_range_methods_agree(case):
+    """Single steps, the reference's run-length loop and the GPU's jump +
+    runs structure give identical results."""
+    from oracle import oracle as O
+    off, size, k = case
+    rs = [O.range_verify(off, size, k, True, method=m, nthreads=4) for m in (0, 1, 2)]
+    keys = [(r.seeds, r.max_st, r.max_st_seed, r.max_exc, r.max_exc_seed) for r in rs]
+    assert keys[0] == keys[1] == keys[2]
+
+
+def test_trajectory_bruteforce():
+    from oracle import oracle as O
+    rng = random.Random(3)
+    seeds = [0, 1, 2, 3, 27, 97] + [rng.getrandbits(rng.randint(2, 80)) for _ in range(300)]
+    out = O.trajectory(seeds)
+    for s, (status, st, E) in zip(seeds, out):
+        if s < 2:
+            assert (status, st, E) == (1, 0, s)
+        else:
+            assert (status, st, E) == (0, *brute(s))
