@@ -7,6 +7,8 @@
 #include <cstring>
 #include <deque>
 #include <thread>
+#include <cstdio>
+#include <cstdlib>
 
 #include "runtime.h"
 
@@ -146,8 +148,9 @@ int lower_range(collatz_ctx* c, const collatz_range& r, uint32_t req, const Rang
   auto add = [&](u128 q, u128 nq, uint32_t s_lo, uint32_t s_hi) {
     if (s_lo >= s_hi || nq == 0) return;
     const uint32_t ipq = (s_hi - s_lo + RANGE_ITEM - 1) / RANGE_ITEM;
+    const u128 max_nq = std::max<uint32_t>(1u, 0xFFFFFFFFu / ipq);  // < 2^32 items per segment
     while (nq > 0) {
-      const uint32_t take = (uint32_t)std::min(nq, (u128)0x7FFFFFFF);
+      const uint32_t take = (uint32_t)std::min(nq, max_nq);
       RangeSeg g{};
       g.item_begin = items;
       g.q_lo = (uint64_t)q;
@@ -243,6 +246,7 @@ extern "C" int collatz_create(const collatz_config* cfg, collatz_ctx** out) {
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);
   for (int i = 0; i < 4 && e == cudaSuccess; i++) e = cudaEventCreate(&c->ev[i]);
+  if (e == cudaSuccess) e = range_init();
   if (e == cudaSuccess) e = build_case_tables(&c->ct, cfg->maxbits, c->own_stream);
   if (e != cudaSuccess) {
     rc = set_cuda_error(c, e, "collatz_create");
@@ -620,8 +624,9 @@ struct collatz_plan {
   RangeTables* T = nullptr;
   std::vector<RangeSeg> segs;
   unsigned long long items = 0;
-  DevBuf d_segs, d_recs, d_cursor, d_widen, d_widen2, d_wcount;
+  DevBuf d_segs, d_recs, d_cursor, d_widen, d_widen2, d_wcount, d_stats;
   HostBuf h_recs;
+  bool stats = false;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   float last_ms = 0;
@@ -665,13 +670,21 @@ static int plan_build(collatz_ctx* c, const collatz_range* r, uint32_t n, collat
   a.widen_cap = WIDEN_CAP;
   a.widen_count = p->d_wcount.as<uint32_t>();
   a.iter_cap = c->iter_cap;
+  a.stats = nullptr;
+  const char* dbg = getenv("COLLATZ_RANGE_STATS");
+  p->stats = dbg && dbg[0] == '1';
+  if (p->stats) {
+    CK(c, p->d_stats.ensure(16 * sizeof(unsigned long long)));
+    a.stats = p->d_stats.as<unsigned long long>();
+  }
   const uint32_t grid = (uint32_t)grid_for(c, 1, c->range_variant);
   cudaStream_t s = c->own_stream;
   CK(c, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   cudaError_t e = cudaMemsetAsync(p->d_recs.p, 0, sizeof(ReqRec) * std::max(1u, n), s);
   if (!e) e = cudaMemsetAsync(p->d_cursor.p, 0, sizeof(unsigned long long), s);
   if (!e) e = cudaMemsetAsync(p->d_wcount.p, 0, sizeof(uint32_t) * 2, s);
-  if (!e) e = launch_range(a, c->range_variant, grid, s);
+  if (!e && p->stats) e = cudaMemsetAsync(p->d_stats.p, 0, 16 * sizeof(unsigned long long), s);
+  if (!e) e = p->stats ? launch_range_stats(a, grid, s) : launch_range(a, c->range_variant, grid, s);
   if (!e)
     e = launch_range_wide(p->d_widen.as<WidenEntry>(), p->d_wcount.as<uint32_t>(), WIDEN_CAP, 6, a.recs,
                           p->d_widen2.as<WidenEntry>(), WIDEN_CAP, p->d_wcount.as<uint32_t>() + 1, c->iter_cap, s);
@@ -720,6 +733,16 @@ extern "C" int collatz_plan_results(collatz_plan* p, collatz_range_result* out) 
   cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);
   const ReqRec* h = p->h_recs.as<ReqRec>();
   int status = COLLATZ_OK;
+  if (p->stats) {  // diagnostics (COLLATZ_RANGE_STATS=1)
+    unsigned long long st8[16];
+    CK(c, cudaMemcpy(st8, p->d_stats.p, sizeof st8, cudaMemcpyDeviceToHost));
+    fprintf(stderr,
+            "collatz range stats: run_pairs=%llu slow_e=%llu replays=%llu jumps=%llu pops=%llu expansions=%llu "
+            "passes=%llu offers=%llu warp_cycles: offers=%llu refill=%llu lanes=%llu (refill: wait=%llu "
+            "stage=%llu thresholds=%llu)\n",
+            st8[0], st8[1], st8[2], st8[3], st8[4], st8[5], st8[6], st8[7], st8[8], st8[9], st8[10], st8[11],
+            st8[12], st8[13]);
+  }
   for (uint32_t i = 0; i < p->n; i++) {
     rec_to_range_result(h[i], &out[i]);
     out[i].device_ms = ms;
@@ -738,6 +761,7 @@ extern "C" void collatz_plan_destroy(collatz_plan* p) {
   p->d_widen.release();
   p->d_widen2.release();
   p->d_wcount.release();
+  p->d_stats.release();
   p->h_recs.release();
   delete p;
 }

@@ -30,8 +30,8 @@ cudaError_t launch_cases(const CasesArgs& a, int variant, uint32_t grid, cudaStr
 cudaError_t cases_occupancy(int variant, int* blocks_per_sm);
 
 // ---------------- range mode (range.cu) ----------------
-constexpr uint32_t RANGE_ITEM = 256;    // survivor-table entries per work item
-constexpr uint32_t DENSE_ITEM = 1024;   // consecutive integers per dense work item
+constexpr uint32_t RANGE_ITEM = 64;     // survivor-table entries per work item
+constexpr uint32_t DENSE_ITEM = 64;     // consecutive integers per dense work item
 
 // A run of work items of one request.  kind 0: survivor entries
 // [s_lo, s_hi) of blocks q .. q+nq-1 (seeds n = q 2^k + r);
@@ -66,8 +66,13 @@ struct RangeArgs {
   uint32_t widen_cap;
   uint32_t* widen_count;
   uint32_t iter_cap;              // odd/even run pairs per seed before ERR_ITER_CAP
+  unsigned long long* stats;      // diagnostics counters (stats variant only), may be null
 };
 int range_variants();
+cudaError_t range_init();  // once per device, before the first launch
+// Diagnostics variant: counts run pairs, slow paths, replays, jumps, pops,
+// expansions, pop-block passes and offers into a.stats[0..7].
+cudaError_t launch_range_stats(const RangeArgs& a, uint32_t grid, cudaStream_t st);
 cudaError_t launch_range(const RangeArgs& a, int variant, uint32_t grid, cudaStream_t st);
 cudaError_t range_occupancy(int variant, int* blocks_per_sm);
 // Seeds of a widen list re-run from scratch with 6 (then 8) limbs; the

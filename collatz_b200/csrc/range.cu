@@ -24,30 +24,205 @@
 
 namespace cz {
 
-constexpr u32 RQ = 1024;  // queue entries per warp (>= 31 + survivors of one dense item)
-constexpr u32 RR = 32;    // item slots per warp
-constexpr u32 RWARPS = 8;
-constexpr u32 KEEP9 = 0xCBu;  // n mod 9 in {0,1,3,6,7} survives (cu:488)
+constexpr u32 RQ = 128;          // queue entries per warp, power of two (>= 32 R + one item)
+constexpr u32 RR = 32;           // item slots per warp (< 32 queued entries span < 32 items)
+constexpr u32 RWARPS = 7;
+constexpr u32 CLAIM = 8;         // items claimed per atomic
+constexpr u32 KEEP9 = 0xCBu;     // n mod 9 in {0,1,3,6,7} survives (cu:488)
+constexpr u32 OVF3 = 1u << 23;   // v >= 2^119 after an odd run: the next run could leave 128 bits
+constexpr u32 ST_CAP = 1u << 20; // steps per seed before ERR_ITER_CAP
 
+// The work item staged for expansion (warp-uniform).
+struct StagedItem {
+  ull q_lo;      // kind 0: block q (low 64 bits); kind 1: first integer
+  ull d_hi;      // kind 1: end (exclusive)
+  u32 q_hi;      // kind 0: block q bits 64..95
+  u32 sbase, send;  // kind 0: survivor-table range of the item
+  u32 req, kind, mod9, valid, pad;
+};
+
+// Per-warp state in shared memory.  Queue entries are fully set-up seeds:
+// qa = v = T^s(n) + 1, qb = (n0, n1, n2, meta) with meta [7:0] steps s,
+// [12:8] item slot, [13] v - 1 is an excursion candidate, [23:16] bitlen(n).
 struct RangeWarp {
-  unsigned short q[RQ];  // (slot << 10) | local index
-  u32 ring[RR][12];      // [0] kind [1] s_base [2..4] q / d limbs [5] req [6] thr_st [7] thr bit length [8..11] thrE
-  u32 lane[32][12];      // [0] st [1..3] seed [4..7] seed-local max E [8..11] thrE
+  uint4 qa[RQ];
+  uint4 qb[RQ];
+  uint4 ring[RR];          // per item slot: request, sigma threshold, excursion window (lo, hi)
+  uint4 stage[RANGE_ITEM]; // survivor entries of the staged item (cp.async)
+  u32 e[4][32];            // per lane: seed-local max excursion
+  u32 pe[4][32];           // per lane: excursion of a pending offer
+  u32 c[5][32];            // per lane: pending offer [0] sigma [1..3] seed [4] request
+  u32 bln[32];             // per lane: bit length of the seed
+  RangeSeg seg;            // cached segment
+  StagedItem nxt;
+  ull item, claim_hi, seg_lo, seg_hi, qi, acc_seeds, acc_items;
+  u32 chunk, since_thr, ring_seq, thr_bl, head, pad;
 };
 
 __device__ __forceinline__ u32 mod9_96(u32 a0, u32 a1, u32 a2) {
   return ((a0 % 9u) + 4u * (a1 % 9u) + 7u * (a2 % 9u)) % 9u;
 }
 
-// x >= ref for 4-limb values
-__device__ __forceinline__ bool ge128(u32 x0, u32 x1, u32 x2, u32 x3, const u32* ref) {
-  return !(lt96(x1, x2, x3, ref[1], ref[2], ref[3]) ||
-           ((x3 == ref[3]) & (x2 == ref[2]) & (x1 == ref[1]) & (x0 < ref[0])));
+// Bits 32..95 of a value below 2^128 given as limbs 1..3; all ones when it
+// is >= 2^96.  Comparing this window is a conservative excursion test.
+__device__ __forceinline__ u64 gate_window(u32 x1, u32 x2, u32 x3) {
+  return x3 ? ~0ull : (((u64)x2 << 32) | x1);
 }
 
-template <int ITERS, int REFILL_MIN>
-__global__ void __launch_bounds__(RWARPS * 32) k_range(const RangeArgs A) {
-  __shared__ RangeWarp S[RWARPS];
+__device__ __forceinline__ u32 bitlen128(unsigned __int128 x) {
+  const u64 hi = (u64)(x >> 64), lo = (u64)x;
+  return hi ? 128u - __clzll(hi) : (lo ? 64u - __clzll(lo) : 0u);
+}
+
+// 3^a for a <= 7 from two byte-permute lookups: low bytes 01 03 09 1B 51 F3 D9 8B,
+// high bytes 00 00 00 00 00 00 02 08 (3^6 = 0x2D9, 3^7 = 0x88B).
+__device__ __forceinline__ u32 pow3_le7(u32 a) {
+  return (__byte_perm(0x1B090301u, 0x8BD9F351u, a) & 0xFFu) | __byte_perm(0u, 0x08020000u, a << 4);
+}
+
+// (a2:a1:a0) < (b2:b1:b0) as one borrow chain.
+__device__ __forceinline__ bool lt96c(u32 a0, u32 a1, u32 a2, u32 b0, u32 b1, u32 b2) {
+  u32 r;
+  asm("{\n\t.reg .u32 t;\n\t"
+      "sub.cc.u32 t, %1, %4;\n\t"
+      "subc.cc.u32 t, %2, %5;\n\t"
+      "subc.cc.u32 t, %3, %6;\n\t"
+      "subc.u32 %0, 0, 0;\n\t}"
+      : "=r"(r)
+      : "r"(a0), "r"(a1), "r"(a2), "r"(b0), "r"(b1), "r"(b2));
+  return r != 0;
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Queue a seed for the 192/256-bit re-run.
+__device__ __forceinline__ void widen_seed(const RangeArgs& A, u32 req, u32 n0, u32 n1, u32 n2) {
+  const u32 wi = atomicAdd(A.widen_count, 1u);
+  if (wi < A.widen_cap) {
+    A.widen[wi] = WidenEntry{req, n0, n1, n2};
+    atomicAdd(&A.recs[req].widened, 1ull);
+  } else {
+    atomicOr(&A.recs[req].errors, ERR_WIDEN_FULL);
+    atomicAdd(&A.recs[req].failures, 1ull);
+  }
+}
+
+// Advances to the next work item (claiming CLAIM items at a time), resolves
+// its segment and block, and starts copying its survivor entries into
+// W.stage with cp.async so that they arrive while the current item is
+// expanded.  Warp-uniform; lane 0 owns the bookkeeping.
+__device__ __forceinline__ void stage_next(RangeWarp& W, const RangeArgs& A, const uint4* __restrict__ T, u32 lane) {
+  ull next = W.item + 1;
+  bool fresh = false;
+  if (next >= W.claim_hi) {
+    ull c = 0;
+    if (lane == 0) c = atomicAdd(A.item_cursor, (ull)CLAIM);
+    c = __shfl_sync(FULL, c, 0);
+    if (c >= A.item_limit) {
+      __syncwarp();
+      if (lane == 0) W.nxt.valid = 0;
+      __syncwarp();
+      return;
+    }
+    next = c;
+    fresh = true;
+    __syncwarp();
+    if (lane == 0) W.claim_hi = min(c + CLAIM, A.item_limit);
+  }
+  if (next < W.seg_lo || next >= W.seg_hi) {
+    u32 si = 0;
+    if (lane == 0) {
+      u32 lo = 0, hi = A.nsegs;
+      while (hi - lo > 1) {
+        const u32 mid = (lo + hi) >> 1;
+        if (A.segs[mid].item_begin <= next) lo = mid; else hi = mid;
+      }
+      si = lo;
+    }
+    si = __shfl_sync(FULL, si, 0);
+    __syncwarp();
+    const u32* src = reinterpret_cast<const u32*>(A.segs + si);
+    if (lane < sizeof(RangeSeg) / 4) reinterpret_cast<u32*>(&W.seg)[lane] = src[lane];
+    if (lane == 0) {
+      W.seg_lo = A.segs[si].item_begin;
+      W.seg_hi = (si + 1 < A.nsegs) ? A.segs[si + 1].item_begin : A.item_limit;
+    }
+    fresh = true;
+    __syncwarp();
+  }
+  ull qi;
+  u32 chunk;
+  const u32 kind = W.seg.kind;
+  if (fresh) {
+    const ull local = next - W.seg_lo;
+    if (kind == 0) {  // segments hold fewer than 2^32 items
+      const u32 l32 = (u32)local, ipq = W.seg.ipq;
+      const u32 q32 = l32 / ipq;
+      qi = q32;
+      chunk = l32 - q32 * ipq;
+    } else {
+      qi = local;
+      chunk = 0;
+    }
+  } else if (kind == 0) {
+    qi = W.qi;
+    chunk = W.chunk + 1;
+    if (chunk == W.seg.ipq) {
+      chunk = 0;
+      qi++;
+    }
+  } else {
+    qi = W.qi + 1;
+    chunk = 0;
+  }
+  StagedItem it;
+  it.req = W.seg.req;
+  it.kind = kind;
+  it.mod9 = W.seg.mod9;
+  it.valid = 1;
+  it.pad = 0;
+  if (kind == 0) {
+    const unsigned __int128 q = (((unsigned __int128)W.seg.q_hi << 64) | W.seg.q_lo) + qi;
+    it.q_lo = (u64)q;
+    it.q_hi = (u32)(q >> 64);
+    it.sbase = W.seg.s_lo + chunk * RANGE_ITEM;
+    it.send = min(it.sbase + RANGE_ITEM, W.seg.s_hi);
+    it.d_hi = 0;
+#pragma unroll
+    for (u32 j = 0; j < RANGE_ITEM / 32; j++) {
+      const u32 idx = it.sbase + j * 32 + lane;
+      if (idx < it.send) cp_async16(&W.stage[j * 32 + lane], T + idx);
+    }
+    cp_async_commit();
+  } else {
+    it.q_lo = W.seg.q_lo + qi * DENSE_ITEM;
+    it.q_hi = 0;
+    it.sbase = it.send = 0;
+    it.d_hi = W.seg.d_hi;
+  }
+  __syncwarp();
+  if (lane == 0) {
+    W.item = next;
+    W.qi = qi;
+    W.chunk = chunk;
+    W.nxt = it;
+  }
+  __syncwarp();
+}
+
+template <int R, int MINB, bool STATS = false>
+__global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) {
+  // diagnostics (STATS variant only): run pairs, excursion slow paths, replays, jumps, pops,
+  // expansions, passes, offers; clock64 cycles per phase (lane 0)
+  u32 c_iter = 0, c_slow = 0, c_replay = 0, c_jump = 0, c_pop = 0, c_exp = 0, c_blk = 0, c_offer = 0;
+  ull t_offer = 0, t_refill = 0, t_lanes = 0, t_mark = 0, t_stage = 0, t_thr = 0, t_wait = 0, t_sub = 0;
+  extern __shared__ __align__(16) unsigned char range_smem[];
+  RangeWarp* S = reinterpret_cast<RangeWarp*>(range_smem);
   __shared__ unsigned long long s_p3[41];
   __shared__ u32 s_pow3[9], s_keep9[9];
   const u32 lane = lane_id();
@@ -64,291 +239,413 @@ __global__ void __launch_bounds__(RWARPS * 32) k_range(const RangeArgs A) {
     for (u32 j = 0; j < 32; j++) m |= ((KEEP9 >> ((r + j) % 9u)) & 1u) << j;
     s_keep9[r] = m;
   }
+  if (lane == 0) {
+    W.item = ~0ull;
+    W.claim_hi = 0;
+    W.seg_lo = 1;
+    W.seg_hi = 0;
+    W.qi = W.acc_seeds = W.acc_items = 0;
+    W.chunk = W.since_thr = W.ring_seq = W.thr_bl = W.head = 0;
+    W.nxt.valid = 0;
+  }
   __syncthreads();
 
   const u32 k = A.k;
   const u32 k9 = (u32)((1ull << (k % 6)) % 9ull);  // 2^k mod 9 (2^6 = 1 mod 9)
-  // warp-uniform state
-  u32 qhead = 0, qcount = 0, ring_seq = 0;
-  bool exhausted = false;
-  // lane state
-  bool active = false;
-  u32 v0 = 0, v1 = 0, v2 = 0, v3 = 0, n0 = 0, n1 = 0, n2 = 0;
-  u32 st = 0, iters = 0, evalid = 0, pend = 0, req = 0, thr_st = 0;
-  u64 thr_top = 0;
+  const uint4* __restrict__ T = reinterpret_cast<const uint4*>(A.table);
+  stage_next(W, A, T, lane);
 
+  // ---- warp-uniform state (the rest lives in W) ----
+  u32 head = 0, tail = 0;  // queued seeds [head, tail)
+  bool exhausted = false;
+  u32 w_thr_st = 0, w_req = 0xFFFFFFFFu;
+  u64 w_gate = 0;  // excursion threshold, bits 32..95 (all ones when it is >= 2^96)
+  // ---- lane state ----
+  u32 v0 = 0, v1 = 0, v2 = 0, v3 = 0, n0 = 0, n1 = 0, n2 = 0, st = 0, req = 0, thr_st = 0;
+  u64 gate = 0;  // the lane's excursion threshold window (bits 32..95)
+  bool active = false, evalid = false;
+  u32 pend = 0;
+
+#define POP_NEXT(idx_)                                                               \
+  do {                                                                               \
+    if (idx_ < tail) {                                                               \
+      const uint4 a_ = W.qa[idx_ & (RQ - 1)], b_ = W.qb[idx_ & (RQ - 1)];            \
+      v0 = a_.x;                                                                     \
+      v1 = a_.y;                                                                     \
+      v2 = a_.z;                                                                     \
+      v3 = a_.w;                                                                     \
+      n0 = b_.x;                                                                     \
+      n1 = b_.y;                                                                     \
+      n2 = b_.z;                                                                     \
+      st = b_.w & 0xFFu;                                                             \
+      const uint4 g_ = W.ring[(b_.w >> 8) & 31u];                                    \
+      req = g_.x;                                                                    \
+      W.bln[lane] = (b_.w >> 16) & 0xFFu;                                            \
+      if (g_.x == w_req) { /* the warp's thresholds are the freshest */              \
+        thr_st = w_thr_st;                                                           \
+        gate = w_gate;                                                               \
+      } else {                                                                       \
+        thr_st = g_.y;                                                               \
+        gate = ((u64)g_.w << 32) | g_.z;                                             \
+      }                                                                              \
+      evalid = (b_.w >> 13) & 1u;                                                    \
+      if (evalid) { /* T^s(n) = v - 1 is an excursion candidate */                   \
+        W.e[0][lane] = v0 - 1;                                                       \
+        W.e[1][lane] = v1 - (v0 == 0);                                               \
+        W.e[2][lane] = v2 - ((v0 | v1) == 0);                                        \
+        W.e[3][lane] = v3 - ((v0 | v1 | v2) == 0);                                   \
+      }                                                                              \
+      active = true;                                                                 \
+      if (STATS) c_pop++;                                                            \
+      if (v3 >= OVF3) { /* the jump already left 2^119 */                            \
+        widen_seed(A, req, n0, n1, n2);                                              \
+        active = false;                                                              \
+      }                                                                              \
+    }                                                                                \
+  } while (0)
+
+  if (STATS) t_mark = clock64();
   for (;;) {
-    // ---- offers of finished seeds, one lane at a time ----
-    {
-      u32 pm = __ballot_sync(FULL, pend != 0);
-      while (pm) {
-        const u32 leader = __ffs(pm) - 1;
-        if (lane == leader) {
-          const u32 seed[4] = {W.lane[lane][1], W.lane[lane][2], W.lane[lane][3], 0};
-          if (pend & 1u) rec_offer_st(A.recs + req, W.lane[lane][0], seed);
-          if (pend & 2u) rec_offer_e<4>(A.recs + req, &W.lane[lane][4], seed);
-          pend = 0;
+    if (STATS) {
+      c_blk++;
+      const ull now = clock64();
+      t_lanes += now - t_mark;
+      t_mark = now;
+    }
+    // ---- warp-synchronous part: offers of finished seeds (rare), refill, exit ----
+    u32 pm = __ballot_sync(FULL, pend != 0);
+    while (pm) {
+      const u32 leader = __ffs(pm) - 1;
+      const u32 lp = __shfl_sync(FULL, pend, leader), lreq = W.c[4][leader];
+      if (lane == leader) {
+        const u32 seed[4] = {W.c[1][lane], W.c[2][lane], W.c[3][lane], 0};
+        if (STATS) c_offer++;
+        if (pend & 1u) rec_offer_st(A.recs + lreq, W.c[0][lane], seed);
+        if (pend & 2u) {
+          const u32 e4[4] = {W.pe[0][lane], W.pe[1][lane], W.pe[2][lane], W.pe[3][lane]};
+          rec_offer_e<4>(A.recs + lreq, e4, seed);
         }
-        pm &= pm - 1;
+        pend = 0;
       }
       __syncwarp();
+      if (lreq == w_req) {  // an offered value is a lower bound of the request's maximum
+        if (lp & 1u) w_thr_st = max(w_thr_st, W.c[0][leader]);
+        if (lp & 2u) {
+          const u32 e1 = W.pe[1][leader], e2 = W.pe[2][leader], e3 = W.pe[3][leader];
+          w_gate = max(w_gate, gate_window(e1, e2, e3));
+          const u32 t = e3 ? e3 : (e2 ? e2 : e1);
+          const u32 bl = t ? (e3 ? 96u : (e2 ? 64u : 32u)) + 32u - __clz(t) : 0u;
+          if (lane == 0) W.thr_bl = max(W.thr_bl, bl > 0 ? bl - 1 : 0u);
+        }
+      }
+      pm &= pm - 1;
     }
-
-    // ---- refill ----
-    const u32 idle = __ballot_sync(FULL, !active);
-    const u32 nidle = __popc(idle);
-    if (nidle >= (u32)REFILL_MIN || nidle == 32u) {
-      while (qcount < nidle && !exhausted) {
-        unsigned long long item = 0;
-        if (lane == 0) item = atomicAdd(A.item_cursor, 1ull);
-        item = __shfl_sync(FULL, item, 0);
-        if (item >= A.item_limit) {
-          exhausted = true;
-          break;
-        }
-        // segment of this item (binary search; the last segment with item_begin <= item)
-        u32 si = 0;
-        if (lane == 0) {
-          u32 lo = 0, hi = A.nsegs;
-          while (hi - lo > 1) {
-            const u32 mid = (lo + hi) >> 1;
-            if (A.segs[mid].item_begin <= item) lo = mid; else hi = mid;
-          }
-          si = lo;
-        }
-        si = __shfl_sync(FULL, si, 0);
-        const RangeSeg& G = A.segs[si];
-        const unsigned long long local = item - G.item_begin;
-        const u32 rq = G.req;
-        ReqRec* R = A.recs + rq;
+    if (STATS) {
+      const ull now = clock64();
+      t_offer += now - t_mark;
+      t_mark = now;
+    }
+    // ---- refill: keep 32 R seeds queued (each lane pops at most R per pass) ----
+    while (tail - head < 32u * R && !exhausted) {
+      if (STATS) t_sub = clock64();
+      cp_async_wait_all();  // this lane's copies of the staged item
+      __syncwarp();
+      if (STATS) {
+        const ull now = clock64();
+        t_wait += now - t_sub;
+        t_sub = now;
+      }
+      const StagedItem it = W.nxt;
+      if (!it.valid) {
+        exhausted = true;
+        break;
+      }
+      uint4 e[RANGE_ITEM / 32];
+      if (it.kind == 0) {
+#pragma unroll
+        for (u32 j = 0; j < RANGE_ITEM / 32; j++) e[j] = W.stage[j * 32 + lane];
+      }
+      __syncwarp();
+      stage_next(W, A, T, lane);  // the following item's copies overlap with this expansion
+      if (STATS) {
+        const ull now = clock64();
+        t_stage += now - t_sub;
+        t_sub = now;
+      }
+      const u32 rq = it.req;
+      if (rq != w_req || ++W.since_thr >= 64) {  // thresholds of the request, refreshed now and then
         ull sk = 0, ek = 0;
+        if (lane == 0 && rq != w_req && w_req != 0xFFFFFFFFu) {
+          if (W.acc_seeds) atomicAdd(&A.recs[w_req].seeds, W.acc_seeds);
+          atomicAdd(&A.recs[w_req].items_done, W.acc_items);
+        }
         if (lane == 0) {
-          sk = *(volatile ull*)&R->st_key;
-          ek = *(volatile ull*)&R->e_key;
+          sk = *(volatile ull*)&A.recs[rq].st_key;
+          ek = *(volatile ull*)&A.recs[rq].e_key;
         }
         sk = __shfl_sync(FULL, sk, 0);
         ek = __shfl_sync(FULL, ek, 0);
-        u32 mask = 0, kind = G.kind, sbase = 0, q0 = 0, q1 = 0, q2 = 0;
-        if (kind == 0) {
-          const unsigned long long qi = local / G.ipq;
-          const u32 chunk = (u32)(local - qi * G.ipq);
-          const unsigned __int128 q = (((unsigned __int128)G.q_hi << 64) | G.q_lo) + qi;
-          q0 = (u32)q;
-          q1 = (u32)(q >> 32);
-          q2 = (u32)(q >> 64);
-          sbase = G.s_lo + chunk * RANGE_ITEM;
-          const u32 send = min(sbase + RANGE_ITEM, G.s_hi);
-          const u32 b9 = (mod9_96(q0, q1, q2) * k9) % 9u;
-          const uint4* T = reinterpret_cast<const uint4*>(A.table);
-#pragma unroll
-          for (u32 j = 0; j < RANGE_ITEM / 32; j++) {
-            const u32 idx = sbase + j * 32 + lane;
-            if (idx < send) {
-              const uint4 e = T[idx];
-              u32 x = b9 + ((e.y >> 16) & 0xFFu);
-              x = (x >= 9u) ? x - 9u : x;
-              if (!G.mod9 || ((KEEP9 >> x) & 1u)) mask |= 1u << j;
-            }
-          }
-        } else {
-          const unsigned long long d = G.q_lo + local * DENSE_ITEM + 32ull * lane;
-          q0 = (u32)(G.q_lo + local * DENSE_ITEM);
-          q1 = (u32)((G.q_lo + local * DENSE_ITEM) >> 32);
-          if (d < G.d_hi) {
-            const unsigned long long cnt = G.d_hi - d;
-            mask = (cnt >= 32) ? FULL : ((1u << cnt) - 1u);
-            if (G.mod9) mask &= s_keep9[d % 9u];
-            if (d < 2) mask &= ~((d == 0) ? 3u : 1u);  // n = 0, 1 have no stopping time
-          }
+        u32 t[4];
+        key_decode<4>(ek, t);
+        if (rq != w_req) {
+          w_thr_st = 0;
+          w_gate = 0;
         }
-        u32 total;
-        const u32 excl = warp_excl_scan(__popc(mask), &total);
+        w_thr_st = max(w_thr_st, (u32)min(sk, 0xFFFFFFFFull));
+        w_gate = max(w_gate, gate_window(t[1], t[2], t[3]));
+        __syncwarp();
         if (lane == 0) {
-          if (total) atomicAdd(&R->seeds, (ull)total);
-          atomicAdd(&R->items_done, 1ull);
+          if (rq != w_req) W.acc_seeds = W.acc_items = W.thr_bl = 0;
+          W.thr_bl = max(W.thr_bl, (u32)(ek >> 54));
+          W.since_thr = 0;
         }
-        if (total) {
-          const u32 slot = ring_seq & (RR - 1);
-          ring_seq++;
-          u32 t[4];
-          key_decode<4>(ek, t);
-          const u32 thr_bl = (u32)(ek >> 54);
-          u32 rv = 0;
-          switch (lane) {
-            case 0: rv = kind; break;
-            case 1: rv = sbase; break;
-            case 2: rv = q0; break;
-            case 3: rv = q1; break;
-            case 4: rv = q2; break;
-            case 5: rv = rq; break;
-            case 6: rv = (u32)min(sk, 0xFFFFFFFFull); break;
-            case 7: rv = thr_bl; break;
-            case 8: rv = t[0]; break;
-            case 9: rv = t[1]; break;
-            case 10: rv = t[2]; break;
-            case 11: rv = t[3]; break;
-          }
-          if (lane < 12) W.ring[slot][lane] = rv;
-          u32 pos = qhead + qcount + excl;
-          const u32 mm = mask;
-          u32 m = mm;
-          while (m) {
-            const u32 j = ctz32(m);
-            m &= m - 1;
-            const u32 li = (kind == 0) ? (j * 32u + lane) : (lane * 32u + j);
-            W.q[pos & (RQ - 1)] = (unsigned short)((slot << 10) | li);
-            pos++;
-          }
-          qcount += total;
-        }
+        w_req = rq;
         __syncwarp();
       }
-      const u32 take = min(nidle, qcount);
-      if (!active) {
-        const u32 rank = __popc(idle & lanemask_lt());
-        if (rank < take) {
-          const u32 e = W.q[(qhead + rank) & (RQ - 1)];
-          const u32* G = W.ring[e >> 10];
-          const u32 li = e & 1023u;
-          req = G[5];
-          thr_st = G[6];
-          const u32 thr_bl = G[7];
-          W.lane[lane][8] = G[8];
-          W.lane[lane][9] = G[9];
-          W.lane[lane][10] = G[10];
-          W.lane[lane][11] = G[11];
-          thr_top = ((u64)G[11] << 32) | G[10];
-          unsigned __int128 N, V;
-          bool replay = true;
-          if (G[0] == 0) {
-            const uint4 en = reinterpret_cast<const uint4*>(A.table)[G[1] + li];
-            const unsigned __int128 Q = ((unsigned __int128)G[4] << 64) | ((u64)G[3] << 32) | G[2];
-            const u64 r = (u64)en.x | ((u64)(en.y & 0xFFu) << 32);
-            const u32 f = (en.y >> 8) & 0xFFu, emax = en.y >> 24;
-            N = (Q << k) | r;
-            const u32 nbl = (u32)(N >> 64) ? 128u - __clzll((u64)(N >> 64)) : 64u - __clzll((u64)N);
-            // all of T^0..T^k(n) < 2^emax (n + 1 + k) <= 2^(bitlen(n) + 1 + emax) <= threshold: skip them
-            replay = nbl + 1 + emax >= thr_bl;
-            if (!replay) {
-              V = Q * (unsigned __int128)s_p3[f] + (((u64)en.w << 32) | en.z);
-              st = k;
+      if (STATS) {
+        const ull now = clock64();
+        t_thr += now - t_sub;
+        t_sub = now;
+      }
+      const u32 w_thr_bl = W.thr_bl;
+      const u64 gate_w = w_gate;
+      const u32 slot = W.ring_seq & (RR - 1);
+      u32 mask = 0, total;
+      u32 pos;
+      if (it.kind == 0) {
+        const u32 q0 = (u32)it.q_lo, q1 = (u32)(it.q_lo >> 32), q2 = it.q_hi;
+        // per item (warp-uniform): n = q 2^k | r as limbs (k <= 34), bitlen(n) = bitlen(q) + k
+        const u32 kb = k & 31;
+        const u32 t0 = q0 << kb, t1 = __funnelshift_l(q0, q1, kb), t2 = __funnelshift_l(q1, q2, kb);
+        const u32 qk0 = (k >= 32) ? 0u : t0, qk1 = (k >= 32) ? t0 : t1, qk2 = (k >= 32) ? t1 : t2;
+        const u32 nbl = (q2 ? 96u - __clz(q2) : (q1 ? 64u - __clz(q1) : 32u - __clz(q0))) + k;
+        const u32 b9 = (mod9_96(q0, q1, q2) * k9) % 9u;
+        const u32 meta_item = (slot << 8) | (nbl << 16);
+        const bool jump_ok_base = true;
+#pragma unroll
+        for (u32 j = 0; j < RANGE_ITEM / 32; j++) {
+          if (it.sbase + j * 32 + lane < it.send) {
+            u32 x = b9 + ((e[j].y >> 16) & 0xFFu);
+            x = (x >= 9u) ? x - 9u : x;
+            if (!it.mod9 || ((KEEP9 >> x) & 1u)) mask |= 1u << j;
+          }
+        }
+        pos = tail + warp_excl_scan(__popc(mask), &total);
+#pragma unroll
+        for (u32 j = 0; j < RANGE_ITEM / 32; j++) {
+          if ((mask >> j) & 1u) {
+            const u32 f = (e[j].y >> 8) & 0xFFu, emax = e[j].y >> 24;
+            const u32 m0 = qk0 | e[j].x, m1 = qk1 | (e[j].y & 0xFFu);
+            u32 V0, V1, V2, V3, s0;
+            // T^0..T^k(n) < 2^emax (n + 1 + k) <= 2^(bitlen(n) + 1 + emax): skip them when that is
+            // below the excursion threshold, else replay the first k steps exactly
+            if (jump_ok_base && nbl + 1 + emax < w_thr_bl) {
+              // v = q 3^f + c in 32-bit limbs (3^f < 2^64, c < 2^64)
+              const u64 p = s_p3[f];
+              const u32 p0 = (u32)p, p1 = (u32)(p >> 32);
+              const u64 a = (u64)q0 * p0 + e[j].z;
+              const u64 bb = (u64)q0 * p1 + (a >> 32) + e[j].w;
+              const u64 cc = (u64)q1 * p0 + (u32)bb;
+              const u64 dd = (u64)q1 * p1 + (bb >> 32) + (cc >> 32);
+              V0 = (u32)a;
+              V1 = (u32)cc;
+              V2 = (u32)dd;
+              V3 = (u32)(dd >> 32);
+              if (q2) {  // q >= 2^64 (seeds >= 2^(64+k))
+                const u64 ee = (u64)q2 * p0 + V2;
+                V2 = (u32)ee;
+                V3 += q2 * p1 + (u32)(ee >> 32);
+              }
+              s0 = k;
+              if (STATS) c_jump++;
+            } else {
+              V0 = m0 + 1;
+              V1 = m1 + (V0 == 0);
+              V2 = qk2 + ((V0 | V1) == 0);
+              V3 = (V0 | V1 | V2) == 0;
+              s0 = 0;
+              if (STATS) c_replay++;
             }
-          } else {
-            N = ((u64)G[3] << 32 | G[2]) + (u64)li;
+            // excursion candidate T^s(n) = v - 1 <= v: bits 32..95 of v against the threshold
+            const u32 cand = ((V3 != 0) | ((((u64)V2 << 32) | V1) >= gate_w)) ? 1u : 0u;
+            W.qa[pos & (RQ - 1)] = make_uint4(V0, V1, V2, V3);
+            W.qb[pos & (RQ - 1)] = make_uint4(m0, m1, qk2, s0 | meta_item | (cand << 13));
+            pos++;
           }
-          if (replay) {
-            V = N + 1;
-            st = 0;
-          }
-          n0 = (u32)N;
-          n1 = (u32)(N >> 32);
-          n2 = (u32)(N >> 64);
-          v0 = (u32)V;
-          v1 = (u32)(V >> 32);
-          v2 = (u32)(V >> 64);
-          v3 = (u32)(V >> 96);
-          iters = 0;
-          evalid = 0;
-          active = true;
-          // excursion candidate: n itself, or T^k(n) = v - 1 after the jump
-          const unsigned __int128 X = V - 1;
-          const u32 x0 = (u32)X, x1 = (u32)(X >> 32), x2 = (u32)(X >> 64), x3 = (u32)(X >> 96);
-          if (ge128(x0, x1, x2, x3, &W.lane[lane][8])) {
-            W.lane[lane][4] = x0;
-            W.lane[lane][5] = x1;
-            W.lane[lane][6] = x2;
-            W.lane[lane][7] = x3;
-            evalid = 1;
+        }
+      } else {
+        // integers below 2^k: [d, d + 64) of [q_lo, d_hi), no residue sieve
+        const ull d = it.q_lo + 2ull * lane;
+#pragma unroll
+        for (u32 j = 0; j < 2; j++) {
+          const ull n = d + j;
+          if (n < it.d_hi && n >= 2 && (!it.mod9 || ((KEEP9 >> (u32)(n % 9u)) & 1u))) mask |= 1u << j;
+        }
+        pos = tail + warp_excl_scan(__popc(mask), &total);
+#pragma unroll
+        for (u32 j = 0; j < 2; j++) {
+          if ((mask >> j) & 1u) {
+            const ull n = d + j;
+            const u32 nbl = 64u - __clzll(n);
+            const u32 cand = ((n >> 32) >= gate_w) ? 1u : 0u;
+            W.qa[pos & (RQ - 1)] = make_uint4((u32)(n + 1), (u32)((n + 1) >> 32), 0u, 0u);
+            W.qb[pos & (RQ - 1)] = make_uint4((u32)n, (u32)(n >> 32), 0u, (slot << 8) | (cand << 13) | (nbl << 16));
+            pos++;
           }
         }
       }
-      qhead = (qhead + take) & (RQ - 1);
-      qcount -= take;
-      if (take == 0 && exhausted && nidle == 32u) break;
+      __syncwarp();
+      if (lane == 0) {
+        W.ring[slot] = make_uint4(rq, w_thr_st, (u32)w_gate, (u32)(w_gate >> 32));
+        W.ring_seq++;
+        W.acc_seeds += total;
+        W.acc_items++;
+      }
+      if (STATS) c_exp++;
+      tail += total;
+      __syncwarp();
     }
+    __syncwarp();
+    if (STATS) {
+      const ull now = clock64();
+      t_refill += now - t_mark;
+      t_mark = now;
+    }
+    if (exhausted && tail == head && __ballot_sync(FULL, active) == 0) break;
 
-    // ---- iterate ----
-    if (active) {
+    // ---- lanes: R times (take a seed if idle, one odd run and one even run) ----
 #pragma unroll 1
-      for (int it = 0; it < ITERS; it++) {
-        bool done = false, widen = false;
-        if (v3 >= (1u << 19)) {
-          widen = true;  // (v >> a) 3^a could leave 128 bits
+    for (int r = 0; r < R; r++) {
+      {
+        // idle lanes take the next queued seeds (a pending offer keeps its scratch until the next pass)
+        const u32 want = __ballot_sync(FULL, !active && !pend);
+        if (want) {
+          const u32 take = min((u32)__popc(want), tail - head);
+          if (!active && !pend) {
+            const u32 rank = __popc(want & lanemask_lt());
+            if (rank < take) POP_NEXT(head + rank);
+          }
+          head += take;
+        }
+      }
+      if (!active) continue;
+      {
+        // odd run capped at 7 steps (a longer run continues in the next pass, after an empty
+        // even run); 3^a from byte lookups in registers keeps shared memory off this path
+        const u32 a = ctz32(v0 | (1u << 7));
+        odd_run4(v0, v1, v2, v3, a, pow3_le7(a));
+        st += a;
+        if (STATS) c_iter++;
+      }
+      // excursion / overflow gate: (v3:v2:v1) >= (0:gate)
+      if (!lt96c(v1, v2, v3, (u32)gate, (u32)(gate >> 32), 0u)) {
+        if (v3 >= OVF3) {
+          // the next odd run could leave 128 bits: re-run this seed with wider limbs
+          widen_seed(A, req, n0, n1, n2);
+          active = false;
+          continue;
+        }
+        // excursion candidate (bits 32..95 at or above the threshold)
+        if (STATS) c_slow++;
+        const u32 x0 = v0 - 1, x1 = v1 - (v0 == 0), x2 = v2 - ((v0 | v1) == 0), x3 = v3 - ((v0 | v1 | v2) == 0);
+        bool take_it = !evalid;
+        if (evalid) take_it = lt96c(W.e[0][lane], W.e[1][lane], W.e[2][lane], x0, x1, x2) ? (W.e[3][lane] <= x3)
+                                                                                           : (W.e[3][lane] < x3);
+        if (take_it) {
+          W.e[0][lane] = x0;
+          W.e[1][lane] = x1;
+          W.e[2][lane] = x2;
+          W.e[3][lane] = x3;
+          evalid = true;
+        }
+      }
+      v0 -= 1;  // v0 == 0 gives b == 0 below, and the borrow cancels against the +1
+      const u32 b = ctz32(v0 | 0x80000000u);
+      const u32 w0 = __funnelshift_r(v0, v1, b), w1 = __funnelshift_r(v1, v2, b);
+      const u32 w2 = __funnelshift_r(v2, v3, b), w3 = v3 >> b;
+      st += b;
+      if (((w3 == 0) & (b != 0) & lt96c(w0, w1, w2, n0, n1, n2)) | (st > ST_CAP)) {
+        if (st > ST_CAP) {
+          atomicOr(&A.recs[req].errors, ERR_ITER_CAP);
+          atomicAdd(&A.recs[req].failures, 1ull);
         } else {
-          const u32 a = ctz32(v0 | (1u << 8));
-          odd_run4(v0, v1, v2, v3, a, s_pow3[a]);
-          st += a;
-          if ((((u64)v3 << 32) | v2) >= thr_top) {
-            const u32 x0 = v0 - 1, x1 = v1 - (v0 == 0), x2 = v2 - ((v0 | v1) == 0), x3 = v3 - ((v0 | v1 | v2) == 0);
-            const u32* ref = evalid ? &W.lane[lane][4] : &W.lane[lane][8];
-            if (ge128(x0, x1, x2, x3, ref)) {
-              W.lane[lane][4] = x0;
-              W.lane[lane][5] = x1;
-              W.lane[lane][6] = x2;
-              W.lane[lane][7] = x3;
-              evalid = 1;
-            }
-          }
-          v0 -= 1;
-          const u32 b = ctz32(v0 | 0x80000000u);
-          const u32 w0 = __funnelshift_r(v0, v1, b), w1 = __funnelshift_r(v1, v2, b);
-          const u32 w2 = __funnelshift_r(v2, v3, b), w3 = v3 >> b;
-          if (b != 0 && w3 == 0 && w2 <= n2 && lt96(w0, w1, w2, n0, n1, n2)) {
-            u32 i = 1;
-            for (; i < b; i++) {
-              const u32 y0 = __funnelshift_r(v0, v1, i), y1 = __funnelshift_r(v1, v2, i);
-              const u32 y2 = __funnelshift_r(v2, v3, i), y3 = v3 >> i;
-              if (y3 == 0 && lt96(y0, y1, y2, n0, n1, n2)) break;
-            }
-            st += i;
-            done = true;
-          } else {
-            st += b;
-            v0 = w0 + 1;
-            v1 = w1;
-            v2 = w2;
-            v3 = w3;
-            if (v0 == 0 && b != 0) {
-              v1 += 1;
-              if (v1 == 0) {
-                v2 += 1;
-                if (v2 == 0) v3 += 1;
-              }
-            }
-          }
-        }
-        if (done) {
-          W.lane[lane][1] = n0;
-          W.lane[lane][2] = n1;
-          W.lane[lane][3] = n2;
+          // the seed fell below its start inside this run; st is an upper bound of sigma
           if (st >= thr_st) {
-            W.lane[lane][0] = st;
-            pend |= 1u;
-          }
-          if (evalid) pend |= 2u;
-          active = false;
-          break;
-        }
-        if (widen || ++iters >= A.iter_cap) {
-          if (widen) {
-            const u32 wi = atomicAdd(A.widen_count, 1u);
-            if (wi < A.widen_cap) {
-              A.widen[wi] = WidenEntry{req, n0, n1, n2};
-              atomicAdd(&A.recs[req].widened, 1ull);
-            } else {
-              atomicOr(&A.recs[req].errors, ERR_WIDEN_FULL);
-              atomicAdd(&A.recs[req].failures, 1ull);
+            // i* = least i with (v-1) >> i < n.  With d = bitlen(v-1) - bitlen(n),
+            // i* is d when (v-1) >> d < n, else d + 1.
+            u32 t = v3, base = 96;
+            if (!t) { t = v2; base = 64; }
+            if (!t) { t = v1; base = 32; }
+            if (!t) { t = v0; base = 0; }
+            const int d = (int)(base + 32u - __clz(t)) - (int)W.bln[lane];
+            u32 istar = 1;
+            if (d >= 1) {
+              const u32 y0 = __funnelshift_r(v0, v1, d), y1 = __funnelshift_r(v1, v2, d);
+              const u32 y2 = __funnelshift_r(v2, v3, d), y3 = v3 >> d;
+              istar = ((y3 == 0) & lt96c(y0, y1, y2, n0, n1, n2)) ? (u32)d : (u32)d + 1;
             }
-          } else {
-            atomicOr(&A.recs[req].errors, ERR_ITER_CAP);
-            atomicAdd(&A.recs[req].failures, 1ull);
+            st = st - b + istar;
+            if (st >= thr_st) {
+              W.c[0][lane] = st;
+              pend |= 1u;
+            }
           }
-          active = false;
-          break;
+          if (evalid) {
+            pend |= 2u;
+            W.pe[0][lane] = W.e[0][lane];
+            W.pe[1][lane] = W.e[1][lane];
+            W.pe[2][lane] = W.e[2][lane];
+            W.pe[3][lane] = W.e[3][lane];
+          }
+          if (pend) {
+            W.c[1][lane] = n0;
+            W.c[2][lane] = n1;
+            W.c[3][lane] = n2;
+            W.c[4][lane] = req;
+          }
+        }
+        active = false;
+        // a lane with a pending offer waits for the next pass (its scratch is in use)
+      } else {
+        v0 = w0 + 1;
+        v1 = w1;
+        v2 = w2;
+        v3 = w3;
+        if ((v0 == 0) & (b != 0)) {
+          v1 += 1;
+          if (v1 == 0) {
+            v2 += 1;
+            if (v2 == 0) v3 += 1;
+          }
         }
       }
     }
   }
+#undef POP_NEXT
+  if (STATS && A.stats && lane == 0) {
+    atomicAdd(&A.stats[8], t_offer);
+    atomicAdd(&A.stats[9], t_refill);
+    atomicAdd(&A.stats[10], t_lanes);
+    atomicAdd(&A.stats[11], t_wait);
+    atomicAdd(&A.stats[12], t_stage);
+    atomicAdd(&A.stats[13], t_thr);
+  }
+  if (STATS && A.stats) {
+    u32 c[8] = {c_iter, c_slow, c_replay, c_jump, c_pop, c_exp, c_blk, c_offer};
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      u32 x = c[i];
+      if (i == 5 || i == 6) x = (lane == 0) ? x : 0u;  // warp-uniform counters
+#pragma unroll
+      for (u32 d = 16; d; d >>= 1) x += __shfl_xor_sync(FULL, x, d);
+      if (lane == 0) atomicAdd(&A.stats[i], (ull)x);
+    }
+  }
+  if (lane == 0 && w_req != 0xFFFFFFFFu) {
+    if (W.acc_seeds) atomicAdd(&A.recs[w_req].seeds, W.acc_seeds);
+    atomicAdd(&A.recs[w_req].items_done, W.acc_items);
+  }
+  cp_async_wait_all();
 }
 
 // ------------------------------------------------------------------
@@ -436,13 +733,21 @@ __global__ void __launch_bounds__(128) k_range_wide(const WidenEntry* __restrict
 // ------------------------------------------------------------------
 int range_variants() { return 4; }
 
-#define CZ_RANGE_VARIANTS(X) X(0, 4, 1) X(1, 4, 4) X(2, 8, 4) X(3, 8, 8)
+constexpr size_t RANGE_SMEM = sizeof(RangeWarp) * RWARPS;
+
+cudaError_t launch_range_stats(const RangeArgs& a, u32 grid, cudaStream_t st) {
+  k_range<2, 3, true><<<grid, RWARPS * 32, RANGE_SMEM, st>>>(a);
+  return cudaGetLastError();
+}
+
+// (run pairs per pass, minimum resident blocks per SM)
+#define CZ_RANGE_VARIANTS(X) X(0, 1, 3) X(1, 2, 3) X(2, 2, 4) X(3, 1, 4)
 
 cudaError_t launch_range(const RangeArgs& a, int variant, u32 grid, cudaStream_t st) {
   switch (variant) {
-#define X(id, it, rm) \
+#define X(id, rm, mb) \
   case id:            \
-    k_range<it, rm><<<grid, RWARPS * 32, 0, st>>>(a); break;
+    k_range<rm, mb><<<grid, RWARPS * 32, RANGE_SMEM, st>>>(a); break;
     CZ_RANGE_VARIANTS(X)
 #undef X
     default: return cudaErrorInvalidValue;
@@ -452,13 +757,26 @@ cudaError_t launch_range(const RangeArgs& a, int variant, u32 grid, cudaStream_t
 
 cudaError_t range_occupancy(int variant, int* bps) {
   switch (variant) {
-#define X(id, it, rm) \
+#define X(id, rm, mb) \
   case id:            \
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_range<it, rm>, RWARPS * 32, 0);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_range<rm, mb>, RWARPS * 32, RANGE_SMEM);
     CZ_RANGE_VARIANTS(X)
 #undef X
     default: return cudaErrorInvalidValue;
   }
+}
+
+// Opts every range kernel into RANGE_SMEM (> 48 KB) of dynamic shared memory.
+cudaError_t range_init() {
+  cudaError_t e = cudaSuccess;
+#define X(id, rm, mb)                                                                                      \
+  if (e == cudaSuccess)                                                                                    \
+    e = cudaFuncSetAttribute(k_range<rm, mb>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RANGE_SMEM);
+  CZ_RANGE_VARIANTS(X)
+#undef X
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_range<2, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RANGE_SMEM);
+  return e;
 }
 
 cudaError_t launch_range_wide(const WidenEntry* list, const u32* count, u32 cap, int limbs, ReqRec* recs,
