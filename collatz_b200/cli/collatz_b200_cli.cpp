@@ -1,0 +1,80 @@
+// collatz_b200 -- drop-in for the reference program collatz_cudav7.cu.
+//
+//   echo "3 2 2 9 1 0" | collatz_b200 [N]
+//
+// Reads one 6-tuple "base sigfig threepower number doubleeven numevens" from
+// stdin (cu:96-101), verifies all n < 2^N below that Step-1 node on the GPU,
+// prints every seed whose trajectory reaches 2^100 on stdout in the
+// reference's format (cu:298) and the reference's summary line on stderr
+// (cu:181-182), followed by one "# results {...}" JSON line with the outputs
+// the reference does not compute.  N defaults to 45 (MAXBITS, cu:43) or the
+// COLLATZ_MAXBITS environment variable.
+#include <cinttypes>
+#include <cstdio>
+#include <cstdlib>
+#include <iostream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "collatz.h"
+
+static std::string u128s(const uint32_t* w, int n) {
+  unsigned __int128 x = 0;
+  for (int i = n - 1; i >= 0; i--) x = (x << 32) | w[i];
+  if (x == 0) return "0";
+  std::string s;
+  while (x) {
+    s.insert(s.begin(), char('0' + (int)(x % 10)));
+    x /= 10;
+  }
+  return s;
+}
+
+int main(int argc, char** argv) {
+  uint32_t maxbits = 45;
+  if (const char* e = std::getenv("COLLATZ_MAXBITS")) maxbits = (uint32_t)std::atoi(e);
+  if (argc > 1) maxbits = (uint32_t)std::atoi(argv[1]);
+  std::string line;
+  std::getline(std::cin, line);
+  std::istringstream iss(line);
+  uint64_t a[6] = {0, 0, 0, 0, 0, 0};
+  iss >> a[0] >> a[1] >> a[2] >> a[3] >> a[4] >> a[5];
+
+  collatz_config cfg;
+  collatz_config_default(&cfg);
+  cfg.maxbits = maxbits;
+  collatz_ctx* ctx = nullptr;
+  int rc = collatz_create(&cfg, &ctx);
+  if (rc) {
+    std::fprintf(stderr, "collatz_create: %s\n", collatz_status_string(rc));
+    return 2;
+  }
+  collatz_case c = {{a[0], 0}, (uint32_t)a[1], (uint32_t)a[2], {a[3], 0}, (uint32_t)a[4], (uint32_t)a[5]};
+  const uint64_t cap = 1u << 20;
+  std::vector<uint32_t> ov(4 * cap);
+  collatz_case_result r = {};
+  r.overflow_seeds = ov.data();
+  r.overflow_cap = cap;
+  rc = collatz_run_case(ctx, &c, &r);
+  if (rc && rc != COLLATZ_E_DEVICE) {
+    std::fprintf(stderr, "collatz_run_case: %s: %s\n", collatz_status_string(rc), collatz_last_error(ctx));
+    collatz_destroy(ctx);
+    return 3;
+  }
+  for (uint64_t i = 0; i < r.n_overflow && i < cap; i++)
+    std::printf("%X%08X%08X\n", ov[4 * i + 2], ov[4 * i + 1], ov[4 * i]);
+  std::fflush(stdout);
+  std::fprintf(stderr, "Number of kernel launches = %" PRIu64 ". ", r.launches);
+  std::fprintf(stderr, "Spot checks = %u. Complete hash = %X.\n", r.spot_checks, r.hash);
+  std::fprintf(stderr,
+               "# results {\"seeds_checked\": %" PRIu64 ", \"pairs\": %" PRIu64 ", \"cpu_pairs\": %" PRIu64
+               ", \"overflow\": %" PRIu64
+               ", \"max_excursion\": \"%s\", \"max_excursion_seed\": \"%s\", \"max_stopping_time\": %" PRIu64
+               ", \"max_stopping_time_seed\": \"%s\", \"errors\": %u, \"device_ms\": %.3f}\n",
+               r.seeds_checked, r.pairs, r.cpu_pairs, r.n_overflow, u128s(r.max_excursion, 4).c_str(),
+               u128s(r.max_excursion_seed, 4).c_str(), r.max_stopping_time, u128s(r.max_stopping_time_seed, 4).c_str(),
+               r.errors, r.device_ms);
+  collatz_destroy(ctx);
+  return r.errors ? 4 : 0;
+}
