@@ -121,6 +121,24 @@ int collatz_run_case(collatz_ctx *ctx, const collatz_case *c, collatz_case_resul
 int collatz_verify_pairs(collatz_ctx *ctx, uint32_t bigindex, const uint32_t *pairs, uint32_t npairs,
                          collatz_case_result *out);
 
+/* No counterpart in the reference.  collatz_verify_pairs for callers that
+ * cannot allocate memory while they verify: an application that gives this
+ * library device buffers from its own memory pool and allows no other
+ * allocation, or a latency-bound loop in which cudaMalloc/cudaFree, which can
+ * block and synchronize the device, are not allowed.  It allocates nothing:
+ * d_pairs (npairs x 8 uint32, same layout as collatz_verify_pairs) is
+ * already in device memory, the result comes back in *out (host), and the
+ * kernel's scratch is a fixed 64 KiB device array that every GPU loading the
+ * library holds until exit.  At most 4064 overflow seeds are reported per
+ * call: out->overflow_cap above 4064 is rejected with COLLATZ_E_LIMIT (when
+ * more seeds overflow than are reported, n_overflow still counts all of
+ * them).  The first call on a device looks up the array's device address;
+ * make that first call before any stream capture.  Calls share the array,
+ * so calls that overlap on the GPU race; the context's mutex serialises
+ * calls made through one context. */
+int collatz_verify_pairs_noalloc(collatz_ctx *ctx, uint32_t bigindex, const uint32_t *d_pairs,
+                                 uint32_t npairs, collatz_case_result *out);
+
 /* Step-1 leaves of a case (search1, cu:497-563) for N = maxbits, in the
  * reference's order, without Steps 2-3: each pair as 8 uint32 with base
  * limb 3 = bigindex.  *count receives the number of leaves (pairs are
