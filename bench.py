@@ -39,6 +39,8 @@ UNIT = "seeds/s"
 # ctz, table, overflow test) and, per even run, 2L + 4 (decrement, ctz, L
 # shifts, increment with carry, descent test).
 OPS_JUMP, OPS_ODD, OPS_EVEN = 16, 14, 12
+# DRAM bytes (read + write) of one k_range launch, measured with ncu.
+K_RANGE_DRAM_BYTES = 5.316864e6 + 0.210944e6
 
 
 def dist_env():
@@ -268,7 +270,11 @@ def main():
                         "max_excursion": str(res.max_excursion),
                         "max_excursion_seed": str(res.max_excursion_seed), "errors": res.errors},
             "roofline": {"bound": "int", "achieved": achieved, "peak": peak, "unit": "Tops/s (32-bit)",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": K_RANGE_DRAM_BYTES,
+                         "traffic_basis": "dram__bytes_read.sum + dram__bytes_write.sum of one k_range "
+                                          "launch (ncu, 2^33 block); the k = 24 survivor table is read "
+                                          "from DRAM once per launch and from L2 after that, so the "
+                                          "figure does not grow with the block size",
                          "model": f"{ops_per_seed:.1f} algorithmic 32-bit ops per surviving seed "
                                   f"({OPS_JUMP} + {OPS_ODD} x {odd_per:.2f} odd runs + {OPS_EVEN} x "
                                   f"{even_per:.2f} even runs) x {res.seeds_checked} seeds per launch",
