@@ -150,6 +150,156 @@ def run_reference(args):
     return 0
 
 
+def _range_key(r):
+    return (r.seeds_checked, r.failures, r.widened, r.max_excursion, r.max_excursion_seed,
+            r.max_stopping_time, r.max_stopping_time_seed, r.errors)
+
+
+def run_batched(v, n_req: int = 4096, seed: int = 4096, lo_log2: int = 20, hi_log2: int = 34) -> dict:
+    """Batched configuration: n_req range requests, sizes log-uniform in
+    [2^lo, 2^hi] seeds, offsets uniform in [2^40, 2^64) aligned to the 2^24
+    sieve modulus (seeded), all in one persistent launch (a plan: lowered work
+    list + captured graph), against the plain path that verifies the same
+    requests one at a time (collatz_verify_range).  Bit-exact per request."""
+    import numpy as np
+    import torch
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(lo_log2 * np.log(2), hi_log2 * np.log(2), n_req)).astype(np.uint64)
+    reqs = []
+    for s in sizes:
+        off = int(rng.integers(1 << 40, 1 << 64, dtype=np.uint64))
+        reqs.append((off - off % (1 << K_SIEVE), int(s), K_SIEVE, True))
+    total = sum(int(s) for s in sizes)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plan = v.plan(reqs)
+    t_plan = time.perf_counter() - t0
+    plan.launch()
+    batched_warm = plan.results()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plan.launch()
+    batched = plan.results()
+    t_batched = time.perf_counter() - t0
+    dev_ms = batched[0].device_ms
+    plan.close()
+    t0 = time.perf_counter()
+    plain = [v.verify_range(*q) for q in reqs]
+    t_plain = time.perf_counter() - t0
+    dev_plain = sum(p.device_ms for p in plain) / 1e3
+    exact = all(_range_key(a) == _range_key(b) for a, b in zip(batched, plain)) and \
+        all(_range_key(a) == _range_key(b) for a, b in zip(batched, batched_warm))
+    return {"workload": f"{n_req} range requests, sizes log-uniform [2^{lo_log2}, 2^{hi_log2}], offsets "
+                        "uniform [2^40, 2^64) aligned to 2^24, k=24, seeded (numpy default_rng"
+                        f"({seed}))",
+            "seeds": total, "batched_seeds_per_s": total / t_batched,
+            "batched_device_seeds_per_s": total / (dev_ms / 1e3), "plan_build_s": t_plan,
+            "plain_seeds_per_s": total / t_plain, "plain_device_seeds_per_s": total / dev_plain,
+            "speedup_vs_plain_wall": t_plain / t_batched,
+            "speedup_vs_plain_device": dev_plain / (dev_ms / 1e3),
+            "bit_exact_vs_plain": bool(exact)}
+
+
+def run_served(v, capacity: float, load: float = 0.7, duration: float = 1.0, seed: int = 5,
+               slice_items: int = 1 << 19, plain_sample: int = 600) -> dict:
+    """Served configuration: Poisson arrivals at `load` x capacity (range seeds
+    per second), 70 % range verifications (sizes log-uniform 2^16..2^32,
+    offsets uniform [2^40, 2^64), unaligned) and 30 % trajectory queries
+    (1..65536 seeds, log-uniform count, bit lengths uniform 64..256), through
+    collatz_server_*; p50/p99 latency, throughput, and the plain path (each
+    request alone, in arrival order) on a sample of the same stream."""
+    import numpy as np
+    import collatz_b200 as cb
+    rng = np.random.default_rng(seed)
+    mean_range = ((1 << 32) - (1 << 16)) / np.log(1 << 16)
+    lam = load * capacity / (0.7 * mean_range)
+    n = max(50, int(lam * duration))
+    gaps = rng.exponential(1.0 / lam, n)
+    arrivals = np.cumsum(gaps) - gaps[0]
+    # seed pool for trajectory queries: random limbs, bit length uniform 64..256
+    pool_n = 1 << 21
+    pool = rng.integers(0, 1 << 32, size=(pool_n, 8), dtype=np.uint64).astype(np.uint32)
+    bl = rng.integers(64, 257, pool_n)
+    for j in range(8):
+        keep = np.clip(bl - 32 * j, 0, 32)
+        mask = np.where(keep >= 32, 0xFFFFFFFF, (1 << keep.astype(np.uint64)) - 1).astype(np.uint32)
+        pool[:, j] &= mask
+    top = (bl - 1) // 32
+    pool[np.arange(pool_n), top] |= (1 << ((bl - 1) % 32)).astype(np.uint32)
+    reqs = []
+    for i in range(n):
+        if rng.random() < 0.7:
+            size = int(np.exp(rng.uniform(16 * np.log(2), 32 * np.log(2))))
+            off = int(rng.integers(1 << 40, 1 << 64, dtype=np.uint64))
+            reqs.append(("range", (off, size, K_SIEVE)))
+        else:
+            m = int(np.exp(rng.uniform(0, 16 * np.log(2))))
+            m = max(1, min(m, 65536))
+            a = int(rng.integers(0, pool_n - m))
+            reqs.append(("traj", pool[a:a + m]))
+    srv = cb.Server(26, range_k=K_SIEVE, slice_items=slice_items)
+    # warm-up: tables, pools, first slices
+    for t in [srv.submit_range(1 << 50, 1 << 30), srv.submit_trajectory_array(pool[:1000])]:
+        srv.wait(t)
+    tickets = [None] * n
+    resps = [None] * n
+
+    def waiter():
+        for i in range(n):
+            while tickets[i] is None:
+                time.sleep(1e-4)
+            resps[i] = srv.wait(tickets[i])
+
+    wt = threading.Thread(target=waiter)
+    wt.start()
+    t0 = time.perf_counter()
+    for i, (kind, arg) in enumerate(reqs):
+        d = t0 + arrivals[i] - time.perf_counter()
+        if d > 0:
+            time.sleep(d)
+        tickets[i] = srv.submit_range(*arg) if kind == "range" else srv.submit_trajectory_array(arg)
+    wt.join()
+    wall = max(r.done_s for r in resps) - min(r.submit_s for r in resps)
+    info = srv.info()
+    srv.stop()
+    lat = np.array([r.latency_s for r in resps]) * 1e3
+    lat_r = np.array([r.latency_s for r, (k, _) in zip(resps, reqs) if k == "range"]) * 1e3
+    lat_t = np.array([r.latency_s for r, (k, _) in zip(resps, reqs) if k == "traj"]) * 1e3
+    range_seeds = sum(a[1] for k, a in reqs if k == "range")
+    traj_seeds = sum(len(a) for k, a in reqs if k == "traj")
+    # plain path: the first plain_sample requests one at a time
+    sub = reqs[:plain_sample]
+    t1 = time.perf_counter()
+    exact = True
+    for (kind, arg), r in zip(sub, resps):
+        if kind == "range":
+            exact &= _range_key(v.verify_range(*arg)) == _range_key(r.range)
+        else:
+            status, st, exc = v.trajectory_array(arg)
+            exact &= bool((status == r.traj_status).all() and (st == r.traj_stopping_time).all()
+                          and (exc == r.traj_excursion).all())
+    t_plain = time.perf_counter() - t1
+    sub_seeds = sum(a[1] for k, a in sub if k == "range")
+    return {"workload": f"Poisson arrivals for {duration:.1f} s at {load:.2f} x the plain kernel's "
+                        "seeds/s; 70% ranges (log-uniform 2^16..2^32 seeds, offsets uniform [2^40, 2^64)), "
+                        "30% trajectory queries (log-uniform 1..65536 seeds of 64..256 bits); numpy "
+                        f"default_rng({seed})",
+            "requests": n, "lambda_per_s": lam, "range_seeds": range_seeds, "traj_seeds": traj_seeds,
+            "seeds_per_s": range_seeds / wall, "traj_seeds_per_s": traj_seeds / wall,
+            "offered_seeds_per_s": load * capacity,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "range_p50_ms": float(np.percentile(lat_r, 50)), "range_p99_ms": float(np.percentile(lat_r, 99)),
+            "traj_p50_ms": float(np.percentile(lat_t, 50)) if len(lat_t) else None,
+            "traj_p99_ms": float(np.percentile(lat_t, 99)) if len(lat_t) else None,
+            "statuses_ok": int(sum(r.status == 0 for r in resps)),
+            "slices": info["range_slices"], "traj_batches": info["traj_batches"],
+            "device_busy_frac": info["device_busy_s"] / wall,
+            "plain_seeds_per_s_same_stream": sub_seeds / t_plain,
+            "plain_sample": f"first {len(sub)} requests one at a time (verify_range / trajectory)",
+            "served_vs_plain": (range_seeds / wall) / (sub_seeds / t_plain),
+            "bit_exact_vs_plain_sample": bool(exact)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -159,6 +309,10 @@ def main():
     ap.add_argument("--size-log2", type=int, default=SIZE_LOG2,
                     help="block size (default 38, the benchmark configuration)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched and served measurements (run at N = 1 only)")
+    ap.add_argument("--served-load", type=float, default=0.7)
+    ap.add_argument("--served-duration", type=float, default=1.0)
     ap.add_argument("--variant", type=int, default=None)
     args = ap.parse_args()
     if args.impl == "reference":
@@ -293,6 +447,14 @@ def main():
             line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": nthreads, "kind": "port",
                                     "sample": f"[2^40, 2^40 + {csize}) in {cdt:.1f} s (oracle run-length "
                                               f"loop after cu:684-715, {nthreads} threads)"}
+        if world == 1 and not args.no_extras:
+            for key, fn in (("batched", lambda: run_batched(v)),
+                            ("served", lambda: run_served(v, value, load=args.served_load,
+                                                          duration=args.served_duration))):
+                try:
+                    line[key] = fn()
+                except Exception as e:  # noqa: BLE001 -- the headline line is printed regardless
+                    line[key] = {"error": f"{type(e).__name__}: {e}"}
         print(json.dumps(line), flush=True)
     plan.close()
     v.close()

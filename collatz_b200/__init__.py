@@ -65,6 +65,36 @@ class RangeResultC(C.Structure):
                 ("errors", C.c_uint32), ("status", C.c_int32), ("device_ms", C.c_double)]
 
 
+REQ_RANGE, REQ_TRAJECTORY = 0, 1
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("max_active", C.c_uint32), ("slice_items", C.c_uint32), ("hbm_reserve", C.c_uint64),
+                ("traj_batch_seeds", C.c_uint32), ("reserved", C.c_uint32 * 7)]
+
+
+class RequestC(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("nseeds", C.c_uint32), ("range", Range),
+                ("seeds", C.c_void_p), ("stopping_time", C.c_void_p), ("excursion", C.c_void_p),
+                ("status", C.c_void_p)]
+
+
+class ResponseC(C.Structure):
+    _fields_ = [("ticket", C.c_uint64), ("status", C.c_int32), ("kind", C.c_uint32),
+                ("range", RangeResultC), ("submit_s", C.c_double), ("admit_s", C.c_double),
+                ("done_s", C.c_double)]
+
+
+class ServerInfoC(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("admitted", C.c_uint64), ("completed", C.c_uint64),
+                ("refused", C.c_uint64), ("range_slices", C.c_uint64), ("traj_batches", C.c_uint64),
+                ("range_seeds_checked", C.c_uint64), ("traj_seeds", C.c_uint64),
+                ("active", C.c_uint32), ("pending", C.c_uint32), ("hbm_free", C.c_uint64),
+                ("hbm_admitted", C.c_uint64), ("device_busy_s", C.c_double), ("loops", C.c_uint64),
+                ("host_admit_s", C.c_double), ("host_slice_s", C.c_double), ("host_batch_s", C.c_double),
+                ("host_complete_s", C.c_double), ("host_idle_s", C.c_double)]
+
+
 def _limbs(arr) -> int:
     return sum(int(w) << (32 * i) for i, w in enumerate(arr))
 
@@ -101,6 +131,12 @@ def lib() -> C.CDLL:
             "collatz_plan_results": (C.c_int, [P, P]),
             "collatz_plan_destroy": (None, [P]),
             "collatz_trajectory": (C.c_int, [P, P, C.c_uint32, P, P, P]),
+            "collatz_server_config_default": (None, [C.POINTER(ServerConfig)]),
+            "collatz_server_start": (C.c_int, [C.POINTER(Config), C.POINTER(ServerConfig), C.POINTER(P)]),
+            "collatz_server_submit": (C.c_int, [P, C.POINTER(RequestC), C.POINTER(C.c_uint64)]),
+            "collatz_server_wait": (C.c_int, [P, C.c_uint64, C.c_double, C.POINTER(ResponseC)]),
+            "collatz_server_info": (C.c_int, [P, C.POINTER(ServerInfoC)]),
+            "collatz_server_stop": (C.c_int, [P]),
             "collatz_variant_count": (C.c_int, [C.c_int]),
             "collatz_set_variant": (C.c_int, [P, C.c_int, C.c_int]),
         }
@@ -356,6 +392,18 @@ class Verifier:
         self._check(lib().collatz_trajectory(self._h, arr, n, st, exc, status), "trajectory")
         return [(status[i], st[i], _limbs(exc[16 * i:16 * i + 16])) for i in range(n)]
 
+    def trajectory_array(self, seeds):
+        """seeds: numpy (n, 8) uint32 limbs -> numpy (status, stopping_time, excursion (n, 16))."""
+        import numpy as np
+        seeds = np.ascontiguousarray(seeds, dtype=np.uint32)
+        n = seeds.shape[0]
+        st = np.zeros(max(1, n), dtype=np.uint64)
+        exc = np.zeros((max(1, n), 16), dtype=np.uint32)
+        status = np.zeros(max(1, n), dtype=np.uint32)
+        self._check(lib().collatz_trajectory(self._h, seeds.ctypes.data, n, st.ctypes.data, exc.ctypes.data,
+                                             status.ctypes.data), "trajectory")
+        return status[:n], st[:n], exc[:n]
+
 
 class Plan:
     """Lowered range requests + a captured CUDA graph, relaunchable."""
@@ -388,6 +436,145 @@ class Plan:
     def __del__(self):
         try:
             self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class Response:
+    """One served request's outcome (collatz_response)."""
+    ticket: int
+    status: int
+    kind: int
+    range: RangeResult | None = None
+    # trajectory queries: numpy arrays status (n,), stopping_time (n,), excursion (n, 16) limbs
+    traj_status: object = None
+    traj_stopping_time: object = None
+    traj_excursion: object = None
+    submit_s: float = 0.0
+    admit_s: float = 0.0
+    done_s: float = 0.0
+
+    @property
+    def latency_s(self) -> float:
+        return self.done_s - self.submit_s
+
+    @property
+    def queue_s(self) -> float:
+        return self.admit_s - self.submit_s
+
+    def trajectory(self) -> list[tuple[int, int, int]]:
+        """[(status, stopping_time, excursion)] per seed, as Verifier.trajectory."""
+        return [(int(self.traj_status[i]), int(self.traj_stopping_time[i]),
+                 _limbs(self.traj_excursion[i])) for i in range(len(self.traj_status))]
+
+
+def seeds_array(seeds):
+    """[int] (each < 2^256) -> numpy (n, 8) uint32 little-endian limbs."""
+    import numpy as np
+    arr = np.zeros((len(seeds), 8), dtype=np.uint32)
+    for i, s in enumerate(seeds):
+        if s < 0 or s >> 256:
+            raise ValueError("seeds must be in [0, 2^256)")
+        for j in range(8):
+            arr[i, j] = (s >> (32 * j)) & 0xFFFFFFFF
+    return arr
+
+
+class Server:
+    """Continuous-batching server (collatz_server_*): submit from any thread,
+    wait for each ticket.  Range requests and trajectory queries share the
+    device; results equal the same request run alone."""
+
+    def __init__(self, maxbits: int = 26, range_k: int = 24, device: int = 0, max_active: int = 256,
+                 slice_items: int = 1 << 19, hbm_reserve: int = 1 << 30,
+                 traj_batch_seeds: int = 1 << 20, iter_cap: int = 0, variant: int | None = None):
+        import threading
+        cfg = Config()
+        lib().collatz_config_default(C.byref(cfg))
+        cfg.maxbits, cfg.range_k, cfg.device, cfg.iter_cap = maxbits, range_k, device, iter_cap
+        if variant is not None:
+            cfg.variant = variant
+        sc = ServerConfig()
+        lib().collatz_server_config_default(C.byref(sc))
+        sc.max_active, sc.slice_items, sc.hbm_reserve = max_active, slice_items, hbm_reserve
+        sc.traj_batch_seeds = traj_batch_seeds
+        h = C.c_void_p()
+        rc = lib().collatz_server_start(C.byref(cfg), C.byref(sc), C.byref(h))
+        if rc:
+            raise CollatzError(rc, f"server_start: {status_string(rc)}")
+        self._h = h
+        self._bufs: dict[int, tuple] = {}
+        self._lock = threading.Lock()
+
+    def submit_range(self, offset: int, size: int, k: int = 0, mod9: bool = True) -> int:
+        q = RequestC()
+        q.kind = REQ_RANGE
+        q.range = make_range(offset, size, k, mod9)
+        t = C.c_uint64()
+        rc = lib().collatz_server_submit(self._h, C.byref(q), C.byref(t))
+        if rc:
+            raise CollatzError(rc, f"submit_range: {status_string(rc)}")
+        return t.value
+
+    def submit_trajectory_array(self, seeds) -> int:
+        """seeds: numpy (n, 8) uint32 limbs (kept alive until wait)."""
+        import numpy as np
+        seeds = np.ascontiguousarray(seeds, dtype=np.uint32)
+        n = seeds.shape[0]
+        st = np.zeros(n, dtype=np.uint64)
+        exc = np.zeros((n, 16), dtype=np.uint32)
+        status = np.zeros(n, dtype=np.uint32)
+        q = RequestC()
+        q.kind, q.nseeds = REQ_TRAJECTORY, n
+        q.seeds, q.stopping_time = seeds.ctypes.data, st.ctypes.data
+        q.excursion, q.status = exc.ctypes.data, status.ctypes.data
+        t = C.c_uint64()
+        with self._lock:
+            rc = lib().collatz_server_submit(self._h, C.byref(q), C.byref(t))
+            if rc:
+                raise CollatzError(rc, f"submit_trajectory: {status_string(rc)}")
+            self._bufs[t.value] = (seeds, st, exc, status)
+        return t.value
+
+    def submit_trajectory(self, seeds) -> int:
+        return self.submit_trajectory_array(seeds_array(seeds))
+
+    def wait(self, ticket: int, timeout: float | None = None) -> Response:
+        r = ResponseC()
+        rc = lib().collatz_server_wait(self._h, ticket, -1.0 if timeout is None else timeout, C.byref(r))
+        if rc == E_TIMEOUT or rc == E_ARG:
+            raise CollatzError(rc, f"wait({ticket}): {status_string(rc)}")
+        with self._lock:
+            bufs = self._bufs.pop(ticket, None)
+        out = Response(r.ticket, r.status, r.kind, submit_s=r.submit_s, admit_s=r.admit_s, done_s=r.done_s)
+        if r.kind == REQ_RANGE:
+            out.range = _range_result(r.range)
+        elif bufs is not None:
+            out.traj_status, out.traj_stopping_time, out.traj_excursion = bufs[3], bufs[1], bufs[2]
+        return out
+
+    def info(self) -> dict:
+        i = ServerInfoC()
+        rc = lib().collatz_server_info(self._h, C.byref(i))
+        if rc:
+            raise CollatzError(rc, "server_info")
+        return {name: getattr(i, name) for name, _ in ServerInfoC._fields_}
+
+    def stop(self):
+        if getattr(self, "_h", None):
+            lib().collatz_server_stop(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.stop()
+
+    def __del__(self):
+        try:
+            self.stop()
         except Exception:
             pass
 

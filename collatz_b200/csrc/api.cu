@@ -824,6 +824,7 @@ extern "C" int collatz_trajectory(collatz_ctx* c, const uint32_t* seeds, uint32_
     a.nseeds = n;
     a.index = c->t_idx[0].as<uint32_t>();
     a.nindex = (uint32_t)L.size();
+    a.nindex_dev = nullptr;
     a.st = c->t_st.as<unsigned long long>();
     a.exc = c->t_exc.as<uint32_t>();
     a.status = c->t_status.as<uint32_t>();

@@ -47,8 +47,11 @@ struct RangeSeg {
   uint32_t req;                   // request index (ReqRec)
   uint32_t kind;
   uint32_t mod9;                  // 1: apply the mod-9 sieve
+  // Item index within the original segment of item_begin (non-zero when a
+  // scheduler cuts a segment into slices; local indices stay < 2^32 for kind 0).
+  uint32_t local0_lo, local0_hi;
 };
-static_assert(sizeof(RangeSeg) == 56, "RangeSeg");
+static_assert(sizeof(RangeSeg) == 64, "RangeSeg");
 
 struct WidenEntry {  // a seed to re-run with wider limbs
   uint32_t req, n0, n1, n2;
@@ -87,7 +90,8 @@ struct TrajArgs {
   const uint32_t* seeds;       // nseeds x 8 limbs
   uint32_t nseeds;
   const uint32_t* index;       // optional: seeds to process (nullptr = all)
-  uint32_t nindex;
+  uint32_t nindex;             // capacity of index
+  const uint32_t* nindex_dev;  // optional: index length on the device (<= nindex)
   unsigned long long* st;      // out: stopping time
   uint32_t* exc;               // out: 16 limbs each
   uint32_t* status;            // out: 0 ok, 1 trivial, 2 overflow, 3 iteration cap

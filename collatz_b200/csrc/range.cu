@@ -159,7 +159,7 @@ __device__ __forceinline__ void stage_next(RangeWarp& W, const RangeArgs& A, con
   u32 chunk;
   const u32 kind = W.seg.kind;
   if (fresh) {
-    const ull local = next - W.seg_lo;
+    const ull local = next - W.seg_lo + (((ull)W.seg.local0_hi << 32) | W.seg.local0_lo);
     if (kind == 0) {  // segments hold fewer than 2^32 items
       const u32 l32 = (u32)local, ipq = W.seg.ipq;
       const u32 q32 = l32 / ipq;

@@ -1,0 +1,891 @@
+// server.cu -- serving mode: continuous batching of range verifications and
+// trajectory queries on one device (collatz_server_* in include/collatz.h).
+//
+// The server owns a context (sieve tables resident in HBM) and two worker
+// threads, each with its own stream:
+//   range thread  -- slices.  A slice is one launch of the persistent range
+//                    kernel over a work list cut from the admitted range
+//                    requests of one sieve exponent k (water-filling: requests
+//                    that need less than an equal share take what they need,
+//                    the rest of the slice budget goes to the larger ones),
+//                    followed by the 192- and 256-bit widening passes and a
+//                    copy of the request records.  Two slices are kept in
+//                    flight, so the next one is queued behind the running one
+//                    and the device does not wait for the host.  A request's
+//                    record lives in one device slot for its whole life, so
+//                    its maxima and counts accumulate over slices exactly as
+//                    in a single launch.
+//   query thread  -- trajectory batches (higher-priority stream).  Admitted
+//                    queries are concatenated into one batch: seeds are sorted
+//                    by bit length into limb classes on the host, and the chain
+//                    of class kernels hands seeds that need wider values to the
+//                    next class on the device (the counts stay on the device).
+//                    Two batches are kept in flight.  The host copies of a
+//                    batch (gathering seeds, scattering results into the
+//                    callers' buffers) run on this thread, off the range path.
+// Admission (arrival order within each kind) needs a free request slot and
+// free device memory: cudaMemGetInfo's free bytes plus this server's idle
+// pool memory, minus the bytes promised to admitted queries that have not
+// allocated yet, minus hbm_reserve.  A query needs 128 bytes per seed; a
+// range request needs its record slot only.  A request that could not fit
+// even on an otherwise empty device is refused (COLLATZ_E_ADMISSION); one
+// that does not fit now waits.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "runtime.h"
+
+using namespace cz;
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+constexpr int SLICE_DEPTH = 2;  // range slices in flight
+constexpr int BATCH_DEPTH = 2;  // trajectory batches in flight
+constexpr uint64_t TRAJ_BYTES_PER_SEED = 128;
+constexpr uint32_t MAX_ACTIVE_LIMIT = 4096;
+constexpr uint32_t MAX_BATCH_SEEDS = 1u << 22;
+// Staging reserved per admitted request for a slice's work list: a request
+// lowers to at most a dense part, two partial blocks and the full blocks
+// split into runs of < 2^32 items (17 runs for the largest request at
+// k = 24); more is allocated on demand.
+constexpr size_t SEGS_PER_REQ = 24;
+constexpr int NCLASS = 5;
+constexpr int CLASS_LIMBS[NCLASS] = {4, 6, 8, 12, 16};
+
+// host-time buckets of the worker threads
+enum { T_ADMIT, T_BUILD, T_COMPLETE, T_IDLE, T_N };
+
+struct Req {
+  uint64_t ticket = 0;
+  collatz_request q{};
+  int32_t status = COLLATZ_OK;
+  double submit_s = 0, admit_s = 0, done_s = 0;
+  // range requests
+  uint32_t k = 0, slot = 0;
+  std::vector<RangeSeg> segs;  // lowered work list, item_begin relative to the request
+  unsigned long long items = 0, cursor = 0;
+  size_t seg_i = 0;            // segment holding the cursor
+  collatz_range_result res{};
+  // trajectory queries
+  uint64_t dev_bytes = 0;
+  uint32_t batch_off = 0;
+};
+
+struct Slice {
+  DevBuf d_segs, d_cursor, d_widen[2], d_wcount;
+  HostBuf h_segs, h_recs;
+  std::vector<Req*> finishing;
+  cudaEvent_t t0 = nullptr, done = nullptr;
+  bool busy = false;
+};
+
+struct Batch {
+  HostBuf h_seeds, h_idx, h_cnt, h_st, h_exc, h_status;
+  std::vector<Req*> reqs;
+  std::vector<uint8_t> cls;
+  uint32_t n = 0;
+  cudaEvent_t done = nullptr;
+  bool busy = false;
+};
+
+double since(Clock::time_point t0) { return std::chrono::duration<double>(Clock::now() - t0).count(); }
+
+uint32_t seed_class(const uint32_t* w) {
+  uint32_t bl = 0;
+  for (int j = 7; j >= 0; j--)
+    if (w[j]) {
+      bl = 32u * j + (32u - __builtin_clz(w[j]));
+      break;
+    }
+  // the same classes as collatz_trajectory: a class of L limbs takes seeds
+  // that leave room for the value to grow before it is handed on
+  return bl <= 96 ? 0 : bl <= 160 ? 1 : bl <= 224 ? 2 : bl <= 352 ? 3 : 4;
+}
+
+}  // namespace
+
+struct collatz_server {
+  collatz_server_config cfg{};
+  collatz_ctx* ctx = nullptr;
+  cudaStream_t sa = nullptr, sb = nullptr;
+  cudaMemPool_t pool = nullptr;
+  Clock::time_point t0;
+  uint32_t grid = 0;
+  size_t total_mem = 0;
+
+  // guarded by mu
+  std::mutex mu;
+  std::condition_variable cv_range, cv_query, cv_done;
+  std::deque<Req*> pend_range, pend_query;
+  std::unordered_map<uint64_t, Req*> done;
+  std::unordered_map<uint64_t, Req*> known;  // tickets not yet collected
+  uint64_t next_ticket = 1;
+  bool stopping = false;
+  collatz_server_info_t info{};
+  double host_t[2][T_N] = {};  // [range, query thread][bucket]
+
+  std::atomic<uint32_t> active{0};  // admitted requests not yet complete
+
+  // admission budget (guarded by mb)
+  std::mutex mb;
+  int64_t budget = 0;
+  uint64_t promised = 0;  // admitted query bytes not yet allocated
+  Clock::time_point budget_read{};
+
+  // range thread only
+  std::vector<Req*> ranges;  // admitted range requests not yet complete
+  std::vector<uint32_t> free_slots;
+  DevBuf d_recs;
+  Slice slices[SLICE_DEPTH];
+  std::deque<int> slice_order;
+  // query thread only
+  std::deque<Req*> queries;  // admitted queries not yet in a batch
+  Batch batches[BATCH_DEPTH];
+  std::deque<int> batch_order;
+
+  std::thread thr_range, thr_query;
+};
+
+namespace {
+
+void publish(collatz_server* s, Req* r, int status) {
+  r->status = status;
+  r->done_s = since(s->t0);
+  std::lock_guard<std::mutex> g(s->mu);
+  s->done[r->ticket] = r;
+  s->info.completed++;
+  if (status == COLLATZ_E_ADMISSION) s->info.refused++;
+  s->cv_done.notify_all();
+}
+
+// Re-reads the device's free memory into the admission budget (caller holds
+// mb): free bytes plus this server's idle pool memory, minus the bytes
+// promised to admitted queries that have not allocated yet, minus
+// hbm_reserve.  Between reads each admission takes its bytes from the
+// budget and frees are not credited, so the budget never over-states what is
+// free.  The read is far slower than an admission, so it happens when a
+// request does not fit (at most every millisecond) and every 100 ms.
+void refresh_budget(collatz_server* s) {
+  size_t fr = 0, tot = 0;
+  s->budget_read = Clock::now();
+  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+    cudaGetLastError();
+    s->budget = -1;
+    return;
+  }
+  uint64_t reserved = 0, used = 0;
+  cudaMemPoolGetAttribute(s->pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+  cudaMemPoolGetAttribute(s->pool, cudaMemPoolAttrUsedMemCurrent, &used);
+  s->budget = (int64_t)fr + (int64_t)(reserved - used) - (int64_t)s->promised - (int64_t)s->cfg.hbm_reserve;
+  std::lock_guard<std::mutex> g(s->mu);
+  s->info.hbm_free = fr;
+  s->info.hbm_admitted = s->promised + used;
+}
+
+// Takes need bytes from the budget if they fit.
+bool take_budget(collatz_server* s, uint64_t need) {
+  std::lock_guard<std::mutex> g(s->mb);
+  const auto age = Clock::now() - s->budget_read;
+  if (age > std::chrono::milliseconds(100) || (s->budget < (int64_t)need && age > std::chrono::milliseconds(1)))
+    refresh_budget(s);
+  if (s->budget < (int64_t)need) return false;
+  s->budget -= (int64_t)need;
+  s->promised += need;
+  return true;
+}
+
+bool take_active(collatz_server* s) {
+  uint32_t a = s->active.load();
+  while (a < s->cfg.max_active)
+    if (s->active.compare_exchange_weak(a, a + 1)) return true;
+  return false;
+}
+
+// Next queued request of one kind, or nullptr.  Requests that could not fit
+// even on an otherwise empty device are refused on the way.
+Req* front(collatz_server* s, std::deque<Req*>& q, uint64_t need_per_seed) {
+  for (;;) {
+    Req* r = nullptr;
+    {
+      std::lock_guard<std::mutex> g(s->mu);
+      if (q.empty()) return nullptr;
+      r = q.front();
+      const uint64_t need = need_per_seed ? need_per_seed * r->q.nseeds + 256 : 0;
+      if ((int64_t)s->total_mem - (int64_t)s->cfg.hbm_reserve >= (int64_t)need) return r;
+      q.pop_front();
+    }
+    publish(s, r, COLLATZ_E_ADMISSION);
+  }
+}
+
+void pop_admitted(collatz_server* s, std::deque<Req*>& q, Req* r) {
+  r->admit_s = since(s->t0);
+  std::lock_guard<std::mutex> g(s->mu);
+  q.pop_front();
+  s->info.admitted++;
+}
+
+// ---------------------------------------------------------------------
+// range thread
+// ---------------------------------------------------------------------
+
+// Admits queued range requests in arrival order while request slots and
+// memory allow, and lowers them (the survivor table of their k is built on
+// first use and stays resident).
+void admit_ranges(collatz_server* s) {
+  collatz_ctx* c = s->ctx;
+  for (;;) {
+    Req* r = front(s, s->pend_range, 0);
+    if (!r || s->free_slots.empty()) return;
+    if (!take_active(s)) return;
+    if (!take_budget(s, 0)) {
+      s->active--;
+      return;
+    }
+    pop_admitted(s, s->pend_range, r);
+    r->k = r->q.range.k ? r->q.range.k : c->cfg.range_k;
+    RangeTables* T = nullptr;
+    int rc = get_range_tables(c, r->k, &T);
+    if (!rc) rc = lower_range(c, r->q.range, 0, *T, r->segs, r->items);
+    if (rc || r->items == 0) {  // an error, or no seed in the range
+      s->active--;
+      publish(s, r, rc);
+      continue;
+    }
+    r->slot = s->free_slots.back();
+    cudaError_t e = cudaMemsetAsync(s->d_recs.as<ReqRec>() + r->slot, 0, sizeof(ReqRec), s->sa);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      s->active--;
+      publish(s, r, COLLATZ_E_CUDA);
+      continue;
+    }
+    s->free_slots.pop_back();
+    s->ranges.push_back(r);
+  }
+}
+
+// Appends up to quota work items of r (from its cursor) to a slice.
+void take_items(Req* r, unsigned long long quota, std::vector<RangeSeg>& out, unsigned long long& slice_items) {
+  unsigned long long taken = 0;
+  while (taken < quota && r->seg_i < r->segs.size()) {
+    const RangeSeg& g = r->segs[r->seg_i];
+    const unsigned long long g_items =
+        ((r->seg_i + 1 < r->segs.size()) ? r->segs[r->seg_i + 1].item_begin : r->items) - g.item_begin;
+    const unsigned long long local = r->cursor - g.item_begin;
+    const unsigned long long n = std::min(g_items - local, quota - taken);
+    RangeSeg p = g;
+    p.item_begin = slice_items;
+    p.local0_lo = (uint32_t)local;
+    p.local0_hi = (uint32_t)(local >> 32);
+    p.req = r->slot;
+    out.push_back(p);
+    slice_items += n;
+    taken += n;
+    r->cursor += n;
+    if (local + n == g_items) r->seg_i++;
+  }
+}
+
+// Builds and enqueues one range slice.  Returns 1 if one was launched, 0 if
+// there is no range work, negative on error.
+int launch_slice(collatz_server* s, int si) {
+  // the sieve exponent of the oldest request with work left
+  uint32_t k = 0;
+  uint64_t oldest = ~0ull;
+  for (Req* r : s->ranges)
+    if (r->cursor < r->items && r->ticket < oldest) {
+      oldest = r->ticket;
+      k = r->k;
+    }
+  if (!k) return 0;
+  std::vector<std::pair<unsigned long long, Req*>> want;
+  for (Req* r : s->ranges)
+    if (r->cursor < r->items && r->k == k) want.push_back({r->items - r->cursor, r});
+  std::sort(want.begin(), want.end(),
+            [](const std::pair<unsigned long long, Req*>& a, const std::pair<unsigned long long, Req*>& b) {
+              return a.first != b.first ? a.first < b.first : a.second->ticket < b.second->ticket;
+            });
+  Slice& S = s->slices[si];
+  S.finishing.clear();
+  std::vector<RangeSeg> segs;
+  unsigned long long slice_items = 0, budget = s->cfg.slice_items;
+  for (size_t i = 0; i < want.size(); i++) {
+    const unsigned long long share = std::max<unsigned long long>(1, budget / (want.size() - i));
+    const unsigned long long q = std::min(want[i].first, share);
+    take_items(want[i].second, q, segs, slice_items);
+    budget -= std::min(budget, q);
+    if (want[i].second->cursor == want[i].second->items) S.finishing.push_back(want[i].second);
+  }
+  collatz_ctx* c = s->ctx;
+  RangeTables* T = nullptr;
+  int rc = get_range_tables(c, k, &T);
+  if (rc) return rc;
+  const size_t sb = sizeof(RangeSeg) * segs.size();
+  const size_t rb = sizeof(ReqRec) * s->cfg.max_active;
+  cudaError_t e = S.d_segs.ensure(sb);
+  if (!e) e = S.h_segs.ensure(sb);
+  if (!e) e = S.h_recs.ensure(rb);
+  if (e) return set_cuda_error(c, e, "server slice buffers");
+  std::memcpy(S.h_segs.p, segs.data(), sb);
+  RangeArgs a;
+  a.table = T->dev.table;
+  a.k = k;
+  a.segs = S.d_segs.as<RangeSeg>();
+  a.nsegs = (uint32_t)segs.size();
+  a.item_cursor = S.d_cursor.as<unsigned long long>();
+  a.item_limit = slice_items;
+  a.recs = s->d_recs.as<ReqRec>();
+  a.widen = S.d_widen[0].as<WidenEntry>();
+  a.widen_cap = WIDEN_CAP;
+  a.widen_count = S.d_wcount.as<uint32_t>();
+  a.iter_cap = c->iter_cap;
+  a.stats = nullptr;
+  cudaStream_t st = s->sa;
+  e = cudaMemcpyAsync(S.d_segs.p, S.h_segs.p, sb, cudaMemcpyHostToDevice, st);
+  if (!e) e = cudaMemsetAsync(S.d_cursor.p, 0, sizeof(unsigned long long), st);
+  if (!e) e = cudaMemsetAsync(S.d_wcount.p, 0, 2 * sizeof(uint32_t), st);
+  if (!e) e = cudaEventRecord(S.t0, st);
+  if (!e) e = launch_range(a, c->range_variant, s->grid, st);
+  if (!e)
+    e = launch_range_wide(S.d_widen[0].as<WidenEntry>(), S.d_wcount.as<uint32_t>(), WIDEN_CAP, 6, a.recs,
+                          S.d_widen[1].as<WidenEntry>(), WIDEN_CAP, S.d_wcount.as<uint32_t>() + 1, c->iter_cap, st);
+  if (!e)
+    e = launch_range_wide(S.d_widen[1].as<WidenEntry>(), S.d_wcount.as<uint32_t>() + 1, WIDEN_CAP, 8, a.recs,
+                          nullptr, 0, nullptr, c->iter_cap, st);
+  if (!e && !S.finishing.empty()) e = cudaMemcpyAsync(S.h_recs.p, s->d_recs.p, rb, cudaMemcpyDeviceToHost, st);
+  if (!e) e = cudaEventRecord(S.done, st);
+  if (e) return set_cuda_error(c, e, "server slice launch");
+  S.busy = true;
+  s->slice_order.push_back(si);
+  std::lock_guard<std::mutex> g(s->mu);
+  s->info.range_slices++;
+  return 1;
+}
+
+void complete_slice(collatz_server* s, int si) {
+  Slice& S = s->slices[si];
+  float ms = 0;
+  cudaEventElapsedTime(&ms, S.t0, S.done);
+  const ReqRec* recs = S.h_recs.as<ReqRec>();
+  uint64_t seeds = 0;
+  for (Req* r : S.finishing) {
+    rec_to_range_result(recs[r->slot], &r->res);
+    seeds += r->res.seeds_checked;
+    s->free_slots.push_back(r->slot);
+    s->ranges.erase(std::find(s->ranges.begin(), s->ranges.end(), r));
+    s->active--;
+    publish(s, r, r->res.status);
+  }
+  S.busy = false;
+  std::lock_guard<std::mutex> g(s->mu);
+  s->info.device_busy_s += ms / 1e3;
+  s->info.range_seeds_checked += seeds;
+}
+
+// ---------------------------------------------------------------------
+// query thread
+// ---------------------------------------------------------------------
+
+void admit_queries(collatz_server* s) {
+  for (;;) {
+    Req* r = front(s, s->pend_query, TRAJ_BYTES_PER_SEED);
+    if (!r) return;
+    const uint64_t need = TRAJ_BYTES_PER_SEED * r->q.nseeds + 256;
+    if (!take_active(s)) return;
+    if (!take_budget(s, need)) {
+      s->active--;
+      return;
+    }
+    pop_admitted(s, s->pend_query, r);
+    r->dev_bytes = need;
+    s->queries.push_back(r);
+  }
+}
+
+// Builds and enqueues one trajectory batch.  Returns 1 if one was launched,
+// 0 if there are no queries waiting, negative on error.
+int launch_batch(collatz_server* s, int bi) {
+  if (s->queries.empty()) return 0;
+  Batch& B = s->batches[bi];
+  B.reqs.clear();
+  uint64_t n = 0;
+  while (!s->queries.empty() &&
+         (B.reqs.empty() || n + s->queries.front()->q.nseeds <= s->cfg.traj_batch_seeds)) {
+    Req* r = s->queries.front();
+    s->queries.pop_front();
+    r->batch_off = (uint32_t)n;
+    n += r->q.nseeds;
+    B.reqs.push_back(r);
+  }
+  collatz_ctx* c = s->ctx;
+  B.n = (uint32_t)n;
+  // host: seeds into pinned memory, class lists (region j holds class j's
+  // own seeds followed by room for every seed of the narrower classes)
+  cudaError_t e = B.h_seeds.ensure(32 * n);
+  if (!e) e = B.h_idx.ensure(4 * NCLASS * n);
+  if (!e) e = B.h_cnt.ensure(64);
+  if (!e) e = B.h_st.ensure(8 * n);
+  if (!e) e = B.h_exc.ensure(64 * n);
+  if (!e) e = B.h_status.ensure(4 * n);
+  if (e) return set_cuda_error(c, e, "server batch buffers");
+  uint32_t* hs = B.h_seeds.as<uint32_t>();
+  for (Req* r : B.reqs) std::memcpy(hs + 8ull * r->batch_off, r->q.seeds, 32ull * r->q.nseeds);
+  uint32_t len[NCLASS] = {0, 0, 0, 0, 0};
+  B.cls.resize(n);
+  for (uint64_t i = 0; i < n; i++) len[B.cls[i] = (uint8_t)seed_class(hs + 8 * i)]++;
+  uint64_t base[NCLASS], cap[NCLASS], before = 0, off = 0;
+  for (int j = 0; j < NCLASS; j++) {
+    base[j] = off;
+    cap[j] = len[j] + before;
+    before += len[j];
+    off += cap[j];
+  }
+  uint32_t* hi = B.h_idx.as<uint32_t>();
+  uint64_t fill[NCLASS];
+  for (int j = 0; j < NCLASS; j++) fill[j] = base[j];
+  for (uint64_t i = 0; i < n; i++) hi[fill[B.cls[i]]++] = (uint32_t)i;
+  uint32_t* hc = B.h_cnt.as<uint32_t>();
+  for (int j = 0; j < 16; j++) hc[j] = 0;
+  for (int j = 0; j < NCLASS; j++) hc[j] = len[j];  // [0..4] list lengths, [8..12] cursors
+  // device: one block from the server's pool, freed in stream order
+  const uint64_t o_st = 32 * n, o_exc = o_st + 8 * n, o_status = o_exc + 64 * n, o_idx = o_status + 4 * n,
+                 o_cnt = (o_idx + 4 * off + 255) & ~255ull, bytes = o_cnt + 64;
+  cudaStream_t st = s->sb;
+  void* block = nullptr;
+  e = cudaMallocFromPoolAsync(&block, bytes, s->pool, st);
+  if (e) return set_cuda_error(c, e, "server batch allocation");
+  {
+    uint64_t promised = 0;
+    for (Req* r : B.reqs) promised += r->dev_bytes;
+    std::lock_guard<std::mutex> g(s->mb);
+    s->promised -= std::min(s->promised, promised);
+  }
+  char* d = static_cast<char*>(block);
+  e = cudaMemcpyAsync(d, hs, 32 * n, cudaMemcpyHostToDevice, st);
+  if (!e) e = cudaMemcpyAsync(d + o_idx, hi, 4 * off, cudaMemcpyHostToDevice, st);
+  if (!e) e = cudaMemcpyAsync(d + o_cnt, hc, 64, cudaMemcpyHostToDevice, st);
+  uint32_t* cnt = reinterpret_cast<uint32_t*>(d + o_cnt);
+  uint32_t* idx = reinterpret_cast<uint32_t*>(d + o_idx);
+  uint64_t reach = 0;  // seeds that may arrive in class j
+  for (int j = 0; j < NCLASS && !e; j++) {
+    reach += len[j];
+    if (reach == 0) continue;
+    TrajArgs a;
+    a.seeds = reinterpret_cast<const uint32_t*>(d);
+    a.nseeds = (uint32_t)n;
+    a.index = idx + base[j];
+    a.nindex = (uint32_t)cap[j];
+    a.nindex_dev = cnt + j;
+    a.st = reinterpret_cast<unsigned long long*>(d + o_st);
+    a.exc = reinterpret_cast<uint32_t*>(d + o_exc);
+    a.status = reinterpret_cast<uint32_t*>(d + o_status);
+    a.next = (j + 1 < NCLASS) ? idx + base[j + 1] : nullptr;
+    a.next_count = (j + 1 < NCLASS) ? cnt + j + 1 : cnt + 15;
+    a.cursor = cnt + 8 + j;
+    a.iter_cap = c->iter_cap;
+    const uint32_t grid = (uint32_t)std::min<uint64_t>((reach + 127) / 128, (uint64_t)c->sm_count * 8);
+    e = launch_traj(a, CLASS_LIMBS[j], grid, st);
+  }
+  if (!e) e = cudaMemcpyAsync(B.h_st.p, d + o_st, 8 * n, cudaMemcpyDeviceToHost, st);
+  if (!e) e = cudaMemcpyAsync(B.h_exc.p, d + o_exc, 64 * n, cudaMemcpyDeviceToHost, st);
+  if (!e) e = cudaMemcpyAsync(B.h_status.p, d + o_status, 4 * n, cudaMemcpyDeviceToHost, st);
+  const cudaError_t ef = cudaFreeAsync(block, st);
+  if (!e) e = ef;
+  if (!e) e = cudaEventRecord(B.done, st);
+  if (e) return set_cuda_error(c, e, "server batch launch");
+  B.busy = true;
+  s->batch_order.push_back(bi);
+  std::lock_guard<std::mutex> g(s->mu);
+  s->info.traj_batches++;
+  return 1;
+}
+
+void complete_batch(collatz_server* s, int bi) {
+  Batch& B = s->batches[bi];
+  for (Req* r : B.reqs) {
+    const uint64_t o = r->batch_off, m = r->q.nseeds;
+    std::memcpy(r->q.stopping_time, B.h_st.as<uint64_t>() + o, 8 * m);
+    std::memcpy(r->q.excursion, B.h_exc.as<uint32_t>() + 16 * o, 64 * m);
+    std::memcpy(r->q.status, B.h_status.as<uint32_t>() + o, 4 * m);
+    s->active--;
+    publish(s, r, COLLATZ_OK);
+  }
+  B.reqs.clear();
+  B.busy = false;
+  std::lock_guard<std::mutex> g(s->mu);
+  s->info.traj_seeds += B.n;
+}
+
+// ---------------------------------------------------------------------
+// worker loops
+// ---------------------------------------------------------------------
+
+// Fails every request a worker holds or that is queued for it (after a
+// device error); the server then accepts no more requests.
+void fail_worker(collatz_server* s, bool range_side, int rc) {
+  std::vector<Req*> all;
+  if (range_side) {
+    all.assign(s->ranges.begin(), s->ranges.end());
+    s->ranges.clear();
+  } else {
+    all.assign(s->queries.begin(), s->queries.end());
+    s->queries.clear();
+    for (Batch& B : s->batches) {
+      all.insert(all.end(), B.reqs.begin(), B.reqs.end());
+      B.reqs.clear();
+    }
+  }
+  std::deque<Req*> pend;
+  {
+    std::lock_guard<std::mutex> g(s->mu);
+    pend.swap(range_side ? s->pend_range : s->pend_query);
+    s->stopping = true;
+  }
+  for (Req* r : all) {
+    s->active--;
+    publish(s, r, rc);
+  }
+  for (Req* r : pend) publish(s, r, rc);
+  s->cv_range.notify_all();
+  s->cv_query.notify_all();
+}
+
+template <class Work>
+void worker(collatz_server* s, bool range_side, Work work) {
+  cudaSetDevice(s->ctx->device);
+  double t[T_N] = {};
+  std::deque<Req*>& pend = range_side ? s->pend_range : s->pend_query;
+  std::condition_variable& cv = range_side ? s->cv_range : s->cv_query;
+  for (;;) {
+    Clock::time_point t_start = Clock::now();
+    bool busy_device = false;
+    {
+      std::unique_lock<std::mutex> g(s->mu);
+      if (s->stopping) {  // queued requests are not started after stop
+        for (Req* r : pend) {
+          r->status = COLLATZ_E_STATE;
+          r->done_s = since(s->t0);
+          s->done[r->ticket] = r;
+          s->info.completed++;
+        }
+        pend.clear();
+        s->cv_done.notify_all();
+      }
+      const bool held = range_side ? (!s->ranges.empty() || !s->slice_order.empty())
+                                   : (!s->queries.empty() || !s->batch_order.empty());
+      if (!held && s->stopping) return;
+      if (!held && pend.empty()) cv.wait_for(g, std::chrono::milliseconds(50));
+      s->info.loops++;
+      for (int i = 0; i < T_N; i++) s->host_t[range_side ? 0 : 1][i] = t[i];
+    }
+    Clock::time_point tp = Clock::now();
+    t[T_IDLE] += std::chrono::duration<double>(tp - t_start).count();
+    const int rc = work(t, tp, busy_device);
+    if (rc < 0) {
+      cudaStreamSynchronize(range_side ? s->sa : s->sb);
+      if (range_side) s->slice_order.clear(); else s->batch_order.clear();
+      fail_worker(s, range_side, rc);
+      return;
+    }
+    if (!rc && busy_device) {  // nothing happened: wait for the device or a new request
+      const Clock::time_point tw = Clock::now();
+      std::unique_lock<std::mutex> g(s->mu);
+      cv.wait_for(g, std::chrono::microseconds(50));
+      t[T_IDLE] += std::chrono::duration<double>(Clock::now() - tw).count();
+    }
+  }
+}
+
+void lap(double* t, int bucket, Clock::time_point& tp) {
+  const Clock::time_point n = Clock::now();
+  t[bucket] += std::chrono::duration<double>(n - tp).count();
+  tp = n;
+}
+
+// One pass of a worker: admit, launch, complete.  Returns < 0 on a device
+// error, 1 if anything happened, 0 otherwise (busy_device: work in flight).
+int range_pass(collatz_server* s, double* t, Clock::time_point tp, bool& busy_device) {
+  int did = 0;
+  admit_ranges(s);
+  lap(t, T_ADMIT, tp);
+  for (int i = 0; i < SLICE_DEPTH; i++)
+    if (!s->slices[i].busy) {
+      const int rc = launch_slice(s, i);
+      if (rc < 0) return rc;
+      if (rc == 0) break;
+      did = 1;
+    }
+  lap(t, T_BUILD, tp);
+  while (!s->slice_order.empty()) {
+    const cudaError_t q = cudaEventQuery(s->slices[s->slice_order.front()].done);
+    if (q == cudaErrorNotReady) break;
+    if (q != cudaSuccess) return set_cuda_error(s->ctx, q, "range slice");
+    complete_slice(s, s->slice_order.front());
+    s->slice_order.pop_front();
+    did = 1;
+  }
+  lap(t, T_COMPLETE, tp);
+  busy_device = !s->slice_order.empty();
+  return did;
+}
+
+int query_pass(collatz_server* s, double* t, Clock::time_point tp, bool& busy_device) {
+  int did = 0;
+  admit_queries(s);
+  lap(t, T_ADMIT, tp);
+  for (int i = 0; i < BATCH_DEPTH; i++)
+    if (!s->batches[i].busy) {
+      const int rc = launch_batch(s, i);
+      if (rc < 0) return rc;
+      if (rc == 0) break;
+      did = 1;
+    }
+  lap(t, T_BUILD, tp);
+  while (!s->batch_order.empty()) {
+    const cudaError_t q = cudaEventQuery(s->batches[s->batch_order.front()].done);
+    if (q == cudaErrorNotReady) break;
+    if (q != cudaSuccess) return set_cuda_error(s->ctx, q, "trajectory batch");
+    complete_batch(s, s->batch_order.front());
+    s->batch_order.pop_front();
+    did = 1;
+  }
+  lap(t, T_COMPLETE, tp);
+  busy_device = !s->batch_order.empty();
+  return did;
+}
+
+void destroy(collatz_server* s) {
+  if (!s) return;
+  if (s->ctx) {
+    cudaSetDevice(s->ctx->device);
+    if (s->sa) cudaStreamSynchronize(s->sa);
+    if (s->sb) cudaStreamSynchronize(s->sb);
+    for (Slice& S : s->slices) {
+      S.d_segs.release();
+      S.d_cursor.release();
+      S.d_widen[0].release();
+      S.d_widen[1].release();
+      S.d_wcount.release();
+      S.h_segs.release();
+      S.h_recs.release();
+      if (S.t0) cudaEventDestroy(S.t0);
+      if (S.done) cudaEventDestroy(S.done);
+    }
+    for (Batch& B : s->batches) {
+      B.h_seeds.release();
+      B.h_idx.release();
+      B.h_cnt.release();
+      B.h_st.release();
+      B.h_exc.release();
+      B.h_status.release();
+      if (B.done) cudaEventDestroy(B.done);
+    }
+    s->d_recs.release();
+    if (s->sa) cudaStreamDestroy(s->sa);
+    if (s->sb) cudaStreamDestroy(s->sb);
+    if (s->pool) cudaMemPoolDestroy(s->pool);
+    collatz_destroy(s->ctx);
+  }
+  for (auto& kv : s->known) delete kv.second;
+  delete s;
+}
+
+}  // namespace
+
+extern "C" void collatz_server_config_default(collatz_server_config* c) {
+  if (!c) return;
+  std::memset(c, 0, sizeof *c);
+  c->max_active = 256;
+  c->slice_items = 1u << 19;  // ~1 ms of device work at k = 24
+  c->hbm_reserve = 1ull << 30;
+  c->traj_batch_seeds = 1u << 20;
+}
+
+extern "C" int collatz_server_start(const collatz_config* cfg, const collatz_server_config* scfg,
+                                    collatz_server** out) {
+  if (!out) return COLLATZ_E_ARG;
+  *out = nullptr;
+  collatz_server* s = new collatz_server();
+  if (scfg) s->cfg = *scfg; else collatz_server_config_default(&s->cfg);
+  if (s->cfg.max_active == 0 || s->cfg.max_active > MAX_ACTIVE_LIMIT || s->cfg.slice_items == 0 ||
+      s->cfg.traj_batch_seeds == 0 || s->cfg.traj_batch_seeds > MAX_BATCH_SEEDS) {
+    delete s;
+    return COLLATZ_E_ARG;
+  }
+  int rc = collatz_create(cfg, &s->ctx);
+  if (rc) {
+    delete s;
+    return rc;
+  }
+  collatz_ctx* c = s->ctx;
+  auto fail = [&](cudaError_t e, const char* where) {
+    set_cuda_error(c, e, where);
+    destroy(s);
+    return COLLATZ_E_CUDA;
+  };
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e) return fail(e, "cudaSetDevice");
+  int lo = 0, hi = 0;
+  cudaDeviceGetStreamPriorityRange(&lo, &hi);
+  if ((e = cudaStreamCreateWithPriority(&s->sa, cudaStreamNonBlocking, lo))) return fail(e, "stream");
+  if ((e = cudaStreamCreateWithPriority(&s->sb, cudaStreamNonBlocking, hi))) return fail(e, "stream");
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = c->device;
+  if ((e = cudaMemPoolCreate(&s->pool, &props))) return fail(e, "cudaMemPoolCreate");
+  uint64_t keep = 1ull << 30;  // idle pool memory kept for the next batches
+  cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  if ((e = s->d_recs.ensure(sizeof(ReqRec) * s->cfg.max_active))) return fail(e, "server records");
+  for (Slice& S : s->slices) {
+    if ((e = S.d_cursor.ensure(sizeof(unsigned long long)))) return fail(e, "slice");
+    if ((e = S.d_widen[0].ensure(sizeof(WidenEntry) * WIDEN_CAP))) return fail(e, "slice");
+    if ((e = S.d_widen[1].ensure(sizeof(WidenEntry) * WIDEN_CAP))) return fail(e, "slice");
+    if ((e = S.d_wcount.ensure(2 * sizeof(uint32_t)))) return fail(e, "slice");
+    if ((e = cudaEventCreate(&S.t0))) return fail(e, "event");
+    if ((e = cudaEventCreate(&S.done))) return fail(e, "event");
+  }
+  // Host and device staging is allocated here, once: growing a pinned or
+  // device buffer later (cudaFreeHost / cudaFree synchronise the device,
+  // large cudaMallocHost calls take milliseconds) would stall both workers.
+  const size_t seg_bytes = sizeof(RangeSeg) * SEGS_PER_REQ * s->cfg.max_active;
+  for (Slice& S : s->slices) {
+    if ((e = S.d_segs.ensure(seg_bytes))) return fail(e, "slice");
+    if ((e = S.h_segs.ensure(seg_bytes))) return fail(e, "slice");
+    if ((e = S.h_recs.ensure(sizeof(ReqRec) * s->cfg.max_active))) return fail(e, "slice");
+  }
+  const uint64_t nb = s->cfg.traj_batch_seeds;
+  for (Batch& B : s->batches) {
+    if ((e = cudaEventCreateWithFlags(&B.done, cudaEventDisableTiming))) return fail(e, "event");
+    if ((e = B.h_seeds.ensure(32 * nb))) return fail(e, "batch");
+    if ((e = B.h_idx.ensure(4 * NCLASS * nb))) return fail(e, "batch");
+    if ((e = B.h_cnt.ensure(64))) return fail(e, "batch");
+    if ((e = B.h_st.ensure(8 * nb))) return fail(e, "batch");
+    if ((e = B.h_exc.ensure(64 * nb))) return fail(e, "batch");
+    if ((e = B.h_status.ensure(4 * nb))) return fail(e, "batch");
+    B.cls.reserve(nb);
+  }
+  int bps = 0;
+  if (range_occupancy(c->range_variant, &bps) != cudaSuccess || bps <= 0) bps = 1;
+  s->grid = (uint32_t)(bps * c->sm_count);
+  size_t fr = 0;
+  if ((e = cudaMemGetInfo(&fr, &s->total_mem))) return fail(e, "cudaMemGetInfo");
+  {
+    std::lock_guard<std::mutex> g(s->mb);
+    refresh_budget(s);
+  }
+  for (uint32_t i = s->cfg.max_active; i-- > 0;) s->free_slots.push_back(i);
+  s->t0 = Clock::now();
+  s->thr_range = std::thread([s] { worker(s, true, [s](double* t, Clock::time_point tp, bool& b) {
+                                       return range_pass(s, t, tp, b);
+                                     }); });
+  s->thr_query = std::thread([s] { worker(s, false, [s](double* t, Clock::time_point tp, bool& b) {
+                                       return query_pass(s, t, tp, b);
+                                     }); });
+  *out = s;
+  return COLLATZ_OK;
+}
+
+extern "C" int collatz_server_submit(collatz_server* s, const collatz_request* q, uint64_t* ticket) {
+  if (!s || !q || !ticket) return COLLATZ_E_ARG;
+  if (q->kind == COLLATZ_REQ_RANGE) {
+    const uint32_t k = q->range.k;
+    if (k && (k < 8 || k > 34)) return COLLATZ_E_ARG;
+    const unsigned __int128 o = ((unsigned __int128)q->range.offset[1] << 64) | q->range.offset[0];
+    if (q->range.size > (1ull << 48) || o + q->range.size > ((unsigned __int128)1 << 96)) return COLLATZ_E_LIMIT;
+  } else if (q->kind == COLLATZ_REQ_TRAJECTORY) {
+    if (!q->nseeds || !q->seeds || !q->stopping_time || !q->excursion || !q->status) return COLLATZ_E_ARG;
+    if (q->nseeds > s->cfg.traj_batch_seeds) return COLLATZ_E_LIMIT;
+  } else {
+    return COLLATZ_E_ARG;
+  }
+  Req* r = new Req();
+  r->q = *q;
+  r->submit_s = since(s->t0);
+  const bool is_range = q->kind == COLLATZ_REQ_RANGE;
+  {
+    std::lock_guard<std::mutex> g(s->mu);
+    if (s->stopping) {
+      delete r;
+      return COLLATZ_E_STATE;
+    }
+    r->ticket = s->next_ticket++;
+    s->known[r->ticket] = r;
+    (is_range ? s->pend_range : s->pend_query).push_back(r);
+    s->info.submitted++;
+  }
+  (is_range ? s->cv_range : s->cv_query).notify_one();
+  *ticket = r->ticket;
+  return COLLATZ_OK;
+}
+
+extern "C" int collatz_server_wait(collatz_server* s, uint64_t ticket, double timeout_s, collatz_response* resp) {
+  if (!s) return COLLATZ_E_ARG;
+  std::unique_lock<std::mutex> g(s->mu);
+  if (!s->known.count(ticket)) return COLLATZ_E_ARG;
+  auto ready = [&] { return s->done.count(ticket) != 0; };
+  if (timeout_s < 0) {
+    s->cv_done.wait(g, ready);
+  } else if (!s->cv_done.wait_for(g, std::chrono::duration<double>(timeout_s), ready)) {
+    return COLLATZ_E_TIMEOUT;
+  }
+  Req* r = s->done[ticket];
+  s->done.erase(ticket);
+  s->known.erase(ticket);
+  g.unlock();
+  if (resp) {
+    std::memset(resp, 0, sizeof *resp);
+    resp->ticket = r->ticket;
+    resp->status = r->status;
+    resp->kind = r->q.kind;
+    resp->range = r->res;
+    resp->range.status = r->status;
+    resp->submit_s = r->submit_s;
+    resp->admit_s = r->admit_s;
+    resp->done_s = r->done_s;
+  }
+  const int st = r->status;
+  delete r;
+  return st;
+}
+
+extern "C" int collatz_server_info(collatz_server* s, collatz_server_info_t* info) {
+  if (!s || !info) return COLLATZ_E_ARG;
+  std::lock_guard<std::mutex> g(s->mu);
+  *info = s->info;
+  info->pending = (uint32_t)(s->pend_range.size() + s->pend_query.size());
+  info->active = s->active.load();
+  info->host_admit_s = s->host_t[0][T_ADMIT] + s->host_t[1][T_ADMIT];
+  info->host_slice_s = s->host_t[0][T_BUILD];
+  info->host_batch_s = s->host_t[1][T_BUILD];
+  info->host_complete_s = s->host_t[0][T_COMPLETE] + s->host_t[1][T_COMPLETE];
+  info->host_idle_s = s->host_t[0][T_IDLE] + s->host_t[1][T_IDLE];
+  return COLLATZ_OK;
+}
+
+extern "C" int collatz_server_stop(collatz_server* s) {
+  if (!s) return COLLATZ_E_ARG;
+  {
+    std::lock_guard<std::mutex> g(s->mu);
+    s->stopping = true;
+  }
+  s->cv_range.notify_all();
+  s->cv_query.notify_all();
+  if (s->thr_range.joinable()) s->thr_range.join();
+  if (s->thr_query.joinable()) s->thr_query.join();
+  destroy(s);
+  return COLLATZ_OK;
+}

@@ -28,7 +28,7 @@ __global__ void __launch_bounds__(128) k_traj(const TrajArgs A) {
     s_pow3[threadIdx.x] = p;
   }
   __syncthreads();
-  const u32 count = A.index ? A.nindex : A.nseeds;
+  const u32 count = A.index ? (A.nindex_dev ? min(*A.nindex_dev, A.nindex) : A.nindex) : A.nseeds;
   u32 slot = atomicAdd(A.cursor, 1u);
   bool active = false;
   Limbs<L> v, N, E;

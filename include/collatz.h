@@ -201,6 +201,82 @@ int collatz_range_sieve(collatz_ctx *ctx, uint32_t k, uint8_t *bits, uint64_t *c
 int collatz_trajectory(collatz_ctx *ctx, const uint32_t *seeds, uint32_t n, uint64_t *stopping_time,
                        uint32_t *excursion, uint32_t *status);
 
+/* ------------------------------------------------------------------ */
+/* Serving (new entry mode): continuous batching of range requests and */
+/* trajectory queries on one device.                                   */
+/* ------------------------------------------------------------------ */
+/* A scheduler thread admits requests in arrival order while request
+ * slots and free device memory allow (cudaMemGetInfo minus hbm_reserve),
+ * cuts the admitted range requests into slices of work items that share
+ * one persistent range launch (small requests take what they need, the
+ * rest of the slice goes to the large ones), runs trajectory queries as
+ * concatenated batches on a second stream so both overlap on the device,
+ * and completes each request as soon as its last slice or batch is done.
+ * Every result is identical to the same request run alone. */
+typedef struct collatz_server collatz_server;
+
+enum { COLLATZ_REQ_RANGE = 0, COLLATZ_REQ_TRAJECTORY = 1 };
+
+typedef struct {
+  uint32_t max_active;        /* requests admitted at once; default 256, at most 4096 */
+  uint32_t slice_items;       /* work items (64 survivor entries) per range slice; default 1 << 19 */
+  uint64_t hbm_reserve;       /* device bytes that admission leaves free; default 1 GiB */
+  uint32_t traj_batch_seeds;  /* seeds per trajectory batch (and per query); default 1 << 20, at
+                                 most 1 << 22; the server pins 2 x 128 bytes per batch seed */
+  uint32_t reserved[7];
+} collatz_server_config;
+
+typedef struct {
+  uint32_t kind;               /* COLLATZ_REQ_* */
+  uint32_t nseeds;             /* trajectory: number of seeds (1 .. traj_batch_seeds) */
+  collatz_range range;         /* range request */
+  /* trajectory: nseeds x 8 uint32 limbs in, outputs as collatz_trajectory;
+   * the caller keeps all four buffers alive until collatz_server_wait
+   * has returned this request's response. */
+  const uint32_t *seeds;
+  uint64_t *stopping_time;
+  uint32_t *excursion;
+  uint32_t *status;
+} collatz_request;
+
+typedef struct {
+  uint64_t ticket;
+  int32_t status;              /* COLLATZ_OK, COLLATZ_E_ADMISSION, COLLATZ_E_DEVICE, ... */
+  uint32_t kind;
+  collatz_range_result range;  /* range requests */
+  double submit_s, admit_s, done_s; /* server clock (seconds since start) */
+} collatz_response;
+
+typedef struct {
+  uint64_t submitted, admitted, completed, refused;
+  uint64_t range_slices, traj_batches;
+  uint64_t range_seeds_checked, traj_seeds;
+  uint32_t active, pending;
+  uint64_t hbm_free;           /* cudaMemGetInfo free bytes at the last admission pass */
+  uint64_t hbm_admitted;       /* device bytes held by admitted requests */
+  double device_busy_s;        /* summed device time of range slices */
+  /* scheduler thread: loop iterations and host seconds spent admitting,
+   * building slices, building batches, completing requests, and idle */
+  uint64_t loops;
+  double host_admit_s, host_slice_s, host_batch_s, host_complete_s, host_idle_s;
+} collatz_server_info_t;
+
+void collatz_server_config_default(collatz_server_config *scfg);
+/* Creates a context for cfg->device (tables built and kept resident) and
+ * starts the scheduler thread. */
+int collatz_server_start(const collatz_config *cfg, const collatz_server_config *scfg, collatz_server **out);
+/* Thread-safe.  Validates the request (COLLATZ_E_ARG / COLLATZ_E_LIMIT)
+ * and queues it; *ticket identifies its response. */
+int collatz_server_submit(collatz_server *s, const collatz_request *req, uint64_t *ticket);
+/* Thread-safe.  Waits up to timeout_s (< 0: forever) for a ticket's
+ * response, fills *resp and forgets the ticket.  Returns the request's
+ * status, COLLATZ_E_TIMEOUT, or COLLATZ_E_ARG for an unknown ticket. */
+int collatz_server_wait(collatz_server *s, uint64_t ticket, double timeout_s, collatz_response *resp);
+int collatz_server_info(collatz_server *s, collatz_server_info_t *info);
+/* Finishes the work on the device, fails queued requests with
+ * COLLATZ_E_STATE, joins the scheduler and frees the server. */
+int collatz_server_stop(collatz_server *s);
+
 /* Kernel variants for the autotuner. */
 int collatz_variant_count(int mode); /* mode 0 cases, 1 range */
 int collatz_set_variant(collatz_ctx *ctx, int mode, int variant);
