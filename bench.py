@@ -32,6 +32,14 @@ sys.path.insert(0, ROOT)
 OFFSET = 1 << 40
 SIZE_LOG2 = 38
 K_SIEVE = 24
+# Range workloads: the single large block (the headline) and the frontier
+# block (2^40 seeds at 2^60 with the 2^34-bit sieve resident in HBM).
+WORKLOADS = {
+    "block": {"offset": OFFSET, "offset_log2": 40, "k": K_SIEVE, "size_log2": SIZE_LOG2,
+              "name": "single large block"},
+    "frontier": {"offset": 1 << 60, "offset_log2": 60, "k": 34, "size_log2": 40,
+                 "name": "frontier block"},
+}
 METRIC = "seeds verified/s"
 UNIT = "seeds/s"
 # Algorithmic 32-bit integer operations per surviving seed (L = 4 limbs):
@@ -123,15 +131,17 @@ def run_reference(args):
     if rank != 0:
         return 0
     from oracle import oracle as O
+    wl = WORKLOADS[args.workload]
+    base, ksv = wl["offset"], wl["k"]
     nthreads = os.cpu_count() or 1
     # one step = a bounded sample of the workload (the full block takes CPU-hours)
-    rate, size, _ = cpu_sample(OFFSET, 2.0, K_SIEVE, nthreads, max_log2=32)
+    rate, size, _ = cpu_sample(base, 2.0, ksv, nthreads, max_log2=32)
     for _ in range(args.warmup):
-        O.range_verify(OFFSET, size, K_SIEVE, True, 1, nthreads)
+        O.range_verify(base, size, ksv, True, 1, nthreads)
     times = []
     for i in range(args.steps):
         t0 = time.perf_counter()
-        O.range_verify(OFFSET + i * size, size, K_SIEVE, True, 1, nthreads)
+        O.range_verify(base + i * size, size, ksv, True, 1, nthreads)
         times.append(time.perf_counter() - t0)
     tot = sum(times)
     value = size * args.steps / tot
@@ -139,12 +149,14 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u128",
             "data": "synthetic (deterministic seed range)",
-            "config": {"workload": f"range [2^40 + i*S, 2^40 + (i+1)*S), S = {size} (bounded sample of "
-                                   f"the 2^38 block), k={K_SIEVE} sieve + mod-9",
-                       "k": K_SIEVE, "sample_size": size},
+            "config": {"workload": f"range [2^{wl['offset_log2']} + i*S, 2^{wl['offset_log2']} + (i+1)*S), "
+                                   f"S = {size} (bounded sample of the 2^{args.size_log2 or wl['size_log2']} "
+                                   f"{wl['name']}), k={ksv} sieve + mod-9",
+                       "k": ksv, "sample_size": size},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
-                             "sample": f"{args.steps} x {size} seeds at 2^40 (oracle/collatz_oracle.c "
-                                       f"run-length loop after cu:684-715, {nthreads} threads)"},
+                             "sample": f"{args.steps} x {size} seeds at 2^{wl['offset_log2']} "
+                                       "(oracle/collatz_oracle.c run-length loop after cu:684-715, "
+                                       f"{nthreads} threads)"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -306,8 +318,10 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--size-log2", type=int, default=SIZE_LOG2,
-                    help="block size (default 38, the benchmark configuration)")
+    ap.add_argument("--workload", default="block", choices=sorted(WORKLOADS),
+                    help="block: [2^40, 2^40 + 2^38), k = 24 (default); frontier: [2^60, 2^60 + 2^40), k = 34")
+    ap.add_argument("--size-log2", type=int, default=None,
+                    help="seeds per GPU as a power of two (default: the workload's, 38 or 40)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched and served measurements (run at N = 1 only)")
@@ -330,12 +344,18 @@ def main():
     torch.cuda.set_device(local)
     import collatz_b200 as cb
 
+    wl = WORKLOADS[args.workload]
+    base, ksv = wl["offset"], wl["k"]
+    if args.size_log2 is None:
+        args.size_log2 = wl["size_log2"]
     size = 1 << args.size_log2
-    off = OFFSET + rank * size
-    v = cb.Verifier(26, range_k=K_SIEVE, device=local, variant=args.variant)
+    off = base + rank * size
+    v = cb.Verifier(26, range_k=ksv, device=local, variant=args.variant)
     stream = torch.cuda.Stream(device=local)
     v.set_stream(stream.cuda_stream)
-    plan = v.plan([(off, size, K_SIEVE, True)])
+    t_tab = time.perf_counter()
+    plan = v.plan([(off, size, ksv, True)])  # builds the k-sieve tables on first use
+    t_tab = time.perf_counter() - t_tab
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
     sm_count, _ = v.device_info()
 
@@ -383,7 +403,7 @@ def main():
     for i in range(2 + max(1, min(args.steps, 3))):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        e2e_res = v.verify_range(off, size, K_SIEVE)
+        e2e_res = v.verify_range(off, size, ksv)
         e2e_times.append(time.perf_counter() - t0)
     e2e_s = statistics.median(e2e_times[2:])
     if pg:
@@ -396,7 +416,7 @@ def main():
         from oracle import oracle as O
         # algorithmic work per step: survivors x ops, runs per survivor from the
         # oracle's jump+runs model on a fixed sample of this workload
-        samp = O.range_verify(OFFSET, 1 << 24, K_SIEVE, True, 2, min(8, os.cpu_count() or 1))
+        samp = O.range_verify(base, 1 << 24, ksv, True, 2, min(8, os.cpu_count() or 1))
         odd_per = samp.odd_runs / samp.seeds
         even_per = samp.even_runs / samp.seeds
         ops_per_seed = OPS_JUMP + OPS_ODD * odd_per + OPS_EVEN * even_per
@@ -410,11 +430,13 @@ def main():
             "warmup": args.warmup, "ms_per_step": 1e3 * dev_s / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic (deterministic seed range)",
-            "config": {"workload": f"range [2^40 + r*2^{args.size_log2}, 2^40 + (r+1)*2^{args.size_log2}) "
-                                   f"per rank r, k={K_SIEVE} residue sieve + mod-9 sieve, 128-bit limbs "
-                                   "widening to 192/256, plain kernel (single large block)",
-                       "offset": OFFSET, "size_per_gpu": size, "k": K_SIEVE,
+            "config": {"workload": f"range [2^{wl['offset_log2']} + r*2^{args.size_log2}, "
+                                   f"2^{wl['offset_log2']} + (r+1)*2^{args.size_log2}) per rank r, k={ksv} "
+                                   "residue sieve + mod-9 sieve, 128-bit limbs widening to 192/256, plain "
+                                   f"kernel ({wl['name']})",
+                       "offset": base, "size_per_gpu": size, "k": ksv,
                        "survivors_per_step_per_gpu": res.seeds_checked,
+                       "table_build_s": t_tab,
                        "l2": "flushed between steps (256 MiB write, outside the timed events)",
                        "parallelism": f"replicas over disjoint blocks x{world}",
                        "kernel_variant": args.variant},
@@ -424,17 +446,19 @@ def main():
                         "max_excursion": str(res.max_excursion),
                         "max_excursion_seed": str(res.max_excursion_seed), "errors": res.errors},
             "roofline": {"bound": "int", "achieved": achieved, "peak": peak, "unit": "Tops/s (32-bit)",
-                         "frac": achieved / peak, "traffic": K_RANGE_DRAM_BYTES,
+                         "frac": achieved / peak,
+                         "traffic": K_RANGE_DRAM_BYTES if args.workload == "block" else None,
                          "traffic_basis": "dram__bytes_read.sum + dram__bytes_write.sum of one k_range "
                                           "launch (ncu, 2^33 block); the k = 24 survivor table is read "
                                           "from DRAM once per launch and from L2 after that, so the "
-                                          "figure does not grow with the block size",
+                                          "figure does not grow with the block size"
+                                          if args.workload == "block" else "not captured for this workload",
                          "model": f"{ops_per_seed:.1f} algorithmic 32-bit ops per surviving seed "
                                   f"({OPS_JUMP} + {OPS_ODD} x {odd_per:.2f} odd runs + {OPS_EVEN} x "
                                   f"{even_per:.2f} even runs) x {res.seeds_checked} seeds per launch",
                          "peak_basis": f"issue peak {sm_count} SMs x 4 SMSP x 32 lanes x {sm_mhz:.0f} MHz "
                                        "(sampled median SM clock); no integer peak in MEASURED_PEAKS.json"},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 32 + 56 * 3,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 32 + 64 * 3,
                     "d2h_bytes_per_step": 136,
                     "call": "collatz_verify_range (lower + upload work list + graph + result copy)"},
             "clocks": clocks,
@@ -443,11 +467,12 @@ def main():
         }
         if not args.no_cpu_baseline:
             nthreads = os.cpu_count() or 1
-            rate, csize, cdt = cpu_sample(OFFSET, 15.0, K_SIEVE, nthreads)
+            rate, csize, cdt = cpu_sample(base, 15.0, ksv, nthreads)
             line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": nthreads, "kind": "port",
-                                    "sample": f"[2^40, 2^40 + {csize}) in {cdt:.1f} s (oracle run-length "
-                                              f"loop after cu:684-715, {nthreads} threads)"}
-        if world == 1 and not args.no_extras:
+                                    "sample": f"[2^{wl['offset_log2']}, 2^{wl['offset_log2']} + {csize}) in "
+                                              f"{cdt:.1f} s (oracle run-length loop after cu:684-715, "
+                                              f"{nthreads} threads)"}
+        if world == 1 and not args.no_extras and args.workload == "block":
             for key, fn in (("batched", lambda: run_batched(v)),
                             ("served", lambda: run_served(v, value, load=args.served_load,
                                                           duration=args.served_duration))):

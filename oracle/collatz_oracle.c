@@ -376,27 +376,29 @@ int orc_run_case(const orc_tables *t, uint64_t base_lo, uint64_t base_hi,
 /* Range mode.                                                           */
 /* ===================================================================== */
 
+/* 1 iff residue r mod 2^k survives the k-step descent sieve:
+ * 3^{f_j(r)} >= 2^j for every 1 <= j <= k (f_j = odd steps among the first j). */
+static int residue_survives(uint64_t r, uint32_t k) {
+  uint64_t n = r;
+  unsigned f = 0;
+  for (unsigned j = 1; j <= k; j++) {
+    if (n & 1) {
+      n = n + (n >> 1) + 1;
+      f++;
+    } else {
+      n >>= 1;
+    }
+    if (pow3(f) < ((u128)1 << j)) return 0;
+  }
+  return 1;
+}
+
 uint64_t orc_range_sieve(uint32_t k, uint8_t *bits) {
   uint64_t count = 0;
   uint64_t nres = 1ull << k;
   if (bits) memset(bits, 0, (size_t)(nres + 7) / 8);
   for (uint64_t r = 0; r < nres; r++) {
-    uint64_t n = r;
-    unsigned f = 0;
-    int ok = 1;
-    for (unsigned j = 1; j <= k; j++) {
-      if (n & 1) {
-        n = n + (n >> 1) + 1;
-        f++;
-      } else {
-        n >>= 1;
-      }
-      if (pow3(f) < ((u128)1 << j)) {
-        ok = 0;
-        break;
-      }
-    }
-    if (ok) {
+    if (residue_survives(r, k)) {
       count++;
       if (bits) bits[r >> 3] |= (uint8_t)(1u << (r & 7));
     }
@@ -705,7 +707,7 @@ static void *range_worker(void *p) {
     }
     if (j->k && n >= K) {
       uint64_t r = (uint64_t)n & mask;
-      if (!((j->bits[r >> 3] >> (r & 7)) & 1)) continue;
+      if (j->bits ? !((j->bits[r >> 3] >> (r & 7)) & 1) : !residue_survives(r, j->k)) continue;
     }
     j->acc.seeds++;
     if (j->method == 0)
@@ -721,11 +723,19 @@ static void *range_worker(void *p) {
 int orc_range(uint64_t offset_lo, uint64_t offset_hi, uint64_t size,
               uint32_t k, int use_mod9, int method, int nthreads,
               orc_range_result *out) {
+  /* the table costs 2^k residue tests, the direct test k steps per seed */
+  const int direct = k > 26 || (u128)size * k < ((u128)1 << k);
+  return orc_range_ex(offset_lo, offset_hi, size, k, use_mod9, method, nthreads, direct, out);
+}
+
+int orc_range_ex(uint64_t offset_lo, uint64_t offset_hi, uint64_t size,
+                 uint32_t k, int use_mod9, int method, int nthreads,
+                 int direct_sieve, orc_range_result *out) {
   u128 offset = U128_OF(offset_lo, offset_hi);
   if (k > 34 || nthreads < 1) return -1;
   memset(out, 0, sizeof *out);
   uint8_t *bits = NULL;
-  if (k) {
+  if (k && !direct_sieve) {
     bits = (uint8_t *)malloc((size_t)((1ull << k) + 7) / 8);
     if (!bits) return -2;
     orc_range_sieve(k, bits);

@@ -138,6 +138,13 @@ uint64_t orc_range_sieve_validate(uint32_t k);
 int orc_range(uint64_t offset_lo, uint64_t offset_hi, uint64_t size,
               uint32_t k, int use_mod9, int method, int nthreads,
               orc_range_result *out);
+/* As orc_range with the sieve applied either from the 2^k-bit table
+ * (direct_sieve = 0) or by testing each seed's residue against the sieve's
+ * definition (direct_sieve = 1; used for k > 26 and for ranges much smaller
+ * than 2^k, where building the table would dominate).  Same results. */
+int orc_range_ex(uint64_t offset_lo, uint64_t offset_hi, uint64_t size,
+                 uint32_t k, int use_mod9, int method, int nthreads,
+                 int direct_sieve, orc_range_result *out);
 
 /* ---------------- trajectory queries ---------------- */
 /* seeds: nseeds x seed_limbs little-endian u32 limbs (seed_limbs <= 8).

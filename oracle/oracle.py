@@ -100,6 +100,9 @@ def lib():
         L.orc_range_sieve_validate.restype = C.c_uint64
         L.orc_range.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint32, C.c_int,
                                 C.c_int, C.c_int, C.POINTER(_RangeResult)]
+        L.orc_range_ex.restype = C.c_int
+        L.orc_range_ex.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint32, C.c_int,
+                                   C.c_int, C.c_int, C.c_int, C.POINTER(_RangeResult)]
         L.orc_trajectory.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
                                      C.c_void_p, C.c_void_p]
         _lib = L
@@ -279,10 +282,15 @@ class RangeResult:
 
 
 def range_verify(offset: int, size: int, k: int, use_mod9: bool = True, method: int = 1,
-                 nthreads: int = 1) -> RangeResult:
+                 nthreads: int = 1, direct_sieve: bool | None = None) -> RangeResult:
+    """orc_range; direct_sieve None = the oracle's choice (table for small k)."""
     r = _RangeResult()
-    rc = lib().orc_range(*_split(offset), size, k, 1 if use_mod9 else 0, method, nthreads,
-                         C.byref(r))
+    if direct_sieve is None:
+        rc = lib().orc_range(*_split(offset), size, k, 1 if use_mod9 else 0, method, nthreads,
+                             C.byref(r))
+    else:
+        rc = lib().orc_range_ex(*_split(offset), size, k, 1 if use_mod9 else 0, method, nthreads,
+                                1 if direct_sieve else 0, C.byref(r))
     if rc:
         raise ValueError(f"orc_range rc={rc}")
     return RangeResult(r.seeds, r.failures, _limbs(r.max_exc), _limbs(r.max_exc_seed),

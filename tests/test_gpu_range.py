@@ -20,6 +20,9 @@ CASES = [
     (1000, 5000, 12, False),                    # no mod-9 sieve
     ((1 << 64) - (1 << 20), 1 << 21, 24, True),  # crosses 2^64
     ((1 << 90) + 3, 1 << 17, 16, True),         # 91-bit seeds
+    ((1 << 60) + (3 << 34), 1 << 22, 34, True),  # frontier sieve (2 GiB bit array), aligned
+    ((1 << 60) + (5 << 34) - 100000, 300000, 34, True),  # crosses a 2^34 block boundary
+    ((1 << 60) + 77777, 1 << 21, 30, True),     # k = 30, unaligned
 ]
 
 
@@ -30,7 +33,7 @@ def _cmp(g, o):
     assert (g.max_excursion, g.max_excursion_seed) == (o.max_exc, o.max_exc_seed)
 
 
-@pytest.mark.parametrize("k", [8, 12, 16, 20, 24])
+@pytest.mark.parametrize("k", [8, 12, 16, 20, 24, 27])
 def test_range_sieve_matches_oracle(verifier, k):
     from oracle import oracle as O
     n, bits = verifier(26).range_sieve(k)

@@ -146,6 +146,47 @@ def test_range_methods_agree(case):
     assert keys[0] == keys[1] == keys[2]
 
 
+@pytest.mark.parametrize("case", [(1 << 40, 1 << 18, 16), ((1 << 60) + 12345, 1 << 17, 20), (3, 1 << 16, 12),
+                                  ((1 << 50) - 4096, 1 << 16, 24)])
+def test_range_direct_sieve_equals_table(case):
+    """Testing each seed's residue against the sieve definition gives the
+    same results as the 2^k-bit table (the direct test is what the oracle
+    uses for k > 26, e.g. the k = 34 frontier configuration)."""
+    from oracle import oracle as O
+    off, size, k = case
+    a = O.range_verify(off, size, k, True, method=2, nthreads=4, direct_sieve=False)
+    b = O.range_verify(off, size, k, True, method=2, nthreads=4, direct_sieve=True)
+    assert (a.seeds, a.max_st, a.max_st_seed, a.max_exc, a.max_exc_seed, a.odd_runs) == \
+        (b.seeds, b.max_st, b.max_st_seed, b.max_exc, b.max_exc_seed, b.odd_runs)
+
+
+def test_range_k34_bruteforce():
+    from oracle import oracle as O
+    k, off, size = 34, (1 << 60) + (7 << 34) + 99991, 2500
+    o = O.range_verify(off, size, k, True, method=2)
+    best_st, best_e, seeds = (-1, 0), (-1, 0), 0
+    for n in range(off, off + size):
+        if n % 9 not in (0, 1, 3, 6, 7):
+            continue
+        x, f, ok = n % (1 << k), 0, True
+        for j in range(1, k + 1):
+            if x & 1:
+                f += 1
+            x = T_step(x)
+            if 3 ** f < 2 ** j:
+                ok = False
+                break
+        if not ok:
+            continue
+        seeds += 1
+        st, E = brute(n)
+        best_st = max(best_st, (st, -n))
+        best_e = max(best_e, (E, -n))
+    assert o.seeds == seeds
+    assert (o.max_st, o.max_st_seed) == (best_st[0], -best_st[1])
+    assert (o.max_exc, o.max_exc_seed) == (best_e[0], -best_e[1])
+
+
 def test_trajectory_bruteforce():
     from oracle import oracle as O
     rng = random.Random(3)
