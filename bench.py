@@ -49,6 +49,10 @@ UNIT = "seeds/s"
 OPS_JUMP, OPS_ODD, OPS_EVEN = 16, 14, 12
 # DRAM bytes (read + write) of one k_range launch, measured with ncu.
 K_RANGE_DRAM_BYTES = 5.316864e6 + 0.210944e6
+# Frontier (k = 34): every block of 2^34 seeds streams the whole 2.43 GB
+# survivor table; ncu on a 4-block launch read 9.724289280e9 and wrote
+# 8.792576e6 bytes, so traffic per launch = blocks x this figure.
+K_RANGE_FRONTIER_DRAM_BYTES_PER_BLOCK = (9.724289280e9 + 8.792576e6) / 4
 
 
 def dist_env():
@@ -447,12 +451,16 @@ def main():
                         "max_excursion_seed": str(res.max_excursion_seed), "errors": res.errors},
             "roofline": {"bound": "int", "achieved": achieved, "peak": peak, "unit": "Tops/s (32-bit)",
                          "frac": achieved / peak,
-                         "traffic": K_RANGE_DRAM_BYTES if args.workload == "block" else None,
+                         "traffic": K_RANGE_DRAM_BYTES if args.workload == "block" else
+                         K_RANGE_FRONTIER_DRAM_BYTES_PER_BLOCK * max(1, size >> ksv),
                          "traffic_basis": "dram__bytes_read.sum + dram__bytes_write.sum of one k_range "
                                           "launch (ncu, 2^33 block); the k = 24 survivor table is read "
                                           "from DRAM once per launch and from L2 after that, so the "
                                           "figure does not grow with the block size"
-                                          if args.workload == "block" else "not captured for this workload",
+                                          if args.workload == "block" else
+                                          "ncu dram__bytes_read.sum + dram__bytes_write.sum of a 4-block "
+                                          "(2^36) launch, scaled by blocks: each 2^34 block streams the "
+                                          "2.43 GB survivor table once",
                          "model": f"{ops_per_seed:.1f} algorithmic 32-bit ops per surviving seed "
                                   f"({OPS_JUMP} + {OPS_ODD} x {odd_per:.2f} odd runs + {OPS_EVEN} x "
                                   f"{even_per:.2f} even runs) x {res.seeds_checked} seeds per launch",
