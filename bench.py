@@ -216,6 +216,47 @@ def run_batched(v, n_req: int = 4096, seed: int = 4096, lo_log2: int = 20, hi_lo
             "bit_exact_vs_plain": bool(exact)}
 
 
+def run_cases() -> dict:
+    """Cases mode, the reference's own verification run (Algorithm 1: host
+    Step 1, GPU Steps 2-3), end to end through collatz_run_case on the golden
+    tuples with more than 10^7 seeds (N = 36 root case; N = 45 cases_tiny
+    lines 1-3), each checked against the reference's hash and launch count.
+    CPU: the oracle's restatement of the reference, one thread like the
+    reference's host program, on the N = 36 root case."""
+    import collatz_b200 as cb
+    from oracle import oracle as O
+    with open(os.path.join(ROOT, "tests", "golden", "cases_runs.json")) as f:
+        runs = [r for r in json.load(f)["runs"] if r["N"] in (36, 45) and r["seeds"] > 10 ** 7]
+    verifiers, out = {}, []
+    for r in runs:
+        if r["N"] not in verifiers:
+            verifiers[r["N"]] = cb.Verifier(r["N"])
+        v = verifiers[r["N"]]
+        v.run_case(*r["tuple"])  # warm-up (host pools, first launches)
+        t0 = time.perf_counter()
+        res = v.run_case(*r["tuple"])
+        dt = time.perf_counter() - t0
+        out.append({"N": r["N"], "tuple": r["tuple"], "seeds": res.seeds_checked, "s": dt,
+                    "seeds_per_s": res.seeds_checked / dt, "device_ms": res.device_ms,
+                    "hash_ok": f"{res.hash:X}" == r["hash"], "launches_ok": res.launches == r["launches"],
+                    "seeds_ok": res.seeds_checked == r["seeds"]})
+    for v in verifiers.values():
+        v.close()
+    T = O.Tables(36)
+    t0 = time.perf_counter()
+    c = T.run_case(3, 2, 2, 9, 1, 0)
+    cdt = time.perf_counter() - t0
+    n45 = [o for o in out if o["N"] == 45]
+    return {"workload": "collatz_run_case (host Step 1 + GPU Steps 2-3) on the reference's golden tuples",
+            "runs": out,
+            "n45_seeds_per_s": sum(o["seeds"] for o in n45) / max(1e-9, sum(o["s"] for o in n45)),
+            "all_match_reference": all(o["hash_ok"] and o["launches_ok"] and o["seeds_ok"] for o in out),
+            "cpu_baseline": {"value": c.seeds / cdt, "unit": UNIT, "cores": 1, "kind": "port",
+                             "sample": f"N=36 root case (3 2 2 9 1 0), {c.seeds} seeds in {cdt:.1f} s "
+                                       "(oracle/collatz_oracle.c orc_run_case, the reference's kernel "
+                                       "semantics cu:185-411 on one thread)"}}
+
+
 def run_served(v, capacity: float, load: float = 0.7, duration: float = 1.0, seed: int = 5,
                slice_items: int = 1 << 19, plain_sample: int = 600) -> dict:
     """Served configuration: Poisson arrivals at `load` x capacity (range seeds
@@ -483,7 +524,8 @@ def main():
         if world == 1 and not args.no_extras and args.workload == "block":
             for key, fn in (("batched", lambda: run_batched(v)),
                             ("served", lambda: run_served(v, value, load=args.served_load,
-                                                          duration=args.served_duration))):
+                                                          duration=args.served_duration)),
+                            ("cases", run_cases)):
                 try:
                     line[key] = fn()
                 except Exception as e:  # noqa: BLE001 -- the headline line is printed regardless

@@ -66,6 +66,12 @@ class RangeResultC(C.Structure):
 
 
 REQ_RANGE, REQ_TRAJECTORY = 0, 1
+TUNE_RANGE, TUNE_CASES, TUNE_NO_CACHE = 0x1, 0x2, 0x4
+
+
+class TuneResultC(C.Structure):
+    _fields_ = [("range_variant", C.c_int32), ("cases_variant", C.c_int32),
+                ("range_ms", C.c_float * 8), ("cases_ms", C.c_float * 8)]
 
 
 class ServerConfig(C.Structure):
@@ -137,6 +143,7 @@ def lib() -> C.CDLL:
             "collatz_server_wait": (C.c_int, [P, C.c_uint64, C.c_double, C.POINTER(ResponseC)]),
             "collatz_server_info": (C.c_int, [P, C.POINTER(ServerInfoC)]),
             "collatz_server_stop": (C.c_int, [P]),
+            "collatz_autotune": (C.c_int, [P, C.c_uint32, C.POINTER(TuneResultC)]),
             "collatz_variant_count": (C.c_int, [C.c_int]),
             "collatz_set_variant": (C.c_int, [P, C.c_int, C.c_int]),
         }
@@ -307,6 +314,15 @@ class Verifier:
 
     def set_variant(self, mode: int, variant: int):
         self._check(lib().collatz_set_variant(self._h, mode, variant), "set_variant")
+
+    def autotune(self, range_mode: bool = True, cases_mode: bool = True, cache: bool = True) -> dict:
+        """Times every kernel variant on this device (collatz_autotune) and keeps the fastest."""
+        flags = (TUNE_RANGE if range_mode else 0) | (TUNE_CASES if cases_mode else 0) | \
+            (0 if cache else TUNE_NO_CACHE)
+        r = TuneResultC()
+        self._check(lib().collatz_autotune(self._h, flags, C.byref(r)), "autotune")
+        return {"range_variant": r.range_variant, "cases_variant": r.cases_variant,
+                "range_ms": [x for x in r.range_ms if x >= 0], "cases_ms": [x for x in r.cases_ms if x >= 0]}
 
     # ---- cases mode ----
     def run_case(self, base, sigfig, threepower, number, doubleeven, numevens,

@@ -254,6 +254,7 @@ extern "C" int collatz_create(const collatz_config* cfg, collatz_ctx** out) {
     return rc;
   }
   c->stream = c->own_stream;
+  if (cfg->variant == COLLATZ_VARIANT_AUTO) tune_on_create(c);
   *out = c;
   return COLLATZ_OK;
 }

@@ -97,4 +97,6 @@ int get_range_tables(collatz_ctx* c, uint32_t k, RangeTables** out);
 int lower_range(collatz_ctx* c, const collatz_range& r, uint32_t req, const RangeTables& T,
                 std::vector<RangeSeg>& segs, unsigned long long& items);
 void rec_to_range_result(const ReqRec& r, collatz_range_result* out);
+// Applies cached autotuner choices to a new context (tune.cu).
+void tune_on_create(collatz_ctx* c);
 }  // namespace cz

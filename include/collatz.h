@@ -277,9 +277,28 @@ int collatz_server_info(collatz_server *s, collatz_server_info_t *info);
  * COLLATZ_E_STATE, joins the scheduler and frees the server. */
 int collatz_server_stop(collatz_server *s);
 
-/* Kernel variants for the autotuner. */
+/* Kernel variants (block shapes) for the autotuner. */
 int collatz_variant_count(int mode); /* mode 0 cases, 1 range */
 int collatz_set_variant(collatz_ctx *ctx, int mode, int variant);
+
+/* Autotuner (no counterpart in the reference).  Times every variant of the
+ * selected modes on a fixed sample on this device -- range: 2^34 seeds at
+ * 2^40 with the context's k; cases: about 2^20 Step-1 pairs of the root case
+ * "3 2 2 9 1 0" for the context's N -- keeps the fastest for the context and
+ * records it in a text cache (COLLATZ_TUNE_CACHE, else
+ * $XDG_CACHE_HOME/collatz_b200/tune.txt or ~/.cache/collatz_b200/tune.txt),
+ * keyed by device, variant set and k or N.  A context created with
+ * COLLATZ_VARIANT_AUTO applies cached choices; with COLLATZ_AUTOTUNE=1 in the
+ * environment it also tunes what the cache lacks.  Variants never change
+ * results, only speed. */
+typedef struct {
+  int32_t range_variant, cases_variant; /* chosen (or kept when not tuned) */
+  float range_ms[8], cases_ms[8];       /* device ms per variant on the sample; -1 = not timed */
+} collatz_tune_result;
+#define COLLATZ_TUNE_RANGE 0x1u
+#define COLLATZ_TUNE_CASES 0x2u
+#define COLLATZ_TUNE_NO_CACHE 0x4u /* do not record the choice in the cache */
+int collatz_autotune(collatz_ctx *ctx, uint32_t flags, collatz_tune_result *out);
 
 #ifdef __cplusplus
 }
