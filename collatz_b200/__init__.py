@@ -144,6 +144,10 @@ def lib() -> C.CDLL:
             "collatz_server_info": (C.c_int, [P, C.POINTER(ServerInfoC)]),
             "collatz_server_stop": (C.c_int, [P]),
             "collatz_autotune": (C.c_int, [P, C.c_uint32, C.POINTER(TuneResultC)]),
+            "collatz_combine_case_results": (C.c_int, [P, C.c_uint32, C.POINTER(CaseResultC)]),
+            "collatz_run_cases": (C.c_int, [P, P, C.c_uint32, C.c_char_p, P, C.POINTER(CaseResultC),
+                                            C.POINTER(C.c_uint32)]),
+            "collatz_journal_load": (C.c_int, [C.c_char_p, P, C.c_uint32, P, P]),
             "collatz_variant_count": (C.c_int, [C.c_int]),
             "collatz_set_variant": (C.c_int, [P, C.c_int, C.c_int]),
         }
@@ -238,6 +242,26 @@ def pack_pairs(pairs) -> "C.Array":
             buf[8 * i + j] = (b >> (32 * j)) & 0xFFFFFFFF
             buf[8 * i + 4 + j] = (m >> (32 * j)) & 0xFFFFFFFF
     return buf
+
+
+def journal_load(journal: str, tuples, overflow_cap: int = 1 << 10):
+    """Host-only: {case index: CaseResult} for the cases a journal records."""
+    n = len(tuples)
+    arr = (Case * max(1, n))()
+    for i, t in enumerate(tuples):
+        arr[i] = make_case(*t)
+    res = (CaseResultC * max(1, n))()
+    bufs = []
+    for i in range(n):
+        b = (C.c_uint32 * (4 * overflow_cap))()
+        bufs.append(b)
+        res[i].overflow_seeds = C.cast(b, C.POINTER(C.c_uint32))
+        res[i].overflow_cap = overflow_cap
+    done = (C.c_uint8 * max(1, n))()
+    rc = lib().collatz_journal_load(journal.encode(), arr, n, res, done)
+    if rc:
+        raise CollatzError(rc, f"journal_load: {status_string(rc)}")
+    return {i: _case_result(res[i], bufs[i], overflow_cap) for i in range(n) if done[i]}
 
 
 def step1_pairs(maxbits: int, base, sigfig, threepower, number, doubleeven, numevens, cap=None):
@@ -354,6 +378,25 @@ class Verifier:
         return _case_result(r, ov, overflow_cap)
 
     verify_pairs = launchkernel
+
+    def run_cases(self, tuples, journal: str | None = None, overflow_cap: int = 1 << 16):
+        """Runs cases_* lines [(base, sigfig, threepower, number, doubleeven, numevens)] in one
+        process (collatz_run_cases); returns (combined CaseResult, [per-case CaseResult], run now)."""
+        n = len(tuples)
+        arr = (Case * max(1, n))()
+        for i, t in enumerate(tuples):
+            arr[i] = make_case(*t)
+        per = (CaseResultC * max(1, n))()
+        comb = CaseResultC()
+        ov = (C.c_uint32 * (4 * overflow_cap))()
+        comb.overflow_seeds = C.cast(ov, C.POINTER(C.c_uint32))
+        comb.overflow_cap = overflow_cap
+        ran = C.c_uint32()
+        rc = lib().collatz_run_cases(self._h, arr, n, journal.encode() if journal else None, per,
+                                     C.byref(comb), C.byref(ran))
+        self._check(rc, "run_cases")
+        return (_case_result(comb, ov, overflow_cap), [_case_result(per[i], None, 0) for i in range(n)],
+                ran.value)
 
     def case_tables(self) -> tuple[bytes, bytes]:
         bv = (C.c_uint32 * (16 * BV_WORDS))()

@@ -146,6 +146,35 @@ int collatz_verify_pairs_noalloc(collatz_ctx *ctx, uint32_t bigindex, const uint
 int collatz_step1_pairs(uint32_t maxbits, const collatz_case *c, uint32_t *pairs, uint64_t cap,
                         uint64_t *count);
 
+/* ---- Cases driver: many cases_* lines with a resume journal ---- */
+/* The reference is run as one process per cases_* line and the results are
+ * combined by hand (multi-copy operation).  These calls do it in one process.
+ *
+ * Merges per-case results: hash by XOR, counts and device time by sum,
+ * maxima by value then smaller seed, overflow seeds concatenated and sorted
+ * (up to out->overflow_cap; n_overflow counts all), errors by OR.
+ * Host-only. */
+int collatz_combine_case_results(const collatz_case_result *parts, uint32_t n, collatz_case_result *out);
+
+/* Runs cases[0..n) in order on one context and combines them into
+ * *combined.  With a journal path, each finished case is appended to the
+ * journal as one text line, flushed and synced before the next case starts;
+ * a later call with the same cases and journal takes the finished cases from
+ * the journal and runs only the rest, so an interrupted run resumes where it
+ * stopped.  A journal line whose tuple differs from the case at its index is
+ * rejected (COLLATZ_E_STATE).  per_case (NULL or n entries) receives each
+ * case's result without overflow seeds.  *n_run (may be NULL) = cases run by
+ * this call. */
+int collatz_run_cases(collatz_ctx *ctx, const collatz_case *cases, uint32_t n, const char *journal,
+                      collatz_case_result *per_case, collatz_case_result *combined, uint32_t *n_run);
+
+/* Host-only: reads a journal.  For every case index it records, done[i] = 1
+ * and results[i] receives that case's result; results[i].overflow_seeds is
+ * filled up to results[i].overflow_cap when set.  A missing journal file
+ * means nothing is done yet. */
+int collatz_journal_load(const char *journal, const collatz_case *cases, uint32_t n,
+                         collatz_case_result *results, uint8_t *done);
+
 /* Copies the device-built tables back: bv = 16 x (2^19 + 32) uint32 (the
  * reference's flat d_flat, cu:138-152), mod9 = 9 x 32 uint32 (cu:159-171). */
 int collatz_case_tables(collatz_ctx *ctx, uint32_t *bv, uint32_t *mod9);
