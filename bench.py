@@ -507,7 +507,10 @@ def main():
                                   f"{even_per:.2f} even runs) x {res.seeds_checked} seeds per launch",
                          "peak_basis": f"issue peak {sm_count} SMs x 4 SMSP x 32 lanes x {sm_mhz:.0f} MHz "
                                        "(sampled median SM clock); no integer peak in MEASURED_PEAKS.json"},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 32 + 64 * 3,
+            # request (32 B) + its work list: an aligned range of many blocks lowers to 55
+            # 64-byte segments (5 kept mod-9 classes of the first and last block, 9 x 5 for the
+            # blocks between)
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 32 + 64 * 55,
                     "d2h_bytes_per_step": 136,
                     "call": "collatz_verify_range (lower + upload work list + graph + result copy)"},
             "clocks": clocks,

@@ -93,17 +93,22 @@ int get_range_tables(collatz_ctx* c, uint32_t k, RangeTables** out) {
   return COLLATZ_OK;
 }
 
-// index of the first survivor >= r
-static int lower_bound_res(collatz_ctx* c, const RangeTables& T, uint64_t r, uint32_t* out) {
+// index of the first survivor >= r within mod-9 class cl of the class-major table
+static int lower_bound_res(collatz_ctx* c, const RangeTables& T, uint32_t cl, uint64_t r, uint32_t* out) {
+  const uint64_t b = T.dev.cls[cl], e = T.dev.cls[cl + 1];
+  if (r == 0 || b == e) {
+    *out = (uint32_t)b;
+    return COLLATZ_OK;
+  }
   if (r >= (1ull << T.dev.k)) {
-    *out = (uint32_t)T.dev.count;
+    *out = (uint32_t)e;
     return COLLATZ_OK;
   }
-  if (!T.residues.empty() || T.dev.count == 0) {
-    *out = (uint32_t)(std::lower_bound(T.residues.begin(), T.residues.end(), r) - T.residues.begin());
+  if (!T.residues.empty()) {
+    *out = (uint32_t)(std::lower_bound(T.residues.begin() + b, T.residues.begin() + e, r) - T.residues.begin());
     return COLLATZ_OK;
   }
-  uint64_t lo = 0, hi = T.dev.count;  // binary search with single-entry reads
+  uint64_t lo = b, hi = e;  // binary search with single-entry reads
   while (lo < hi) {
     const uint64_t mid = (lo + hi) / 2;
     RangeEntry e;
@@ -136,16 +141,21 @@ int lower_range(collatz_ctx* c, const collatz_range& r, uint32_t req, const Rang
     segs.push_back(g);
     items += (d_hi - d_lo + DENSE_ITEM - 1) / DENSE_ITEM;
   }
+  // Seeds >= 2^k: blocks q of 2^k residues.  The table is class-major (r mod
+  // 9), and with the mod-9 sieve a block keeps exactly the classes c with
+  // (q 2^k + c) mod 9 in {0,1,3,6,7}: 5 of the 9, depending only on q mod 9.
+  // So each emitted segment covers one whole class (or, in a partial first
+  // or last block, the class's residues in range), and every entry it names
+  // is a seed.  Blocks strictly between the first and the last are grouped
+  // by q mod 9 into segments with block stride 9.
   const u128 lo = std::max(O, K);
   if (lo >= E) return COLLATZ_OK;
   const u128 qa = lo >> k, qb = (E - 1) >> k;
-  uint32_t sa, sb;
-  int rc = lower_bound_res(c, T, (uint64_t)(lo & (K - 1)), &sa);
-  if (rc) return rc;
-  rc = lower_bound_res(c, T, (uint64_t)((E - 1) & (K - 1)) + 1, &sb);
-  if (rc) return rc;
-  const uint32_t ns = (uint32_t)T.dev.count;
-  auto add = [&](u128 q, u128 nq, uint32_t s_lo, uint32_t s_hi) {
+  const uint32_t k9 = (uint32_t)(((u128)1 << (k % 6)) % 9);  // 2^k mod 9 (2^6 = 1 mod 9)
+  auto live = [&](u128 q, uint32_t cl) {
+    return !mod9 || ((0xCBu >> (((uint32_t)(q % 9) * k9 + cl) % 9)) & 1u);  // keep {0,1,3,6,7} (cu:488)
+  };
+  auto add = [&](u128 q, u128 nq, uint32_t stride, uint32_t s_lo, uint32_t s_hi) {
     if (s_lo >= s_hi || nq == 0) return;
     const uint32_t ipq = (s_hi - s_lo + RANGE_ITEM - 1) / RANGE_ITEM;
     const u128 max_nq = std::max<uint32_t>(1u, 0xFFFFFFFFu / ipq);  // < 2^32 items per segment
@@ -161,21 +171,43 @@ int lower_range(collatz_ctx* c, const collatz_range& r, uint32_t req, const Rang
       g.ipq = ipq;
       g.req = req;
       g.kind = 0;
-      g.mod9 = mod9;
+      g.qstride = (uint16_t)stride;
+      g.mod9 = 0;  // every class of the segment is kept
       segs.push_back(g);
       items += (unsigned long long)take * ipq;
-      q += take;
+      q += (u128)take * stride;
       nq -= take;
     }
   };
-  if (qa == qb) {
-    add(qa, 1, sa, sb);
-  } else {
-    add(qa, 1, sa, ns);
-    add(qa + 1, qb - qa - 1, 0, ns);
-    add(qb, 1, 0, sb);
+  // one block q, residues [r0, r1)
+  auto partial = [&](u128 q, uint64_t r0, uint64_t r1) -> int {
+    for (uint32_t cl = 0; cl < 9; cl++) {
+      if (!live(q, cl)) continue;
+      uint32_t a = 0, b = 0;
+      int rc = lower_bound_res(c, T, cl, r0, &a);
+      if (!rc) rc = lower_bound_res(c, T, cl, r1, &b);
+      if (rc) return rc;
+      add(q, 1, 1, a, b);
+    }
+    return COLLATZ_OK;
+  };
+  const uint64_t ra = (uint64_t)(lo & (K - 1)), rb = (uint64_t)((E - 1) & (K - 1)) + 1;
+  if (qa == qb) return partial(qa, ra, rb);
+  int rc = partial(qa, ra, (uint64_t)K);
+  if (rc) return rc;
+  const u128 m0 = qa + 1, nm = qb - qa - 1;  // whole blocks in between
+  if (nm > 0) {
+    if (!mod9) {
+      for (uint32_t cl = 0; cl < 9; cl++) add(m0, nm, 1, (uint32_t)T.dev.cls[cl], (uint32_t)T.dev.cls[cl + 1]);
+    } else {
+      for (uint32_t t = 0; t < 9 && (u128)t < nm; t++) {
+        const u128 qt = m0 + t, nt = (nm - t + 8) / 9;  // blocks m0 + t, m0 + t + 9, ...
+        for (uint32_t cl = 0; cl < 9; cl++)
+          if (live(qt, cl)) add(qt, nt, 9, (uint32_t)T.dev.cls[cl], (uint32_t)T.dev.cls[cl + 1]);
+      }
+    }
   }
-  return COLLATZ_OK;
+  return partial(qb, 0, rb);
 }
 
 }  // namespace cz

@@ -34,7 +34,8 @@ constexpr uint32_t RANGE_ITEM = 64;     // survivor-table entries per work item
 constexpr uint32_t DENSE_ITEM = 64;     // consecutive integers per dense work item
 
 // A run of work items of one request.  kind 0: survivor entries
-// [s_lo, s_hi) of blocks q .. q+nq-1 (seeds n = q 2^k + r);
+// [s_lo, s_hi) (one mod-9 class of the class-major table, or all of it) of
+// blocks q, q + qstride, ... (nq blocks; seeds n = q 2^k + r);
 // kind 1: integers [d_lo, d_hi) iterated without the residue sieve.
 struct RangeSeg {
   unsigned long long item_begin;  // global index of the first item
@@ -45,8 +46,10 @@ struct RangeSeg {
   uint32_t s_lo, s_hi;            // kind 0: survivor index range
   uint32_t ipq;                   // kind 0: items per block
   uint32_t req;                   // request index (ReqRec)
-  uint32_t kind;
-  uint32_t mod9;                  // 1: apply the mod-9 sieve
+  uint16_t kind;
+  uint16_t qstride;               // kind 0: block stride (0 or 1: consecutive blocks; 9: one q mod 9)
+  uint32_t mod9;                  // 1: apply the mod-9 sieve to each entry (0 when the segment's
+                                  //    classes are all kept by it)
   // Item index within the original segment of item_begin (non-zero when a
   // scheduler cuts a segment into slices; local indices stay < 2^32 for kind 0).
   uint32_t local0_lo, local0_hi;

@@ -113,10 +113,13 @@ __device__ __forceinline__ void widen_seed(const RangeArgs& A, u32 req, u32 n0, 
 }
 
 // Advances to the next work item (claiming CLAIM items at a time), resolves
-// its segment and block, and starts copying its survivor entries into
-// W.stage with cp.async so that they arrive while the current item is
-// expanded.  Warp-uniform; lane 0 owns the bookkeeping.
-__device__ __forceinline__ void stage_next(RangeWarp& W, const RangeArgs& A, const uint4* __restrict__ T, u32 lane) {
+// its segment and block, and starts copying its survivor entries into dst
+// with cp.async so that they arrive while the current item is worked on.
+// Warp-uniform; lane 0 owns the bookkeeping.  WT is the kernel's per-warp
+// state (fields seg, nxt, item, claim_hi, seg_lo, seg_hi, qi, chunk).
+template <class WT>
+__device__ __forceinline__ void stage_next(WT& W, uint4* dst, const RangeArgs& A, const uint4* __restrict__ T,
+                                           u32 lane) {
   ull next = W.item + 1;
   bool fresh = false;
   if (next >= W.claim_hi) {
@@ -187,7 +190,8 @@ __device__ __forceinline__ void stage_next(RangeWarp& W, const RangeArgs& A, con
   it.valid = 1;
   it.pad = 0;
   if (kind == 0) {
-    const unsigned __int128 q = (((unsigned __int128)W.seg.q_hi << 64) | W.seg.q_lo) + qi;
+    const u32 qs = W.seg.qstride ? W.seg.qstride : 1u;
+    const unsigned __int128 q = (((unsigned __int128)W.seg.q_hi << 64) | W.seg.q_lo) + (unsigned __int128)qi * qs;
     it.q_lo = (u64)q;
     it.q_hi = (u32)(q >> 64);
     it.sbase = W.seg.s_lo + chunk * RANGE_ITEM;
@@ -196,7 +200,7 @@ __device__ __forceinline__ void stage_next(RangeWarp& W, const RangeArgs& A, con
 #pragma unroll
     for (u32 j = 0; j < RANGE_ITEM / 32; j++) {
       const u32 idx = it.sbase + j * 32 + lane;
-      if (idx < it.send) cp_async16(&W.stage[j * 32 + lane], T + idx);
+      if (idx < it.send) cp_async16(&dst[j * 32 + lane], T + idx);
     }
     cp_async_commit();
   } else {
@@ -253,7 +257,7 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
   const u32 k = A.k;
   const u32 k9 = (u32)((1ull << (k % 6)) % 9ull);  // 2^k mod 9 (2^6 = 1 mod 9)
   const uint4* __restrict__ T = reinterpret_cast<const uint4*>(A.table);
-  stage_next(W, A, T, lane);
+  stage_next(W, W.stage, A, T, lane);
 
   // ---- warp-uniform state (the rest lives in W) ----
   u32 head = 0, tail = 0;  // queued seeds [head, tail)
@@ -366,7 +370,7 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
         for (u32 j = 0; j < RANGE_ITEM / 32; j++) e[j] = W.stage[j * 32 + lane];
       }
       __syncwarp();
-      stage_next(W, A, T, lane);  // the following item's copies overlap with this expansion
+      stage_next(W, W.stage, A, T, lane);  // the following item's copies overlap with this expansion
       if (STATS) {
         const ull now = clock64();
         t_stage += now - t_sub;

@@ -57,10 +57,10 @@ constexpr uint64_t TRAJ_BYTES_PER_SEED = 128;
 constexpr uint32_t MAX_ACTIVE_LIMIT = 4096;
 constexpr uint32_t MAX_BATCH_SEEDS = 1u << 22;
 // Staging reserved per admitted request for a slice's work list: a request
-// lowers to at most a dense part, two partial blocks and the full blocks
-// split into runs of < 2^32 items (17 runs for the largest request at
-// k = 24); more is allocated on demand.
-constexpr size_t SEGS_PER_REQ = 24;
+// lowers to a dense part, up to 5 class segments for each partial block and
+// up to 45 (9 residues of q mod 9 x 5 kept classes) for the whole blocks in
+// between; more is allocated on demand.
+constexpr size_t SEGS_PER_REQ = 64;
 constexpr int NCLASS = 5;
 constexpr int CLASS_LIMBS[NCLASS] = {4, 6, 8, 12, 16};
 

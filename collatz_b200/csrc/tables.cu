@@ -309,6 +309,60 @@ void free_case_tables(CaseTables* t) {
   t->bv = t->mod9 = t->magic = t->pow3 = nullptr;
 }
 
+// Pass D: stable partition of the residue-ordered table by r mod 9 into
+// class-major order.  One warp per block of CLS_BLOCK entries: D1 counts
+// each class (hist[c * nblk + block]), an exclusive scan of hist in that
+// order gives every (class, block) its output offset, and D2 scatters the
+// block's entries with one ballot per class per 32 entries, which keeps
+// residue order inside each class.
+constexpr u32 CLS_BLOCK = 2048;
+
+__global__ void k_class_hist(const RangeEntry* __restrict__ t, u64 n, u32* __restrict__ hist, u32 nblk) {
+  const u32 warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = lane_id();
+  if (warp >= nblk) return;
+  u32 cnt[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (u32 i = lane; i < CLS_BLOCK; i += 32) {
+    const u64 idx = (u64)warp * CLS_BLOCK + i;
+    if (idx < n) {
+      const u32 c = (t[idx].meta >> 16) & 0xFFu;
+#pragma unroll
+      for (u32 j = 0; j < 9; j++) cnt[j] += (c == j);
+    }
+  }
+#pragma unroll
+  for (u32 j = 0; j < 9; j++) {
+    u32 x = cnt[j];
+#pragma unroll
+    for (u32 d = 16; d; d >>= 1) x += __shfl_xor_sync(FULL, x, d);
+    if (lane == 0) hist[j * nblk + warp] = x;
+  }
+}
+
+__global__ void k_class_scatter(const RangeEntry* __restrict__ t, u64 n, const ull* __restrict__ offs, u32 nblk,
+                                RangeEntry* __restrict__ out) {
+  const u32 warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = lane_id();
+  if (warp >= nblk) return;
+  ull base[9];
+#pragma unroll
+  for (u32 j = 0; j < 9; j++) base[j] = offs[j * nblk + warp];
+  const u32 lt = lanemask_lt();
+  for (u32 i = 0; i < CLS_BLOCK; i += 32) {
+    const u64 idx = (u64)warp * CLS_BLOCK + i + lane;
+    const bool ok = idx < n;
+    RangeEntry e{0, 0, 0, 0};
+    if (ok) e = t[idx];
+    const u32 c = ok ? ((e.meta >> 16) & 0xFFu) : 9u;
+    ull pos = 0;
+#pragma unroll
+    for (u32 j = 0; j < 9; j++) {
+      const u32 m = __ballot_sync(FULL, c == j);
+      if (c == j) pos = base[j] + __popc(m & lt);
+      base[j] += __popc(m);
+    }
+    if (ok) out[pos] = e;
+  }
+}
+
 cudaError_t build_range_table(RangeTable* t, u32 k, bool validate, cudaStream_t st) {
   t->k = k;
   const u64 nres = 1ull << k;
@@ -346,6 +400,31 @@ cudaError_t build_range_table(RangeTable* t, u32 k, bool validate, cudaStream_t 
   if ((e = cudaStreamSynchronize(st))) return e;
   cudaFree(counts);
   cudaFree(offs);
+  // class-major order (pass D)
+  const u32 nblk = (u32)((total + CLS_BLOCK - 1) / CLS_BLOCK);
+  for (int c = 0; c < 10; c++) t->cls[c] = 0;
+  if (nblk) {
+    u32* hist = nullptr;
+    ull* coffs = nullptr;
+    RangeEntry* out = nullptr;
+    if ((e = cudaMalloc(&hist, sizeof(u32) * 9 * nblk))) return e;
+    if ((e = cudaMalloc(&coffs, sizeof(ull) * (9 * nblk + 1)))) return e;
+    if ((e = cudaMalloc(&out, sizeof(RangeEntry) * total))) return e;
+    const u32 wpb = 8;  // warps per block
+    k_class_hist<<<(nblk + wpb - 1) / wpb, 32 * wpb, 0, st>>>(t->table, total, hist, nblk);
+    k_scan_counts<<<1, 1024, 0, st>>>(hist, coffs, 9 * nblk);
+    k_class_scatter<<<(nblk + wpb - 1) / wpb, 32 * wpb, 0, st>>>(t->table, total, coffs, nblk, out);
+    for (int c = 0; c < 9 && !e; c++)
+      e = cudaMemcpyAsync(&t->cls[c], coffs + (size_t)c * nblk, sizeof(ull), cudaMemcpyDeviceToHost, st);
+    if (!e) e = cudaGetLastError();
+    if (!e) e = cudaStreamSynchronize(st);
+    cudaFree(hist);
+    cudaFree(coffs);
+    cudaFree(t->table);
+    t->table = out;
+    if (e) return e;
+  }
+  t->cls[9] = total;
   return cudaSuccess;
 }
 

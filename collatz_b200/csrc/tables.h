@@ -29,11 +29,18 @@ struct RangeEntry {
 };
 static_assert(sizeof(RangeEntry) == 16, "RangeEntry");
 
+// The survivor table is class-major: the survivors with r = 0 mod 9 in
+// residue order, then those with r = 1 mod 9, and so on.  For a block q the
+// mod-9 sieve keeps n = q 2^k + r iff (q 2^k + r) mod 9 is in {0,1,3,6,7},
+// which depends only on q mod 9 and r mod 9; so a block's seeds are 5 whole
+// classes, and a work item (64 consecutive entries of one class) holds only
+// seeds -- no entry is loaded and then dropped by the mod-9 sieve.
 struct RangeTable {
   uint32_t k = 0;
   uint32_t* bits = nullptr;         // 2^k bits
-  RangeEntry* table = nullptr;      // survivors in residue order
+  RangeEntry* table = nullptr;      // survivors, class-major (see above)
   unsigned long long count = 0;     // number of survivors
+  unsigned long long cls[10] = {};  // class c = table[cls[c], cls[c+1])
   unsigned long long violations = 0;// sieve validation failures (must be 0)
 };
 

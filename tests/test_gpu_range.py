@@ -51,6 +51,31 @@ def test_range_matches_oracle(verifier, case):
     _cmp(g, o)
 
 
+VARIANT_CASES = [CASES[i] for i in (0, 3, 4, 5, 6, 7, 8, 10)]
+
+
+@pytest.mark.parametrize("variant", range(4))
+def test_range_variants_match_oracle(verifier, variant):
+    """Every range-kernel variant (block shape) gives the oracle's results."""
+    import collatz_b200 as cb
+    from oracle import oracle as O
+    assert cb.lib().collatz_variant_count(1) == 4
+    v = verifier(26)
+    v.set_variant(1, variant)
+    try:
+        for off, size, k, mod9 in VARIANT_CASES:
+            g = v.verify_range(off, size, k, mod9)
+            o = O.range_verify(off, size, k, mod9, method=1, nthreads=NT)
+            _cmp(g, o)
+        reqs = [((1 << 40) + i * (1 << 24) + 9 * i, (1 << 18) + 1000 * i, 24, True) for i in range(6)]
+        reqs.append((17, 40000, 24, True))
+        for q, m in zip(reqs, v.verify_batch(reqs)):
+            o = O.range_verify(*q, method=1, nthreads=NT)
+            _cmp(m, o)
+    finally:
+        v.set_variant(1, 2)
+
+
 def test_batch_equals_alone(verifier):
     """Each request's result is the same alone and in a mixed batch."""
     v = verifier(26)
