@@ -48,11 +48,12 @@ UNIT = "seeds/s"
 # shifts, increment with carry, descent test).
 OPS_JUMP, OPS_ODD, OPS_EVEN = 16, 14, 12
 # DRAM bytes (read + write) of one k_range launch, measured with ncu.
-K_RANGE_DRAM_BYTES = 5.316864e6 + 0.210944e6
-# Frontier (k = 34): every block of 2^34 seeds streams the whole 2.43 GB
-# survivor table; ncu on a 4-block launch read 9.724289280e9 and wrote
-# 8.792576e6 bytes, so traffic per launch = blocks x this figure.
-K_RANGE_FRONTIER_DRAM_BYTES_PER_BLOCK = (9.724289280e9 + 8.792576e6) / 4
+K_RANGE_DRAM_BYTES = 5.339648e6 + 0.219904e6
+# Frontier (k = 34): every block of 2^34 seeds streams the 5 mod-9 classes
+# of the 2.43 GB survivor table that it keeps; ncu on a 4-block launch read
+# 5.406020352e9 and wrote 9.036032e6 bytes, so traffic per launch = blocks x
+# this figure.
+K_RANGE_FRONTIER_DRAM_BYTES_PER_BLOCK = (5.406020352e9 + 9.036032e6) / 4
 
 
 def dist_env():
@@ -500,8 +501,8 @@ def main():
                                           "figure does not grow with the block size"
                                           if args.workload == "block" else
                                           "ncu dram__bytes_read.sum + dram__bytes_write.sum of a 4-block "
-                                          "(2^36) launch, scaled by blocks: each 2^34 block streams the "
-                                          "2.43 GB survivor table once",
+                                          "(2^36) launch, scaled by blocks: each 2^34 block streams the 5 "
+                                          "mod-9 classes it keeps (1.35 GB of the 2.43 GB survivor table)",
                          "model": f"{ops_per_seed:.1f} algorithmic 32-bit ops per surviving seed "
                                   f"({OPS_JUMP} + {OPS_ODD} x {odd_per:.2f} odd runs + {OPS_EVEN} x "
                                   f"{even_per:.2f} even runs) x {res.seeds_checked} seeds per launch",
