@@ -6,16 +6,15 @@
 //
 // One kernel serves the plain single range and the batched form: the
 // host lowers every request into segments of work items, and persistent
-// warps claim items from a global cursor.  A sieved item is 256 consecutive
-// entries of the survivor table for one block q (seeds n = q 2^k + r); the
-// warp reads them with coalesced 16-byte loads, applies the mod-9 sieve
-// (n mod 9 from q mod 9 and the stored r mod 9), ranks the survivors with
-// popc + a warp scan into its shared-memory queue, and idle lanes pull
-// seeds from the queue.  A seed starts after one k-step jump,
-// T^k(n) + 1 = q 3^f + c (no descent is possible in those k steps), then
-// runs odd/even runs in 4 x 32-bit limbs with the exact stopping time and
-// excursion.  A value that could leave 2^128 sends the seed to the widen
-// list, re-run from scratch with 6 and then 8 limbs.
+// warps claim items from a global cursor.  A sieved item is 64 consecutive
+// entries of one mod-9 class of the (class-major) survivor table for one
+// block q (seeds n = q 2^k + r); the warp stages them with cp.async, sets
+// every seed up with a warp scan into its shared-memory queue, and idle
+// lanes pull seeds from the queue with one ballot per step.  A seed starts
+// after one k-step jump, T^k(n) + 1 = q 3^f + c (no descent is possible in
+// those k steps), then runs odd/even runs in 4 x 32-bit limbs with the exact
+// stopping time and excursion.  A value that could leave 2^128 sends the
+// seed to the widen list, re-run from scratch with 6 and then 8 limbs.
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -25,7 +24,7 @@
 namespace cz {
 
 constexpr u32 RQ = 128;          // queue entries per warp, power of two (>= 32 R + one item)
-constexpr u32 RR = 32;           // item slots per warp (< 32 queued entries span < 32 items)
+constexpr u32 RR = 32;           // item slots per warp (one per lane; see expand_one)
 constexpr u32 RWARPS = 7;
 constexpr u32 CLAIM = 8;         // items claimed per atomic
 constexpr u32 KEEP9 = 0xCBu;     // n mod 9 in {0,1,3,6,7} survives (cu:488)
@@ -48,6 +47,7 @@ struct RangeWarp {
   uint4 qa[RQ];
   uint4 qb[RQ];
   uint4 ring[RR];          // per item slot: request, sigma threshold, excursion window (lo, hi)
+  u32 ring_end[RR];        // per item slot: queue position after the item's last seed
   uint4 stage[RANGE_ITEM]; // survivor entries of the staged item (cp.async)
   u32 e[4][32];            // per lane: seed-local max excursion
   u32 pe[4][32];           // per lane: excursion of a pending offer
@@ -219,12 +219,199 @@ __device__ __forceinline__ void stage_next(WT& W, uint4* dst, const RangeArgs& A
   __syncwarp();
 }
 
+// Diagnostics of the stats variant: cycles waiting for staged entries,
+// staging the next item and refreshing thresholds; items expanded, seeds
+// set up by the k-step jump and by an exact replay of the first k steps.
+struct ExpandStats {
+  ull t_wait = 0, t_stage = 0, t_thr = 0, t_sub = 0;
+  u32 c_exp = 0, c_jump = 0, c_replay = 0;
+};
+
+// Expands the staged item into the warp's seed queue (W.qa, W.qb from
+// position tail): waits for its entries, starts staging the next item,
+// refreshes the request's thresholds when the request changes (and every 64
+// items), applies the mod-9 sieve when the segment asks for it, ranks the
+// seeds with a warp scan and writes each seed's start state -- the k-step
+// jump v = q 3^f + c, or n + 1 when the excursion threshold could be
+// reached within the first k steps -- with its item slot.  Sets exhausted
+// when no item is left.  Returns false, doing nothing, while the item slot
+// it would take still has seeds in the queue (queued seeds read their
+// request and thresholds from their item's slot when they are popped, so a
+// slot is reused only after the last seed of its previous item has left the
+// queue; the queue is then not empty).  Warp-uniform.
+template <bool STATS, class WT>
+__device__ __forceinline__ bool expand_one(WT& W, const RangeArgs& A, const uint4* __restrict__ T, u32 lane, u32 k,
+                                           u32 k9, const unsigned long long* s_p3, u32 head, u32& tail,
+                                           bool& exhausted, u32& w_thr_st, u32& w_req, u64& w_gate, ExpandStats& X) {
+  if ((int)(W.ring_end[W.ring_seq & (RR - 1)] - head) > 0) return false;
+  if (STATS) X.t_sub = clock64();
+  cp_async_wait_all();  // this lane's copies of the staged item
+  __syncwarp();
+  if (STATS) {
+    const ull now = clock64();
+    X.t_wait += now - X.t_sub;
+    X.t_sub = now;
+  }
+  const StagedItem it = W.nxt;
+  if (!it.valid) {
+    exhausted = true;
+    return true;
+  }
+  uint4 e[RANGE_ITEM / 32];
+  if (it.kind == 0) {
+#pragma unroll
+    for (u32 j = 0; j < RANGE_ITEM / 32; j++) e[j] = W.stage[j * 32 + lane];
+  }
+  __syncwarp();
+  stage_next(W, W.stage, A, T, lane);  // the following item's copies overlap with this expansion
+  if (STATS) {
+    const ull now = clock64();
+    X.t_stage += now - X.t_sub;
+    X.t_sub = now;
+  }
+  const u32 rq = it.req;
+  if (rq != w_req || ++W.since_thr >= 64) {  // thresholds of the request, refreshed now and then
+    ull sk = 0, ek = 0;
+    if (lane == 0 && rq != w_req && w_req != 0xFFFFFFFFu) {
+      if (W.acc_seeds) atomicAdd(&A.recs[w_req].seeds, W.acc_seeds);
+      atomicAdd(&A.recs[w_req].items_done, W.acc_items);
+    }
+    if (lane == 0) {
+      sk = *(volatile ull*)&A.recs[rq].st_key;
+      ek = *(volatile ull*)&A.recs[rq].e_key;
+    }
+    sk = __shfl_sync(FULL, sk, 0);
+    ek = __shfl_sync(FULL, ek, 0);
+    u32 t[4];
+    key_decode<4>(ek, t);
+    if (rq != w_req) {
+      w_thr_st = 0;
+      w_gate = 0;
+    }
+    w_thr_st = max(w_thr_st, (u32)min(sk, 0xFFFFFFFFull));
+    w_gate = max(w_gate, gate_window(t[1], t[2], t[3]));
+    __syncwarp();
+    if (lane == 0) {
+      if (rq != w_req) W.acc_seeds = W.acc_items = W.thr_bl = 0;
+      W.thr_bl = max(W.thr_bl, (u32)(ek >> 54));
+      W.since_thr = 0;
+    }
+    w_req = rq;
+    __syncwarp();
+  }
+  if (STATS) {
+    const ull now = clock64();
+    X.t_thr += now - X.t_sub;
+    X.t_sub = now;
+  }
+  const u32 w_thr_bl = W.thr_bl;
+  const u64 gate_w = w_gate;
+  const u32 slot = W.ring_seq & (RR - 1);
+  u32 mask = 0, total;
+  u32 pos;
+  if (it.kind == 0) {
+    const u32 q0 = (u32)it.q_lo, q1 = (u32)(it.q_lo >> 32), q2 = it.q_hi;
+    // per item (warp-uniform): n = q 2^k | r as limbs (k <= 34), bitlen(n) = bitlen(q) + k
+    const u32 kb = k & 31;
+    const u32 t0 = q0 << kb, t1 = __funnelshift_l(q0, q1, kb), t2 = __funnelshift_l(q1, q2, kb);
+    const u32 qk0 = (k >= 32) ? 0u : t0, qk1 = (k >= 32) ? t0 : t1, qk2 = (k >= 32) ? t1 : t2;
+    const u32 nbl = (q2 ? 96u - __clz(q2) : (q1 ? 64u - __clz(q1) : 32u - __clz(q0))) + k;
+    const u32 b9 = (mod9_96(q0, q1, q2) * k9) % 9u;
+    const u32 meta_item = (slot << 8) | (nbl << 16);
+    const bool jump_ok_base = true;
+#pragma unroll
+    for (u32 j = 0; j < RANGE_ITEM / 32; j++) {
+      if (it.sbase + j * 32 + lane < it.send) {
+        u32 x = b9 + ((e[j].y >> 16) & 0xFFu);
+        x = (x >= 9u) ? x - 9u : x;
+        if (!it.mod9 || ((KEEP9 >> x) & 1u)) mask |= 1u << j;
+      }
+    }
+    pos = tail + warp_excl_scan(__popc(mask), &total);
+#pragma unroll
+    for (u32 j = 0; j < RANGE_ITEM / 32; j++) {
+      if ((mask >> j) & 1u) {
+        const u32 f = (e[j].y >> 8) & 0xFFu, emax = e[j].y >> 24;
+        const u32 m0 = qk0 | e[j].x, m1 = qk1 | (e[j].y & 0xFFu);
+        u32 V0, V1, V2, V3, s0;
+        // T^0..T^k(n) < 2^emax (n + 1 + k) <= 2^(bitlen(n) + 1 + emax): skip them when that is
+        // below the excursion threshold, else replay the first k steps exactly
+        if (jump_ok_base && nbl + 1 + emax < w_thr_bl) {
+          // v = q 3^f + c in 32-bit limbs (3^f < 2^64, c < 2^64)
+          const u64 p = s_p3[f];
+          const u32 p0 = (u32)p, p1 = (u32)(p >> 32);
+          const u64 a = (u64)q0 * p0 + e[j].z;
+          const u64 bb = (u64)q0 * p1 + (a >> 32) + e[j].w;
+          const u64 cc = (u64)q1 * p0 + (u32)bb;
+          const u64 dd = (u64)q1 * p1 + (bb >> 32) + (cc >> 32);
+          V0 = (u32)a;
+          V1 = (u32)cc;
+          V2 = (u32)dd;
+          V3 = (u32)(dd >> 32);
+          if (q2) {  // q >= 2^64 (seeds >= 2^(64+k))
+            const u64 ee = (u64)q2 * p0 + V2;
+            V2 = (u32)ee;
+            V3 += q2 * p1 + (u32)(ee >> 32);
+          }
+          s0 = k;
+          if (STATS) X.c_jump++;
+        } else {
+          V0 = m0 + 1;
+          V1 = m1 + (V0 == 0);
+          V2 = qk2 + ((V0 | V1) == 0);
+          V3 = (V0 | V1 | V2) == 0;
+          s0 = 0;
+          if (STATS) X.c_replay++;
+        }
+        // excursion candidate T^s(n) = v - 1 <= v: bits 32..95 of v against the threshold
+        const u32 cand = ((V3 != 0) | ((((u64)V2 << 32) | V1) >= gate_w)) ? 1u : 0u;
+        W.qa[pos & (RQ - 1)] = make_uint4(V0, V1, V2, V3);
+        W.qb[pos & (RQ - 1)] = make_uint4(m0, m1, qk2, s0 | meta_item | (cand << 13));
+        pos++;
+      }
+    }
+  } else {
+    // integers below 2^k: [d, d + 64) of [q_lo, d_hi), no residue sieve
+    const ull d = it.q_lo + 2ull * lane;
+#pragma unroll
+    for (u32 j = 0; j < 2; j++) {
+      const ull n = d + j;
+      if (n < it.d_hi && n >= 2 && (!it.mod9 || ((KEEP9 >> (u32)(n % 9u)) & 1u))) mask |= 1u << j;
+    }
+    pos = tail + warp_excl_scan(__popc(mask), &total);
+#pragma unroll
+    for (u32 j = 0; j < 2; j++) {
+      if ((mask >> j) & 1u) {
+        const ull n = d + j;
+        const u32 nbl = 64u - __clzll(n);
+        const u32 cand = ((n >> 32) >= gate_w) ? 1u : 0u;
+        W.qa[pos & (RQ - 1)] = make_uint4((u32)(n + 1), (u32)((n + 1) >> 32), 0u, 0u);
+        W.qb[pos & (RQ - 1)] = make_uint4((u32)n, (u32)(n >> 32), 0u, (slot << 8) | (cand << 13) | (nbl << 16));
+        pos++;
+      }
+    }
+  }
+  __syncwarp();
+  if (lane == 0) {
+    W.ring[slot] = make_uint4(rq, w_thr_st, (u32)w_gate, (u32)(w_gate >> 32));
+    W.ring_end[slot] = tail + total;
+    W.ring_seq++;
+    W.acc_seeds += total;
+    W.acc_items++;
+  }
+  if (STATS) X.c_exp++;
+  tail += total;
+  __syncwarp();
+  return true;
+}
+
 template <int R, int MINB, bool STATS = false>
 __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) {
   // diagnostics (STATS variant only): run pairs, excursion slow paths, replays, jumps, pops,
   // expansions, passes, offers; clock64 cycles per phase (lane 0)
-  u32 c_iter = 0, c_slow = 0, c_replay = 0, c_jump = 0, c_pop = 0, c_exp = 0, c_blk = 0, c_offer = 0;
-  ull t_offer = 0, t_refill = 0, t_lanes = 0, t_mark = 0, t_stage = 0, t_thr = 0, t_wait = 0, t_sub = 0;
+  u32 c_iter = 0, c_slow = 0, c_pop = 0, c_blk = 0, c_offer = 0;
+  ull t_offer = 0, t_refill = 0, t_lanes = 0, t_mark = 0;
+  ExpandStats X;
   extern __shared__ __align__(16) unsigned char range_smem[];
   RangeWarp* S = reinterpret_cast<RangeWarp*>(range_smem);
   __shared__ unsigned long long s_p3[41];
@@ -252,6 +439,7 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
     W.chunk = W.since_thr = W.ring_seq = W.thr_bl = W.head = 0;
     W.nxt.valid = 0;
   }
+  W.ring_end[lane] = 0;  // RR == 32: one slot per lane
   __syncthreads();
 
   const u32 k = A.k;
@@ -351,163 +539,7 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
     }
     // ---- refill: keep 32 R seeds queued (each lane pops at most R per pass) ----
     while (tail - head < 32u * R && !exhausted) {
-      if (STATS) t_sub = clock64();
-      cp_async_wait_all();  // this lane's copies of the staged item
-      __syncwarp();
-      if (STATS) {
-        const ull now = clock64();
-        t_wait += now - t_sub;
-        t_sub = now;
-      }
-      const StagedItem it = W.nxt;
-      if (!it.valid) {
-        exhausted = true;
-        break;
-      }
-      uint4 e[RANGE_ITEM / 32];
-      if (it.kind == 0) {
-#pragma unroll
-        for (u32 j = 0; j < RANGE_ITEM / 32; j++) e[j] = W.stage[j * 32 + lane];
-      }
-      __syncwarp();
-      stage_next(W, W.stage, A, T, lane);  // the following item's copies overlap with this expansion
-      if (STATS) {
-        const ull now = clock64();
-        t_stage += now - t_sub;
-        t_sub = now;
-      }
-      const u32 rq = it.req;
-      if (rq != w_req || ++W.since_thr >= 64) {  // thresholds of the request, refreshed now and then
-        ull sk = 0, ek = 0;
-        if (lane == 0 && rq != w_req && w_req != 0xFFFFFFFFu) {
-          if (W.acc_seeds) atomicAdd(&A.recs[w_req].seeds, W.acc_seeds);
-          atomicAdd(&A.recs[w_req].items_done, W.acc_items);
-        }
-        if (lane == 0) {
-          sk = *(volatile ull*)&A.recs[rq].st_key;
-          ek = *(volatile ull*)&A.recs[rq].e_key;
-        }
-        sk = __shfl_sync(FULL, sk, 0);
-        ek = __shfl_sync(FULL, ek, 0);
-        u32 t[4];
-        key_decode<4>(ek, t);
-        if (rq != w_req) {
-          w_thr_st = 0;
-          w_gate = 0;
-        }
-        w_thr_st = max(w_thr_st, (u32)min(sk, 0xFFFFFFFFull));
-        w_gate = max(w_gate, gate_window(t[1], t[2], t[3]));
-        __syncwarp();
-        if (lane == 0) {
-          if (rq != w_req) W.acc_seeds = W.acc_items = W.thr_bl = 0;
-          W.thr_bl = max(W.thr_bl, (u32)(ek >> 54));
-          W.since_thr = 0;
-        }
-        w_req = rq;
-        __syncwarp();
-      }
-      if (STATS) {
-        const ull now = clock64();
-        t_thr += now - t_sub;
-        t_sub = now;
-      }
-      const u32 w_thr_bl = W.thr_bl;
-      const u64 gate_w = w_gate;
-      const u32 slot = W.ring_seq & (RR - 1);
-      u32 mask = 0, total;
-      u32 pos;
-      if (it.kind == 0) {
-        const u32 q0 = (u32)it.q_lo, q1 = (u32)(it.q_lo >> 32), q2 = it.q_hi;
-        // per item (warp-uniform): n = q 2^k | r as limbs (k <= 34), bitlen(n) = bitlen(q) + k
-        const u32 kb = k & 31;
-        const u32 t0 = q0 << kb, t1 = __funnelshift_l(q0, q1, kb), t2 = __funnelshift_l(q1, q2, kb);
-        const u32 qk0 = (k >= 32) ? 0u : t0, qk1 = (k >= 32) ? t0 : t1, qk2 = (k >= 32) ? t1 : t2;
-        const u32 nbl = (q2 ? 96u - __clz(q2) : (q1 ? 64u - __clz(q1) : 32u - __clz(q0))) + k;
-        const u32 b9 = (mod9_96(q0, q1, q2) * k9) % 9u;
-        const u32 meta_item = (slot << 8) | (nbl << 16);
-        const bool jump_ok_base = true;
-#pragma unroll
-        for (u32 j = 0; j < RANGE_ITEM / 32; j++) {
-          if (it.sbase + j * 32 + lane < it.send) {
-            u32 x = b9 + ((e[j].y >> 16) & 0xFFu);
-            x = (x >= 9u) ? x - 9u : x;
-            if (!it.mod9 || ((KEEP9 >> x) & 1u)) mask |= 1u << j;
-          }
-        }
-        pos = tail + warp_excl_scan(__popc(mask), &total);
-#pragma unroll
-        for (u32 j = 0; j < RANGE_ITEM / 32; j++) {
-          if ((mask >> j) & 1u) {
-            const u32 f = (e[j].y >> 8) & 0xFFu, emax = e[j].y >> 24;
-            const u32 m0 = qk0 | e[j].x, m1 = qk1 | (e[j].y & 0xFFu);
-            u32 V0, V1, V2, V3, s0;
-            // T^0..T^k(n) < 2^emax (n + 1 + k) <= 2^(bitlen(n) + 1 + emax): skip them when that is
-            // below the excursion threshold, else replay the first k steps exactly
-            if (jump_ok_base && nbl + 1 + emax < w_thr_bl) {
-              // v = q 3^f + c in 32-bit limbs (3^f < 2^64, c < 2^64)
-              const u64 p = s_p3[f];
-              const u32 p0 = (u32)p, p1 = (u32)(p >> 32);
-              const u64 a = (u64)q0 * p0 + e[j].z;
-              const u64 bb = (u64)q0 * p1 + (a >> 32) + e[j].w;
-              const u64 cc = (u64)q1 * p0 + (u32)bb;
-              const u64 dd = (u64)q1 * p1 + (bb >> 32) + (cc >> 32);
-              V0 = (u32)a;
-              V1 = (u32)cc;
-              V2 = (u32)dd;
-              V3 = (u32)(dd >> 32);
-              if (q2) {  // q >= 2^64 (seeds >= 2^(64+k))
-                const u64 ee = (u64)q2 * p0 + V2;
-                V2 = (u32)ee;
-                V3 += q2 * p1 + (u32)(ee >> 32);
-              }
-              s0 = k;
-              if (STATS) c_jump++;
-            } else {
-              V0 = m0 + 1;
-              V1 = m1 + (V0 == 0);
-              V2 = qk2 + ((V0 | V1) == 0);
-              V3 = (V0 | V1 | V2) == 0;
-              s0 = 0;
-              if (STATS) c_replay++;
-            }
-            // excursion candidate T^s(n) = v - 1 <= v: bits 32..95 of v against the threshold
-            const u32 cand = ((V3 != 0) | ((((u64)V2 << 32) | V1) >= gate_w)) ? 1u : 0u;
-            W.qa[pos & (RQ - 1)] = make_uint4(V0, V1, V2, V3);
-            W.qb[pos & (RQ - 1)] = make_uint4(m0, m1, qk2, s0 | meta_item | (cand << 13));
-            pos++;
-          }
-        }
-      } else {
-        // integers below 2^k: [d, d + 64) of [q_lo, d_hi), no residue sieve
-        const ull d = it.q_lo + 2ull * lane;
-#pragma unroll
-        for (u32 j = 0; j < 2; j++) {
-          const ull n = d + j;
-          if (n < it.d_hi && n >= 2 && (!it.mod9 || ((KEEP9 >> (u32)(n % 9u)) & 1u))) mask |= 1u << j;
-        }
-        pos = tail + warp_excl_scan(__popc(mask), &total);
-#pragma unroll
-        for (u32 j = 0; j < 2; j++) {
-          if ((mask >> j) & 1u) {
-            const ull n = d + j;
-            const u32 nbl = 64u - __clzll(n);
-            const u32 cand = ((n >> 32) >= gate_w) ? 1u : 0u;
-            W.qa[pos & (RQ - 1)] = make_uint4((u32)(n + 1), (u32)((n + 1) >> 32), 0u, 0u);
-            W.qb[pos & (RQ - 1)] = make_uint4((u32)n, (u32)(n >> 32), 0u, (slot << 8) | (cand << 13) | (nbl << 16));
-            pos++;
-          }
-        }
-      }
-      __syncwarp();
-      if (lane == 0) {
-        W.ring[slot] = make_uint4(rq, w_thr_st, (u32)w_gate, (u32)(w_gate >> 32));
-        W.ring_seq++;
-        W.acc_seeds += total;
-        W.acc_items++;
-      }
-      if (STATS) c_exp++;
-      tail += total;
-      __syncwarp();
+      if (!expand_one<STATS>(W, A, T, lane, k, k9, s_p3, head, tail, exhausted, w_thr_st, w_req, w_gate, X)) break;
     }
     __syncwarp();
     if (STATS) {
@@ -630,12 +662,12 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
     atomicAdd(&A.stats[8], t_offer);
     atomicAdd(&A.stats[9], t_refill);
     atomicAdd(&A.stats[10], t_lanes);
-    atomicAdd(&A.stats[11], t_wait);
-    atomicAdd(&A.stats[12], t_stage);
-    atomicAdd(&A.stats[13], t_thr);
+    atomicAdd(&A.stats[11], X.t_wait);
+    atomicAdd(&A.stats[12], X.t_stage);
+    atomicAdd(&A.stats[13], X.t_thr);
   }
   if (STATS && A.stats) {
-    u32 c[8] = {c_iter, c_slow, c_replay, c_jump, c_pop, c_exp, c_blk, c_offer};
+    u32 c[8] = {c_iter, c_slow, X.c_replay, X.c_jump, c_pop, X.c_exp, c_blk, c_offer};
 #pragma unroll
     for (int i = 0; i < 8; i++) {
       u32 x = c[i];

@@ -76,6 +76,26 @@ def test_range_variants_match_oracle(verifier, variant):
         v.set_variant(1, 2)
 
 
+def test_batch_of_tiny_requests(verifier):
+    """Hundreds of requests of 1..400 seeds in one launch: work items of one
+    or two seeds each, so a warp's seed queue holds seeds of far more items
+    than it has item slots; every request must still get exactly its own
+    seeds and maxima."""
+    import random
+    from oracle import oracle as O
+    rng = random.Random(77)
+    reqs = []
+    for _ in range(600):
+        off = rng.randrange(1 << 40, 1 << 50)
+        reqs.append((off, rng.randint(1, 400), 24, True))
+    reqs.append((3, 300, 24, True))  # below 2^k
+    v = verifier(26)
+    got = v.verify_batch(reqs)
+    for q, g in zip(reqs, got):
+        o = O.range_verify(*q, method=1)
+        _cmp(g, o)
+
+
 def test_batch_equals_alone(verifier):
     """Each request's result is the same alone and in a mixed batch."""
     v = verifier(26)
