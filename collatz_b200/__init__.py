@@ -23,6 +23,7 @@ OK = 0
 E_ARG, E_CUDA, E_NOMEM, E_LIMIT, E_DEVICE, E_TIMEOUT, E_STATE, E_ADMISSION, E_NODEV = \
     -1, -2, -3, -4, -5, -6, -7, -8, -9
 RANGE_NO_MOD9 = 0x1
+RANGE_NEGATIVE = 0x2
 VARIANT_AUTO = 0xFFFFFFFF
 BV_WORDS = (1 << 19) + 32
 
@@ -227,10 +228,12 @@ def make_case(base, sigfig, threepower, number, doubleeven, numevens) -> Case:
     return c
 
 
-def make_range(offset: int, size: int, k: int = 0, mod9: bool = True) -> Range:
+def make_range(offset: int, size: int, k: int = 0, mod9: bool = True, negative: bool = False) -> Range:
+    """negative: seeds m stand for -m (the map T'(m) = (3m-1)/2, m/2)."""
     r = Range()
     r.offset[0], r.offset[1] = offset & (2**64 - 1), offset >> 64
-    r.size, r.k, r.flags = size, k, 0 if mod9 else RANGE_NO_MOD9
+    r.size, r.k = size, k
+    r.flags = (0 if mod9 else RANGE_NO_MOD9) | (RANGE_NEGATIVE if negative else 0)
     return r
 
 
@@ -412,8 +415,8 @@ class Verifier:
         return cnt.value, bytes(buf)
 
     def verify_range(self, offset: int, size: int, k: int = 0, mod9: bool = True,
-                     check: bool = True) -> RangeResult:
-        r = make_range(offset, size, k, mod9)
+                     check: bool = True, negative: bool = False) -> RangeResult:
+        r = make_range(offset, size, k, mod9, negative)
         out = RangeResultC()
         rc = lib().collatz_verify_range(self._h, C.byref(r), C.byref(out))
         if check:
@@ -566,10 +569,10 @@ class Server:
         self._bufs: dict[int, tuple] = {}
         self._lock = threading.Lock()
 
-    def submit_range(self, offset: int, size: int, k: int = 0, mod9: bool = True) -> int:
+    def submit_range(self, offset: int, size: int, k: int = 0, mod9: bool = True, negative: bool = False) -> int:
         q = RequestC()
         q.kind = REQ_RANGE
-        q.range = make_range(offset, size, k, mod9)
+        q.range = make_range(offset, size, k, mod9, negative)
         t = C.c_uint64()
         rc = lib().collatz_server_submit(self._h, C.byref(q), C.byref(t))
         if rc:

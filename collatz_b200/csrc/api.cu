@@ -64,14 +64,15 @@ void rec_to_range_result(const ReqRec& r, collatz_range_result* out) {
 // Range tables and lowering of requests into work segments.
 // ---------------------------------------------------------------------
 
-int get_range_tables(collatz_ctx* c, uint32_t k, RangeTables** out) {
-  auto it = c->rt.find(k);
+int get_range_tables(collatz_ctx* c, uint32_t k, RangeTables** out, bool negative) {
+  const uint32_t key = k | (negative ? 0x100u : 0u);
+  auto it = c->rt.find(key);
   if (it != c->rt.end()) {
     *out = &it->second;
     return COLLATZ_OK;
   }
   RangeTables T;
-  cudaError_t e = build_range_table(&T.dev, k, true, c->own_stream);
+  cudaError_t e = build_range_table(&T.dev, k, true, c->own_stream, negative);
   if (e != cudaSuccess) {
     free_range_table(&T.dev);
     return set_cuda_error(c, e, "build_range_table");
@@ -88,7 +89,7 @@ int get_range_tables(collatz_ctx* c, uint32_t k, RangeTables** out) {
     T.residues.resize(T.dev.count);
     for (size_t i = 0; i < h.size(); i++) T.residues[i] = (uint64_t)h[i].r_lo | ((uint64_t)(h[i].meta & 0xFF) << 32);
   }
-  auto ins = c->rt.emplace(k, std::move(T));
+  auto ins = c->rt.emplace(key, std::move(T));
   *out = &ins.first->second;
   return COLLATZ_OK;
 }
@@ -127,6 +128,8 @@ int lower_range(collatz_ctx* c, const collatz_range& r, uint32_t req, const Rang
   const u128 O = u128_of(r.offset), S = r.size, E = O + S;
   if (r.size > (1ull << 48) || E > ((u128)1 << 96) || E < O) return COLLATZ_E_LIMIT;
   const uint32_t mod9 = (r.flags & COLLATZ_RANGE_NO_MOD9) ? 0u : 1u;
+  // kept residues mod 9: {0,1,3,6,7} for T (cu:488), {0,2,3,6,8} for the negative variant
+  const uint32_t keep9 = (r.flags & COLLATZ_RANGE_NEGATIVE) ? 0x14Du : 0xCBu;
   const u128 K = (u128)1 << k;
   if (S == 0) return COLLATZ_OK;
   if (O < K) {  // integers below 2^k: no residue sieve
@@ -153,7 +156,7 @@ int lower_range(collatz_ctx* c, const collatz_range& r, uint32_t req, const Rang
   const u128 qa = lo >> k, qb = (E - 1) >> k;
   const uint32_t k9 = (uint32_t)(((u128)1 << (k % 6)) % 9);  // 2^k mod 9 (2^6 = 1 mod 9)
   auto live = [&](u128 q, uint32_t cl) {
-    return !mod9 || ((0xCBu >> (((uint32_t)(q % 9) * k9 + cl) % 9)) & 1u);  // keep {0,1,3,6,7} (cu:488)
+    return !mod9 || ((keep9 >> (((uint32_t)(q % 9) * k9 + cl) % 9)) & 1u);
   };
   auto add = [&](u128 q, u128 nq, uint32_t stride, uint32_t s_lo, uint32_t s_hi) {
     if (s_lo >= s_hi || nq == 0) return;
@@ -659,7 +662,7 @@ struct collatz_plan {
   unsigned long long items = 0;
   DevBuf d_segs, d_recs, d_cursor, d_widen, d_widen2, d_wcount, d_stats;
   HostBuf h_recs;
-  bool stats = false;
+  bool stats = false, negative = false;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   float last_ms = 0;
@@ -667,10 +670,13 @@ struct collatz_plan {
 
 static int plan_build(collatz_ctx* c, const collatz_range* r, uint32_t n, collatz_plan* p) {
   const uint32_t k = r[0].k ? r[0].k : c->cfg.range_k;
-  for (uint32_t i = 0; i < n; i++)
-    if ((r[i].k ? r[i].k : c->cfg.range_k) != k) return COLLATZ_E_ARG;  // one sieve per launch
+  const bool neg = (r[0].flags & COLLATZ_RANGE_NEGATIVE) != 0;
+  for (uint32_t i = 0; i < n; i++)  // one sieve (k, sign) per launch
+    if ((r[i].k ? r[i].k : c->cfg.range_k) != k || ((r[i].flags & COLLATZ_RANGE_NEGATIVE) != 0) != neg)
+      return COLLATZ_E_ARG;
   if (k < 8 || k > 34) return COLLATZ_E_ARG;
-  int rc = get_range_tables(c, k, &p->T);
+  p->negative = neg;
+  int rc = get_range_tables(c, k, &p->T, neg);
   if (rc) return rc;
   for (uint32_t i = 0; i < n; i++) {
     rc = lower_range(c, r[i], i, *p->T, p->segs, p->items);
@@ -704,6 +710,7 @@ static int plan_build(collatz_ctx* c, const collatz_range* r, uint32_t n, collat
   a.widen_count = p->d_wcount.as<uint32_t>();
   a.iter_cap = c->iter_cap;
   a.stats = nullptr;
+  a.negative = p->negative ? 1u : 0u;
   const char* dbg = getenv("COLLATZ_RANGE_STATS");
   p->stats = dbg && dbg[0] == '1';
   if (p->stats) {
@@ -717,13 +724,14 @@ static int plan_build(collatz_ctx* c, const collatz_range* r, uint32_t n, collat
   if (!e) e = cudaMemsetAsync(p->d_cursor.p, 0, sizeof(unsigned long long), s);
   if (!e) e = cudaMemsetAsync(p->d_wcount.p, 0, sizeof(uint32_t) * 2, s);
   if (!e && p->stats) e = cudaMemsetAsync(p->d_stats.p, 0, 16 * sizeof(unsigned long long), s);
-  if (!e) e = p->stats ? launch_range_stats(a, grid, s) : launch_range(a, c->range_variant, grid, s);
+  if (!e) e = (p->stats && !p->negative) ? launch_range_stats(a, grid, s) : launch_range(a, c->range_variant, grid, s);
   if (!e)
     e = launch_range_wide(p->d_widen.as<WidenEntry>(), p->d_wcount.as<uint32_t>(), WIDEN_CAP, 6, a.recs,
-                          p->d_widen2.as<WidenEntry>(), WIDEN_CAP, p->d_wcount.as<uint32_t>() + 1, c->iter_cap, s);
+                          p->d_widen2.as<WidenEntry>(), WIDEN_CAP, p->d_wcount.as<uint32_t>() + 1, c->iter_cap, s,
+                          p->negative);
   if (!e)
     e = launch_range_wide(p->d_widen2.as<WidenEntry>(), p->d_wcount.as<uint32_t>() + 1, WIDEN_CAP, 8, a.recs,
-                          nullptr, 0, nullptr, c->iter_cap, s);
+                          nullptr, 0, nullptr, c->iter_cap, s, p->negative);
   if (!e) e = cudaMemcpyAsync(p->h_recs.p, p->d_recs.p, sizeof(ReqRec) * std::max(1u, n), cudaMemcpyDeviceToHost, s);
   cudaError_t e2 = cudaStreamEndCapture(s, &p->graph);
   if (e) return set_cuda_error(c, e, "plan capture");

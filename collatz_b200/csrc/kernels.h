@@ -72,6 +72,7 @@ struct RangeArgs {
   uint32_t widen_cap;
   uint32_t* widen_count;
   uint32_t iter_cap;              // odd/even run pairs per seed before ERR_ITER_CAP
+  uint32_t negative;              // 1: the negative-integer variant (a table built for it)
   unsigned long long* stats;      // diagnostics counters (stats variant only), may be null
 };
 int range_variants();
@@ -86,7 +87,7 @@ cudaError_t range_occupancy(int variant, int* blocks_per_sm);
 // sit in a captured graph right behind the range kernel.
 cudaError_t launch_range_wide(const WidenEntry* list, const uint32_t* count, uint32_t cap, int limbs,
                               ReqRec* recs, WidenEntry* next, uint32_t next_cap, uint32_t* next_count,
-                              uint32_t iter_cap, cudaStream_t st);
+                              uint32_t iter_cap, cudaStream_t st, bool negative = false);
 
 // ---------------- trajectory queries (traj.cu) ----------------
 struct TrajArgs {

@@ -28,6 +28,10 @@ constexpr u32 RR = 32;           // item slots per warp (one per lane; see expan
 constexpr u32 RWARPS = 7;
 constexpr u32 CLAIM = 8;         // items claimed per atomic
 constexpr u32 KEEP9 = 0xCBu;     // n mod 9 in {0,1,3,6,7} survives (cu:488)
+// Negative variant T'(m) = (3m-1)/2, m/2: m = 1 mod 3 (m > 1) is T' of the smaller
+// (2m+1)/3 and m = 5 mod 9 (m > 5) is T'^3 of the smaller (8m+5)/9, so m mod 9 in
+// {0,2,3,6,8} survives (and m = 5, the minimum of a cycle).
+constexpr u32 KEEP9N = 0x14Du;
 constexpr u32 OVF3 = 1u << 23;   // v >= 2^119 after an odd run: the next run could leave 128 bits
 constexpr u32 ST_CAP = 1u << 20; // steps per seed before ERR_ITER_CAP
 
@@ -99,6 +103,26 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// The trajectory value a run state stands for: T^s(n) = v - 1 (the state is
+// v = T^s(n) + 1), or for the negative variant T'^s(n) = u + 1 (the state is
+// u = T'^s(n) - 1).
+template <bool NEG>
+__device__ __forceinline__ void value_of(u32 v0, u32 v1, u32 v2, u32 v3, u32* x) {
+  if (NEG) {
+    x[0] = v0 + 1;
+    const u32 c0 = x[0] == 0;
+    x[1] = v1 + c0;
+    const u32 c1 = c0 & (x[1] == 0);
+    x[2] = v2 + c1;
+    x[3] = v3 + (c1 & (x[2] == 0));
+  } else {
+    x[0] = v0 - 1;
+    x[1] = v1 - (v0 == 0);
+    x[2] = v2 - ((v0 | v1) == 0);
+    x[3] = v3 - ((v0 | v1 | v2) == 0);
+  }
+}
 
 // Queue a seed for the 192/256-bit re-run.
 __device__ __forceinline__ void widen_seed(const RangeArgs& A, u32 req, u32 n0, u32 n1, u32 n2) {
@@ -239,7 +263,7 @@ struct ExpandStats {
 // request and thresholds from their item's slot when they are popped, so a
 // slot is reused only after the last seed of its previous item has left the
 // queue; the queue is then not empty).  Warp-uniform.
-template <bool STATS, class WT>
+template <bool STATS, bool NEG, class WT>
 __device__ __forceinline__ bool expand_one(WT& W, const RangeArgs& A, const uint4* __restrict__ T, u32 lane, u32 k,
                                            u32 k9, const unsigned long long* s_p3, u32 head, u32& tail,
                                            bool& exhausted, u32& w_thr_st, u32& w_req, u64& w_gate, ExpandStats& X) {
@@ -324,7 +348,7 @@ __device__ __forceinline__ bool expand_one(WT& W, const RangeArgs& A, const uint
       if (it.sbase + j * 32 + lane < it.send) {
         u32 x = b9 + ((e[j].y >> 16) & 0xFFu);
         x = (x >= 9u) ? x - 9u : x;
-        if (!it.mod9 || ((KEEP9 >> x) & 1u)) mask |= 1u << j;
+        if (!it.mod9 || (((NEG ? KEEP9N : KEEP9) >> x) & 1u)) mask |= 1u << j;
       }
     }
     pos = tail + warp_excl_scan(__popc(mask), &total);
@@ -356,15 +380,23 @@ __device__ __forceinline__ bool expand_one(WT& W, const RangeArgs& A, const uint
           s0 = k;
           if (STATS) X.c_jump++;
         } else {
-          V0 = m0 + 1;
-          V1 = m1 + (V0 == 0);
-          V2 = qk2 + ((V0 | V1) == 0);
-          V3 = (V0 | V1 | V2) == 0;
+          if (NEG) {  // u = n - 1 (n >= 2^k: no borrow out of 96 bits)
+            V0 = m0 - 1;
+            V1 = m1 - (m0 == 0);
+            V2 = qk2 - ((m0 | m1) == 0);
+            V3 = 0;
+          } else {
+            V0 = m0 + 1;
+            V1 = m1 + (V0 == 0);
+            V2 = qk2 + ((V0 | V1) == 0);
+            V3 = (V0 | V1 | V2) == 0;
+          }
           s0 = 0;
           if (STATS) X.c_replay++;
         }
         // excursion candidate T^s(n) = v - 1 <= v: bits 32..95 of v against the threshold
-        const u32 cand = ((V3 != 0) | ((((u64)V2 << 32) | V1) >= gate_w)) ? 1u : 0u;
+        // T': the candidate is u + 1, whose window exceeds u's by at most 1
+        const u32 cand = ((V3 != 0) | ((((u64)V2 << 32) | V1) >= (NEG ? gate_w - (gate_w != 0) : gate_w))) ? 1u : 0u;
         W.qa[pos & (RQ - 1)] = make_uint4(V0, V1, V2, V3);
         W.qb[pos & (RQ - 1)] = make_uint4(m0, m1, qk2, s0 | meta_item | (cand << 13));
         pos++;
@@ -376,7 +408,9 @@ __device__ __forceinline__ bool expand_one(WT& W, const RangeArgs& A, const uint
 #pragma unroll
     for (u32 j = 0; j < 2; j++) {
       const ull n = d + j;
-      if (n < it.d_hi && n >= 2 && (!it.mod9 || ((KEEP9 >> (u32)(n % 9u)) & 1u))) mask |= 1u << j;
+      const u32 r9 = (u32)(n % 9u);
+      const bool keep9 = NEG ? ((((KEEP9N >> r9) & 1u) != 0) | (n == 5)) : (((KEEP9 >> r9) & 1u) != 0);
+      if (n < it.d_hi && n >= 2 && (!it.mod9 || keep9)) mask |= 1u << j;
     }
     pos = tail + warp_excl_scan(__popc(mask), &total);
 #pragma unroll
@@ -385,7 +419,8 @@ __device__ __forceinline__ bool expand_one(WT& W, const RangeArgs& A, const uint
         const ull n = d + j;
         const u32 nbl = 64u - __clzll(n);
         const u32 cand = ((n >> 32) >= gate_w) ? 1u : 0u;
-        W.qa[pos & (RQ - 1)] = make_uint4((u32)(n + 1), (u32)((n + 1) >> 32), 0u, 0u);
+        const ull v = NEG ? n - 1 : n + 1;
+        W.qa[pos & (RQ - 1)] = make_uint4((u32)v, (u32)(v >> 32), 0u, 0u);
         W.qb[pos & (RQ - 1)] = make_uint4((u32)n, (u32)(n >> 32), 0u, (slot << 8) | (cand << 13) | (nbl << 16));
         pos++;
       }
@@ -405,7 +440,7 @@ __device__ __forceinline__ bool expand_one(WT& W, const RangeArgs& A, const uint
   return true;
 }
 
-template <int R, int MINB, bool STATS = false>
+template <int R, int MINB, bool STATS = false, bool NEG = false>
 __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) {
   // diagnostics (STATS variant only): run pairs, excursion slow paths, replays, jumps, pops,
   // expansions, passes, offers; clock64 cycles per phase (lane 0)
@@ -481,11 +516,13 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
         gate = ((u64)g_.w << 32) | g_.z;                                             \
       }                                                                              \
       evalid = (b_.w >> 13) & 1u;                                                    \
-      if (evalid) { /* T^s(n) = v - 1 is an excursion candidate */                   \
-        W.e[0][lane] = v0 - 1;                                                       \
-        W.e[1][lane] = v1 - (v0 == 0);                                               \
-        W.e[2][lane] = v2 - ((v0 | v1) == 0);                                        \
-        W.e[3][lane] = v3 - ((v0 | v1 | v2) == 0);                                   \
+      if (evalid) { /* the value T^s(n) = v -/+ 1 is an excursion candidate */        \
+        u32 x_[4];                                                                   \
+        value_of<NEG>(v0, v1, v2, v3, x_);                                           \
+        W.e[0][lane] = x_[0];                                                        \
+        W.e[1][lane] = x_[1];                                                        \
+        W.e[2][lane] = x_[2];                                                        \
+        W.e[3][lane] = x_[3];                                                        \
       }                                                                              \
       active = true;                                                                 \
       if (STATS) c_pop++;                                                            \
@@ -539,7 +576,8 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
     }
     // ---- refill: keep 32 R seeds queued (each lane pops at most R per pass) ----
     while (tail - head < 32u * R && !exhausted) {
-      if (!expand_one<STATS>(W, A, T, lane, k, k9, s_p3, head, tail, exhausted, w_thr_st, w_req, w_gate, X)) break;
+      if (!expand_one<STATS, NEG>(W, A, T, lane, k, k9, s_p3, head, tail, exhausted, w_thr_st, w_req, w_gate, X))
+        break;
     }
     __syncwarp();
     if (STATS) {
@@ -573,8 +611,10 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
         st += a;
         if (STATS) c_iter++;
       }
-      // excursion / overflow gate: (v3:v2:v1) >= (0:gate)
-      if (!lt96c(v1, v2, v3, (u32)gate, (u32)(gate >> 32), 0u)) {
+      // excursion / overflow gate: (v3:v2:v1) >= (0:gate) (T': >= gate - 1, since the
+      // value v + 1 has a window at most 1 above v's)
+      const u64 g_eff = NEG ? gate - (gate != 0) : gate;
+      if (!lt96c(v1, v2, v3, (u32)g_eff, (u32)(g_eff >> 32), 0u)) {
         if (v3 >= OVF3) {
           // the next odd run could leave 128 bits: re-run this seed with wider limbs
           widen_seed(A, req, n0, n1, n2);
@@ -583,7 +623,9 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
         }
         // excursion candidate (bits 32..95 at or above the threshold)
         if (STATS) c_slow++;
-        const u32 x0 = v0 - 1, x1 = v1 - (v0 == 0), x2 = v2 - ((v0 | v1) == 0), x3 = v3 - ((v0 | v1 | v2) == 0);
+        u32 xv[4];
+        value_of<NEG>(v0, v1, v2, v3, xv);
+        const u32 x0 = xv[0], x1 = xv[1], x2 = xv[2], x3 = xv[3];
         bool take_it = !evalid;
         if (evalid) take_it = lt96c(W.e[0][lane], W.e[1][lane], W.e[2][lane], x0, x1, x2) ? (W.e[3][lane] <= x3)
                                                                                            : (W.e[3][lane] < x3);
@@ -595,7 +637,19 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
           evalid = true;
         }
       }
-      v0 -= 1;  // v0 == 0 gives b == 0 below, and the borrow cancels against the +1
+      if (NEG) {
+        // t = u + 1 with a full carry (a low limb of all ones gives b = 31 below)
+        v0 += 1;
+        if (v0 == 0) {
+          v1 += 1;
+          if (v1 == 0) {
+            v2 += 1;
+            if (v2 == 0) v3 += 1;
+          }
+        }
+      } else {
+        v0 -= 1;  // v0 == 0 gives b == 0 below, and the borrow cancels against the +1
+      }
       const u32 b = ctz32(v0 | 0x80000000u);
       const u32 w0 = __funnelshift_r(v0, v1, b), w1 = __funnelshift_r(v1, v2, b);
       const u32 w2 = __funnelshift_r(v2, v3, b), w3 = v3 >> b;
@@ -642,6 +696,16 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
         }
         active = false;
         // a lane with a pending offer waits for the next pass (its scratch is in use)
+      } else if (NEG && (w3 == 0) & (w0 == n0) & (w1 == n1) & (w2 == n2)) {
+        // T': back at the seed -- it lies on a cycle and never descends (the minima 5, 17)
+        atomicAdd(&A.recs[req].failures, 1ull);
+        active = false;
+      } else if (NEG) {
+        // u = w - 1 (w >= 1)
+        v0 = w0 - 1;
+        v1 = w1 - (w0 == 0);
+        v2 = w2 - ((w0 | w1) == 0);
+        v3 = w3 - ((w0 | w1 | w2) == 0);
       } else {
         v0 = w0 + 1;
         v1 = w1;
@@ -687,7 +751,7 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
 // ------------------------------------------------------------------
 // Wide re-run: one seed per thread with L limbs, from scratch.
 // ------------------------------------------------------------------
-template <int L>
+template <int L, bool NEG>
 __global__ void __launch_bounds__(128) k_range_wide(const WidenEntry* __restrict__ list, const u32* count,
                                                    u32 cap, ReqRec* recs, WidenEntry* next, u32 next_cap,
                                                    u32* next_count, u32 iter_cap) {
@@ -703,7 +767,7 @@ __global__ void __launch_bounds__(128) k_range_wide(const WidenEntry* __restrict
 #pragma unroll
     for (int j = 0; j < L; j++) N.w[j] = (j == 0) ? e.n0 : (j == 1) ? e.n1 : (j == 2) ? e.n2 : 0u;
     v = N;
-    inc_l<L>(v);
+    if (NEG) dec_l<L>(v); else inc_l<L>(v);  // v = n + 1, or u = n - 1 for T'
     E = N;
     u32 it = 0;
     for (;;) {
@@ -729,10 +793,10 @@ __global__ void __launch_bounds__(128) k_range_wide(const WidenEntry* __restrict
       for (u32 j = 0; j < a; j++) m *= 3u;
       odd_run_l<L>(v, a, m);
       st += a;
-      Limbs<L> x = v;
-      dec_l<L>(x);
+      Limbs<L> x = v;  // the value: v - 1, or u + 1 for T'
+      if (NEG) inc_l<L>(x); else dec_l<L>(x);
       if (limbs_lt<L>(E, x)) E = x;
-      // even run on x = v - 1
+      // even run on the value x
       const u32 b = ctz32(x.w[0] | 0x80000000u);
       Limbs<L> w = x;
       shr_l<L>(w, b);
@@ -748,8 +812,12 @@ __global__ void __launch_bounds__(128) k_range_wide(const WidenEntry* __restrict
         break;
       }
       st += b;
+      if (NEG && !limbs_lt<L>(w, N) && !limbs_lt<L>(N, w)) {  // back at the seed: a cycle
+        atomicAdd(&recs[e.req].failures, 1ull);
+        break;
+      }
       v = w;
-      inc_l<L>(v);
+      if (NEG) dec_l<L>(v); else inc_l<L>(v);
     }
   }
   u32 pm = __ballot_sync(FULL, ok);
@@ -781,9 +849,13 @@ cudaError_t launch_range_stats(const RangeArgs& a, u32 grid, cudaStream_t st) {
 
 cudaError_t launch_range(const RangeArgs& a, int variant, u32 grid, cudaStream_t st) {
   switch (variant) {
-#define X(id, rm, mb) \
-  case id:            \
-    k_range<rm, mb><<<grid, RWARPS * 32, RANGE_SMEM, st>>>(a); break;
+#define X(id, rm, mb)                                                                 \
+  case id:                                                                            \
+    if (a.negative)                                                                   \
+      k_range<rm, mb, false, true><<<grid, RWARPS * 32, RANGE_SMEM, st>>>(a);         \
+    else                                                                              \
+      k_range<rm, mb><<<grid, RWARPS * 32, RANGE_SMEM, st>>>(a);                      \
+    break;
     CZ_RANGE_VARIANTS(X)
 #undef X
     default: return cudaErrorInvalidValue;
@@ -805,9 +877,12 @@ cudaError_t range_occupancy(int variant, int* bps) {
 // Opts every range kernel into RANGE_SMEM (> 48 KB) of dynamic shared memory.
 cudaError_t range_init() {
   cudaError_t e = cudaSuccess;
-#define X(id, rm, mb)                                                                                      \
-  if (e == cudaSuccess)                                                                                    \
-    e = cudaFuncSetAttribute(k_range<rm, mb>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RANGE_SMEM);
+#define X(id, rm, mb)                                                                                          \
+  if (e == cudaSuccess)                                                                                        \
+    e = cudaFuncSetAttribute(k_range<rm, mb>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RANGE_SMEM);    \
+  if (e == cudaSuccess)                                                                                        \
+    e = cudaFuncSetAttribute(k_range<rm, mb, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,         \
+                             (int)RANGE_SMEM);
   CZ_RANGE_VARIANTS(X)
 #undef X
   if (e == cudaSuccess)
@@ -816,12 +891,20 @@ cudaError_t range_init() {
 }
 
 cudaError_t launch_range_wide(const WidenEntry* list, const u32* count, u32 cap, int limbs, ReqRec* recs,
-                              WidenEntry* next, u32 next_cap, u32* next_count, u32 iter_cap, cudaStream_t st) {
+                              WidenEntry* next, u32 next_cap, u32* next_count, u32 iter_cap, cudaStream_t st,
+                              bool negative) {
   const u32 grid = (cap + 127) / 128;
-  if (limbs == 6)
-    k_range_wide<6><<<grid, 128, 0, st>>>(list, count, cap, recs, next, next_cap, next_count, iter_cap);
-  else
-    k_range_wide<8><<<grid, 128, 0, st>>>(list, count, cap, recs, nullptr, 0, nullptr, iter_cap);
+  if (limbs == 6) {
+    if (negative)
+      k_range_wide<6, true><<<grid, 128, 0, st>>>(list, count, cap, recs, next, next_cap, next_count, iter_cap);
+    else
+      k_range_wide<6, false><<<grid, 128, 0, st>>>(list, count, cap, recs, next, next_cap, next_count, iter_cap);
+  } else {
+    if (negative)
+      k_range_wide<8, true><<<grid, 128, 0, st>>>(list, count, cap, recs, nullptr, 0, nullptr, iter_cap);
+    else
+      k_range_wide<8, false><<<grid, 128, 0, st>>>(list, count, cap, recs, nullptr, 0, nullptr, iter_cap);
+  }
   return cudaGetLastError();
 }
 

@@ -93,7 +93,7 @@ struct collatz_ctx {
 
 namespace cz {
 int set_cuda_error(collatz_ctx* c, cudaError_t e, const char* where);
-int get_range_tables(collatz_ctx* c, uint32_t k, RangeTables** out);
+int get_range_tables(collatz_ctx* c, uint32_t k, RangeTables** out, bool negative = false);
 int lower_range(collatz_ctx* c, const collatz_range& r, uint32_t req, const RangeTables& T,
                 std::vector<RangeSeg>& segs, unsigned long long& items);
 void rec_to_range_result(const ReqRec& r, collatz_range_result* out);

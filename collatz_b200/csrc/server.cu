@@ -74,6 +74,7 @@ struct Req {
   double submit_s = 0, admit_s = 0, done_s = 0;
   // range requests
   uint32_t k = 0, slot = 0;
+  bool neg = false;            // the negative-integer variant
   std::vector<RangeSeg> segs;  // lowered work list, item_begin relative to the request
   unsigned long long items = 0, cursor = 0;
   size_t seg_i = 0;            // segment holding the cursor
@@ -256,8 +257,9 @@ void admit_ranges(collatz_server* s) {
     }
     pop_admitted(s, s->pend_range, r);
     r->k = r->q.range.k ? r->q.range.k : c->cfg.range_k;
+    r->neg = (r->q.range.flags & COLLATZ_RANGE_NEGATIVE) != 0;
     RangeTables* T = nullptr;
-    int rc = get_range_tables(c, r->k, &T);
+    int rc = get_range_tables(c, r->k, &T, r->neg);
     if (!rc) rc = lower_range(c, r->q.range, 0, *T, r->segs, r->items);
     if (rc || r->items == 0) {  // an error, or no seed in the range
       s->active--;
@@ -302,18 +304,20 @@ void take_items(Req* r, unsigned long long quota, std::vector<RangeSeg>& out, un
 // Builds and enqueues one range slice.  Returns 1 if one was launched, 0 if
 // there is no range work, negative on error.
 int launch_slice(collatz_server* s, int si) {
-  // the sieve exponent of the oldest request with work left
+  // the sieve (exponent k, sign) of the oldest request with work left
   uint32_t k = 0;
+  bool neg = false;
   uint64_t oldest = ~0ull;
   for (Req* r : s->ranges)
     if (r->cursor < r->items && r->ticket < oldest) {
       oldest = r->ticket;
       k = r->k;
+      neg = r->neg;
     }
   if (!k) return 0;
   std::vector<std::pair<unsigned long long, Req*>> want;
   for (Req* r : s->ranges)
-    if (r->cursor < r->items && r->k == k) want.push_back({r->items - r->cursor, r});
+    if (r->cursor < r->items && r->k == k && r->neg == neg) want.push_back({r->items - r->cursor, r});
   std::sort(want.begin(), want.end(),
             [](const std::pair<unsigned long long, Req*>& a, const std::pair<unsigned long long, Req*>& b) {
               return a.first != b.first ? a.first < b.first : a.second->ticket < b.second->ticket;
@@ -331,7 +335,7 @@ int launch_slice(collatz_server* s, int si) {
   }
   collatz_ctx* c = s->ctx;
   RangeTables* T = nullptr;
-  int rc = get_range_tables(c, k, &T);
+  int rc = get_range_tables(c, k, &T, neg);
   if (rc) return rc;
   const size_t sb = sizeof(RangeSeg) * segs.size();
   const size_t rb = sizeof(ReqRec) * s->cfg.max_active;
@@ -353,6 +357,7 @@ int launch_slice(collatz_server* s, int si) {
   a.widen_count = S.d_wcount.as<uint32_t>();
   a.iter_cap = c->iter_cap;
   a.stats = nullptr;
+  a.negative = neg ? 1u : 0u;
   cudaStream_t st = s->sa;
   e = cudaMemcpyAsync(S.d_segs.p, S.h_segs.p, sb, cudaMemcpyHostToDevice, st);
   if (!e) e = cudaMemsetAsync(S.d_cursor.p, 0, sizeof(unsigned long long), st);
@@ -361,10 +366,11 @@ int launch_slice(collatz_server* s, int si) {
   if (!e) e = launch_range(a, c->range_variant, s->grid, st);
   if (!e)
     e = launch_range_wide(S.d_widen[0].as<WidenEntry>(), S.d_wcount.as<uint32_t>(), WIDEN_CAP, 6, a.recs,
-                          S.d_widen[1].as<WidenEntry>(), WIDEN_CAP, S.d_wcount.as<uint32_t>() + 1, c->iter_cap, st);
+                          S.d_widen[1].as<WidenEntry>(), WIDEN_CAP, S.d_wcount.as<uint32_t>() + 1, c->iter_cap, st,
+                          neg);
   if (!e)
     e = launch_range_wide(S.d_widen[1].as<WidenEntry>(), S.d_wcount.as<uint32_t>() + 1, WIDEN_CAP, 8, a.recs,
-                          nullptr, 0, nullptr, c->iter_cap, st);
+                          nullptr, 0, nullptr, c->iter_cap, st, neg);
   if (!e && !S.finishing.empty()) e = cudaMemcpyAsync(S.h_recs.p, s->d_recs.p, rb, cudaMemcpyDeviceToHost, st);
   if (!e) e = cudaEventRecord(S.done, st);
   if (e) return set_cuda_error(c, e, "server slice launch");

@@ -124,7 +124,7 @@ __device__ __forceinline__ bool pow3_gt_pow2(u32 f, u32 j, u64 p3) {
 }
 
 // Pass A: the sieve bit array.  One thread per residue, one ballot per word.
-__global__ void k_range_bits(u32* __restrict__ bits, u32 k, u64 nres) {
+__global__ void k_range_bits(u32* __restrict__ bits, u32 k, u64 nres, u32 up) {
   const u64 r = (u64)blockIdx.x * blockDim.x + threadIdx.x;
   bool ok = false;
   if (r < nres) {
@@ -133,7 +133,7 @@ __global__ void k_range_bits(u32* __restrict__ bits, u32 k, u64 nres) {
     ok = true;
     for (u32 j = 1; j <= k; j++) {
       if (n & 1) {
-        n = n + (n >> 1) + 1;
+        n = n + (n >> 1) + up;  // (3n+1)/2, or (3n-1)/2 for the negative variant (up = 0)
         f++;
         p3 *= 3;
       } else {
@@ -203,7 +203,7 @@ __global__ void k_scan_counts(const u32* __restrict__ counts, ull* __restrict__ 
 // set bits with popc + scan and the owning lanes write entries in residue
 // order with their k-step jump.
 __global__ void k_range_compact(const u32* __restrict__ bits, const ull* __restrict__ offs,
-                                RangeEntry* __restrict__ table, u32 k, u64 nwords, u32 nchunks) {
+                                RangeEntry* __restrict__ table, u32 k, u64 nwords, u32 nchunks, u32 up) {
   const u32 warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const u32 lane = lane_id();
   if (warp >= nchunks) return;
@@ -224,7 +224,7 @@ __global__ void k_range_compact(const u32* __restrict__ bits, const ull* __restr
       u32 f = 0, emax = 0;
       for (u32 j = 1; j <= k; j++) {
         if (n & 1) {
-          n = n + (n >> 1) + 1;
+          n = n + (n >> 1) + up;
           f++;
           p3 *= 3;
         } else {
@@ -237,7 +237,7 @@ __global__ void k_range_compact(const u32* __restrict__ bits, const ull* __restr
       RangeEntry e;
       e.r_lo = (u32)r;
       e.meta = (u32)(r >> 32) | (f << 8) | ((u32)(r % 9) << 16) | (emax << 24);
-      const u64 c = n + 1;  // T^k(r) + 1
+      const u64 c = up ? n + 1 : n - 1;  // T^k(r) + 1, or T'^k(r) - 1 (>= 0: survivors have r >= 1)
       e.c_lo = (u32)c;
       e.c_hi = (u32)(c >> 32);
       table[out++] = e;
@@ -249,7 +249,7 @@ __global__ void k_range_compact(const u32* __restrict__ bits, const ull* __restr
 // For every removed residue r: with tau the first j where 3^{f_j} < 2^j,
 // T^tau(2^k + r) < 2^k + r must hold.  Since T^tau is affine with slope
 // 3^f / 2^tau < 1 on the class, this proves the sieve for all n >= 2^k.
-__global__ void k_range_validate(const u32* __restrict__ bits, u32 k, u64 nres, ull* __restrict__ bad) {
+__global__ void k_range_validate(const u32* __restrict__ bits, u32 k, u64 nres, ull* __restrict__ bad, u32 up) {
   const u64 r = (u64)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= nres) return;
   if ((bits[r >> 5] >> (r & 31)) & 1u) return;
@@ -257,7 +257,7 @@ __global__ void k_range_validate(const u32* __restrict__ bits, u32 k, u64 nres, 
   u32 f = 0, tau = 0;
   for (u32 j = 1; j <= k; j++) {
     if (n & 1) {
-      n = n + (n >> 1) + 1;
+      n = n + (n >> 1) + up;
       f++;
       p3 *= 3;
     } else {
@@ -271,7 +271,7 @@ __global__ void k_range_validate(const u32* __restrict__ bits, u32 k, u64 nres, 
   // x = 2^k + r in two limbs (k <= 40 keeps x < 2^41; values stay < 2^64 for tau <= k)
   const u64 s = (1ull << k) + r;
   u64 x = s;
-  for (u32 j = 0; j < tau; j++) x = (x & 1) ? x + (x >> 1) + 1 : x >> 1;
+  for (u32 j = 0; j < tau; j++) x = (x & 1) ? x + (x >> 1) + up : x >> 1;
   if (tau == 0 || !(x < s)) atomicAdd(bad, 1ull);
 }
 
@@ -363,7 +363,7 @@ __global__ void k_class_scatter(const RangeEntry* __restrict__ t, u64 n, const u
   }
 }
 
-cudaError_t build_range_table(RangeTable* t, u32 k, bool validate, cudaStream_t st) {
+cudaError_t build_range_table(RangeTable* t, u32 k, bool validate, cudaStream_t st, bool negative) {
   t->k = k;
   const u64 nres = 1ull << k;
   const u64 nwords = (nres + 31) / 32;
@@ -377,7 +377,9 @@ cudaError_t build_range_table(RangeTable* t, u32 k, bool validate, cudaStream_t 
   if ((e = cudaMalloc(&counts, sizeof(u32) * nchunks))) return e;
   if ((e = cudaMalloc(&offs, sizeof(ull) * (nchunks + 1)))) return e;
   const u32 tpb = 256;
-  k_range_bits<<<(u32)((nres + tpb - 1) / tpb), tpb, 0, st>>>(t->bits, k, nres);
+  const u32 up = negative ? 0u : 1u;
+  t->negative = negative;
+  k_range_bits<<<(u32)((nres + tpb - 1) / tpb), tpb, 0, st>>>(t->bits, k, nres, up);
   k_range_count<<<(nchunks + 127) / 128, 128, 0, st>>>((const uint4*)t->bits, counts, nwords_pad / 4, nchunks);
   k_scan_counts<<<1, 1024, 0, st>>>(counts, offs, nchunks);
   ull total = 0;
@@ -385,13 +387,13 @@ cudaError_t build_range_table(RangeTable* t, u32 k, bool validate, cudaStream_t 
   if ((e = cudaStreamSynchronize(st))) return e;
   t->count = total;
   if ((e = cudaMalloc(&t->table, sizeof(RangeEntry) * (total ? total : 1)))) return e;
-  k_range_compact<<<(nchunks * 32 + 255) / 256, 256, 0, st>>>(t->bits, offs, t->table, k, nwords, nchunks);
+  k_range_compact<<<(nchunks * 32 + 255) / 256, 256, 0, st>>>(t->bits, offs, t->table, k, nwords, nchunks, up);
   t->violations = 0;
   if (validate) {
     ull* bad = nullptr;
     if ((e = cudaMalloc(&bad, sizeof(ull)))) return e;
     cudaMemsetAsync(bad, 0, sizeof(ull), st);
-    k_range_validate<<<(u32)((nres + tpb - 1) / tpb), tpb, 0, st>>>(t->bits, k, nres, bad);
+    k_range_validate<<<(u32)((nres + tpb - 1) / tpb), tpb, 0, st>>>(t->bits, k, nres, bad, up);
     cudaMemcpyAsync(&t->violations, bad, sizeof(ull), cudaMemcpyDeviceToHost, st);
     cudaStreamSynchronize(st);
     cudaFree(bad);

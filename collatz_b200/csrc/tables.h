@@ -42,11 +42,14 @@ struct RangeTable {
   unsigned long long count = 0;     // number of survivors
   unsigned long long cls[10] = {};  // class c = table[cls[c], cls[c+1])
   unsigned long long violations = 0;// sieve validation failures (must be 0)
+  bool negative = false;            // built for the negative-integer variant
 };
 
 cudaError_t build_case_tables(CaseTables* t, uint32_t maxbits, cudaStream_t st);
 void free_case_tables(CaseTables* t);
-cudaError_t build_range_table(RangeTable* t, uint32_t k, bool validate, cudaStream_t st);
+// negative: the sieve and jumps of the negative-integer variant T'(m) = (3m-1)/2, m/2 (the
+// entries then hold c = T'^k(r) - 1, so that T'^k(n) - 1 = q 3^f + c).
+cudaError_t build_range_table(RangeTable* t, uint32_t k, bool validate, cudaStream_t st, bool negative = false);
 void free_range_table(RangeTable* t);
 
 }  // namespace cz

@@ -190,9 +190,18 @@ typedef struct {
   uint64_t offset[2];
   uint64_t size;
   uint32_t k;      /* 0 = the context's range_k */
-  uint32_t flags;  /* COLLATZ_RANGE_NO_MOD9 */
+  uint32_t flags;  /* COLLATZ_RANGE_NO_MOD9, COLLATZ_RANGE_NEGATIVE */
 } collatz_range;
 #define COLLATZ_RANGE_NO_MOD9 0x1u
+/* Negative integers (no counterpart in the reference): seed m stands for -m,
+ * and the map is T'(m) = (3m-1)/2 for odd m, m/2 for even m (T acting on
+ * -m).  The residue sieve uses T's parity steps with the same descent
+ * test; the mod-9 sieve keeps m mod 9 in {0,2,3,6,8} (m = 1 mod 3 is T' of
+ * the smaller (2m+1)/3, m = 5 mod 9 is T'^3 of the smaller (8m+5)/9) and
+ * m = 5.  A seed that returns to itself never descends: the cycle minima 5
+ * and 17 are reported in failures (no error bit).  Requests of one batch
+ * or plan are all negative or all positive. */
+#define COLLATZ_RANGE_NEGATIVE 0x2u
 
 typedef struct {
   uint64_t seeds_checked;

@@ -378,12 +378,12 @@ int orc_run_case(const orc_tables *t, uint64_t base_lo, uint64_t base_hi,
 
 /* 1 iff residue r mod 2^k survives the k-step descent sieve:
  * 3^{f_j(r)} >= 2^j for every 1 <= j <= k (f_j = odd steps among the first j). */
-static int residue_survives(uint64_t r, uint32_t k) {
+static int residue_survives_v(uint64_t r, uint32_t k, int neg) {
   uint64_t n = r;
   unsigned f = 0;
   for (unsigned j = 1; j <= k; j++) {
     if (n & 1) {
-      n = n + (n >> 1) + 1;
+      n = n + (n >> 1) + (neg ? 0 : 1);  /* (3n+1)/2, or (3n-1)/2 for T' */
       f++;
     } else {
       n >>= 1;
@@ -392,6 +392,7 @@ static int residue_survives(uint64_t r, uint32_t k) {
   }
   return 1;
 }
+static int residue_survives(uint64_t r, uint32_t k) { return residue_survives_v(r, k, 0); }
 
 uint64_t orc_range_sieve(uint32_t k, uint8_t *bits) {
   uint64_t count = 0;
@@ -454,11 +455,12 @@ static void big_shr1(big *x) {
   for (int i = 0; i < 7; i++) x->w[i] = (x->w[i] >> 1) | (x->w[i + 1] << 63);
   x->w[7] >>= 1;
 }
-/* x <- (3x+1)/2 = x + (x>>1) + 1 for odd x; returns 1 on overflow */
-static int big_odd_step(big *x) {
+/* x <- (3x+1)/2 = x + (x>>1) + 1 for odd x (cin = 1), or the negative
+ * variant's (3x-1)/2 = x + (x>>1) (cin = 0); returns 1 on overflow */
+static int big_odd_step_c(big *x, unsigned cin) {
   big h = *x;
   big_shr1(&h);
-  unsigned __int128 c = 1;
+  unsigned __int128 c = cin;
   for (int i = 0; i < 8; i++) {
     c += (unsigned __int128)x->w[i] + h.w[i];
     x->w[i] = (uint64_t)c;
@@ -467,25 +469,35 @@ static int big_odd_step(big *x) {
   return c != 0;
 }
 
-/* sigma and E of one seed with single T-steps on 512-bit values.
- * Returns 0 ok, 2 overflow. */
-static int big_seed(const big *n, uint64_t *st_out, big *E_out, uint64_t *steps) {
+/* Steps after which a seed of the negative variant counts as not
+ * descending (the known non-descending seeds, the cycle minima 5 and 17,
+ * are caught exactly by returning to themselves). */
+#define NEG_STEP_CAP (1u << 22)
+
+/* sigma and E of one seed with single steps on 512-bit values (T, or T'
+ * when neg).  Returns 0 ok, 2 overflow, 3 (neg) returned to the seed or
+ * reached the step cap: the seed does not descend. */
+static int big_seed_v(const big *n, uint64_t *st_out, big *E_out, uint64_t *steps, int neg) {
   big x = *n, E = *n;
   uint64_t st = 0;
   for (;;) {
     if (x.w[0] & 1) {
-      if (big_odd_step(&x)) return 2;
+      if (big_odd_step_c(&x, neg ? 0u : 1u)) return 2;
       if (big_cmp(&x, &E) > 0) E = x;
     } else {
       big_shr1(&x);
     }
     st++;
     if (big_cmp(&x, n) < 0) break;
+    if (neg && (big_cmp(&x, n) == 0 || st >= NEG_STEP_CAP)) return 3;
   }
   *st_out = st;
   *E_out = E;
   if (steps) *steps += st;
   return 0;
+}
+static int big_seed(const big *n, uint64_t *st_out, big *E_out, uint64_t *steps) {
+  return big_seed_v(n, st_out, E_out, steps, 0);
 }
 
 typedef struct {
@@ -687,10 +699,115 @@ wide : {
 }
 }
 
+/* ---- negative variant: m stands for -m, T'(m) = (3m-1)/2 (odd m), m/2
+ * (even m), which is T acting on -m.  sigma and E as for T.  A seed that
+ * returns to itself lies on a cycle and never descends (in range: the cycle
+ * minima 5 and 17); it counts as a failure, as does one that reaches the
+ * step cap or leaves 512 bits. */
+
+static void neg_wide(range_acc *a, u128 n) {
+  big nb, Eb;
+  big_from_u128(&nb, n);
+  uint64_t st2;
+  if (big_seed_v(&nb, &st2, &Eb, &a->steps, 1)) {
+    a->failures++;
+    return;
+  }
+  acc_seed(a, n, st2, &Eb);
+}
+
+/* method 0: single T'-steps in u128 */
+static void seed_steps_neg(range_acc *a, u128 n) {
+  u128 x = n, E = n;
+  uint64_t st = 0;
+  for (;;) {
+    if (x & 1) {
+      if (x > U128_MAX - (x >> 1)) {
+        neg_wide(a, n);
+        return;
+      }
+      x = x + (x >> 1);
+      if (x > E) E = x;
+    } else {
+      x >>= 1;
+    }
+    st++;
+    if (x < n) break;
+    if (x == n || st >= NEG_STEP_CAP) {
+      a->failures++;
+      return;
+    }
+  }
+  big Eb;
+  big_from_u128(&Eb, E);
+  a->steps += st;
+  acc_seed(a, n, st, &Eb);
+}
+
+/* the run-length loop in the "-1" space, u = T'^k(m) - 1: odd run
+ * a = ctz(u | 2^8), u = 3^a (u >> a); even run b = ctz((u+1) | 2^31),
+ * u = ((u+1) >> b) - 1.  Descent happens inside an even run; a return to
+ * the seed happens at the end of one.  Starts from u after s steps. */
+static void runs_neg(range_acc *a, u128 n, u128 u, uint64_t st, u128 E) {
+  for (;;) {
+    unsigned oa = ctz32((uint32_t)u | (1u << 8));
+    u128 q = u >> oa;
+    if (q > U128_MAX / P3[oa] || q * P3[oa] == U128_MAX) {
+      neg_wide(a, n);
+      return;
+    }
+    u = q * P3[oa];
+    st += oa;
+    a->odd_runs++;
+    if (u + 1 > E) E = u + 1;
+    u128 t = u + 1;
+    unsigned b = ctz32((uint32_t)t | 0x80000000u);
+    a->even_runs++;
+    if ((t >> b) < n) {
+      unsigned i = 1;
+      while ((t >> i) >= n) i++;
+      st += i;
+      break;
+    }
+    st += b;
+    if ((t >> b) == n || st >= NEG_STEP_CAP) {
+      a->failures++;
+      return;
+    }
+    u = (t >> b) - 1;
+  }
+  big Eb;
+  big_from_u128(&Eb, E);
+  a->steps += st;
+  acc_seed(a, n, st, &Eb);
+}
+
+/* method 1 */
+static void seed_runs_neg(range_acc *a, u128 n) { runs_neg(a, n, n - 1, 0, n); }
+
+/* method 2: the first k steps as single steps (no descent for a survivor),
+ * then the run-length loop */
+static void seed_jump_runs_neg(range_acc *a, u128 n, uint32_t k) {
+  u128 x = n, E = n;
+  for (uint32_t j = 0; j < k; j++) {
+    if (x & 1) {
+      if (x > U128_MAX - (x >> 1)) {
+        neg_wide(a, n);
+        return;
+      }
+      x = x + (x >> 1);
+      if (x > E) E = x;
+    } else {
+      x >>= 1;
+    }
+  }
+  runs_neg(a, n, x - 1, k, E);
+}
+
 typedef struct {
   u128 lo, hi; /* [lo, hi) */
   uint32_t k;
-  int use_mod9, method;
+  int use_mod9, method, neg;
   const uint8_t *bits;
   range_acc acc;
 } range_job;
@@ -703,19 +820,30 @@ static void *range_worker(void *p) {
     if (n < 2) continue;
     if (j->use_mod9) {
       unsigned r9 = (unsigned)(n % 9);
-      if (!((0xCBu >> r9) & 1)) continue; /* keep {0,1,3,6,7} */
+      /* T: keep {0,1,3,6,7} (cu:488).  T': m = 1 mod 3 (m > 1) is T' of the
+       * smaller odd (2m+1)/3, and m = 5 mod 9 (m > 5) is T'^3 of the smaller
+       * x = (8m+5)/9 (x = 5 mod 8: odd, odd, even steps); keep {0,2,3,6,8}. */
+      if (j->neg ? !(((0x14Du >> r9) & 1) || n == 5) : !((0xCBu >> r9) & 1)) continue;
     }
     if (j->k && n >= K) {
       uint64_t r = (uint64_t)n & mask;
-      if (j->bits ? !((j->bits[r >> 3] >> (r & 7)) & 1) : !residue_survives(r, j->k)) continue;
+      if (j->bits ? !((j->bits[r >> 3] >> (r & 7)) & 1) : !residue_survives_v(r, j->k, j->neg)) continue;
     }
     j->acc.seeds++;
-    if (j->method == 0)
+    if (j->neg) {
+      if (j->method == 0)
+        seed_steps_neg(&j->acc, n);
+      else if (j->method == 2 && j->k && n >= K)
+        seed_jump_runs_neg(&j->acc, n, j->k);
+      else
+        seed_runs_neg(&j->acc, n);
+    } else if (j->method == 0) {
       seed_steps(&j->acc, n);
-    else if (j->method == 2 && j->k && n >= K)
+    } else if (j->method == 2 && j->k && n >= K) {
       seed_jump_runs(&j->acc, n, j->k);
-    else
+    } else {
       seed_runs(&j->acc, n);
+    }
   }
   return NULL;
 }
@@ -725,14 +853,17 @@ int orc_range(uint64_t offset_lo, uint64_t offset_hi, uint64_t size,
               orc_range_result *out) {
   /* the table costs 2^k residue tests, the direct test k steps per seed */
   const int direct = k > 26 || (u128)size * k < ((u128)1 << k);
-  return orc_range_ex(offset_lo, offset_hi, size, k, use_mod9, method, nthreads, direct, out);
+  return orc_range_ex(offset_lo, offset_hi, size, k, use_mod9, method, nthreads,
+                      direct ? ORC_RANGE_DIRECT_SIEVE : 0, out);
 }
 
 int orc_range_ex(uint64_t offset_lo, uint64_t offset_hi, uint64_t size,
                  uint32_t k, int use_mod9, int method, int nthreads,
-                 int direct_sieve, orc_range_result *out) {
+                 int flags, orc_range_result *out) {
   u128 offset = U128_OF(offset_lo, offset_hi);
   if (k > 34 || nthreads < 1) return -1;
+  const int neg = (flags & ORC_RANGE_NEGATIVE) != 0;
+  const int direct_sieve = neg || (flags & ORC_RANGE_DIRECT_SIEVE);
   memset(out, 0, sizeof *out);
   uint8_t *bits = NULL;
   if (k && !direct_sieve) {
@@ -752,6 +883,7 @@ int orc_range_ex(uint64_t offset_lo, uint64_t offset_hi, uint64_t size,
     jobs[i].k = k;
     jobs[i].use_mod9 = use_mod9;
     jobs[i].method = method;
+    jobs[i].neg = neg;
     jobs[i].bits = bits;
   }
   for (int i = 1; i < nthreads; i++) pthread_create(&th[i], NULL, range_worker, &jobs[i]);

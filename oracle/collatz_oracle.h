@@ -138,13 +138,22 @@ uint64_t orc_range_sieve_validate(uint32_t k);
 int orc_range(uint64_t offset_lo, uint64_t offset_hi, uint64_t size,
               uint32_t k, int use_mod9, int method, int nthreads,
               orc_range_result *out);
-/* As orc_range with the sieve applied either from the 2^k-bit table
- * (direct_sieve = 0) or by testing each seed's residue against the sieve's
- * definition (direct_sieve = 1; used for k > 26 and for ranges much smaller
- * than 2^k, where building the table would dominate).  Same results. */
+/* As orc_range, with flags:
+ *   ORC_RANGE_DIRECT_SIEVE -- test each seed's residue against the sieve's
+ *     definition instead of building the 2^k-bit table (what orc_range does
+ *     for k > 26 and for ranges much smaller than 2^k).  Same results.
+ *   ORC_RANGE_NEGATIVE -- the negative-integer variant: seed m stands for
+ *     -m and the map is T'(m) = (3m-1)/2 for odd m, m/2 for even m (T on
+ *     -m).  The k-step sieve uses T's parity steps with the same descent
+ *     test; the mod-9 sieve keeps m mod 9 in {0,2,3,6,8} (and m = 5), the
+ *     analogue of {0,1,3,6,7} for T.  A seed that returns to itself (the
+ *     cycle minima 5 and 17) or runs 2^22 steps without descending counts
+ *     as a failure and enters neither maximum. */
+#define ORC_RANGE_DIRECT_SIEVE 0x1
+#define ORC_RANGE_NEGATIVE 0x2
 int orc_range_ex(uint64_t offset_lo, uint64_t offset_hi, uint64_t size,
                  uint32_t k, int use_mod9, int method, int nthreads,
-                 int direct_sieve, orc_range_result *out);
+                 int flags, orc_range_result *out);
 
 /* ---------------- trajectory queries ---------------- */
 /* seeds: nseeds x seed_limbs little-endian u32 limbs (seed_limbs <= 8).

@@ -27,7 +27,9 @@ def build(force: bool = False) -> str:
         mt = os.path.getmtime(LIB)
         if mt >= os.path.getmtime(SRC) and mt >= os.path.getmtime(hdr):
             return LIB
-    tmp = LIB + ".tmp"
+    # a private temporary per process: concurrent builders (e.g. two ranks of
+    # a multi-process test) each rename a complete library into place
+    tmp = f"{LIB}.tmp{os.getpid()}"
     subprocess.check_call(["gcc", "-std=gnu11", "-O2", "-fPIC", "-shared", "-pthread",
                            "-Wall", "-o", tmp, SRC])
     os.replace(tmp, LIB)
@@ -282,15 +284,18 @@ class RangeResult:
 
 
 def range_verify(offset: int, size: int, k: int, use_mod9: bool = True, method: int = 1,
-                 nthreads: int = 1, direct_sieve: bool | None = None) -> RangeResult:
-    """orc_range; direct_sieve None = the oracle's choice (table for small k)."""
+                 nthreads: int = 1, direct_sieve: bool | None = None,
+                 negative: bool = False) -> RangeResult:
+    """orc_range; direct_sieve None = the oracle's choice (table for small k);
+    negative: the negative-integer variant T'(m) = (3m-1)/2, m/2."""
     r = _RangeResult()
-    if direct_sieve is None:
+    if direct_sieve is None and not negative:
         rc = lib().orc_range(*_split(offset), size, k, 1 if use_mod9 else 0, method, nthreads,
                              C.byref(r))
     else:
+        flags = (1 if direct_sieve else 0) | (2 if negative else 0)
         rc = lib().orc_range_ex(*_split(offset), size, k, 1 if use_mod9 else 0, method, nthreads,
-                                1 if direct_sieve else 0, C.byref(r))
+                                flags, C.byref(r))
     if rc:
         raise ValueError(f"orc_range rc={rc}")
     return RangeResult(r.seeds, r.failures, _limbs(r.max_exc), _limbs(r.max_exc_seed),

@@ -96,6 +96,43 @@ def test_batch_of_tiny_requests(verifier):
         _cmp(g, o)
 
 
+NEG_CASES = [
+    (2, 1 << 20, 16, True),                     # dense part and sieved part; the cycle minima 5, 17
+    ((1 << 40) + 12345, 1 << 21, 24, True),     # unaligned
+    (1 << 40, 1 << 22, 20, False),              # no mod-9 sieve
+    ((1 << 62) - 999, 1 << 20, 24, True),
+    ((1 << 60) + (3 << 34) - 5000, 300000, 34, True),  # frontier sieve, crosses a block
+]
+
+
+@pytest.mark.parametrize("case", NEG_CASES, ids=lambda c: f"neg-o{c[0]:x}-s{c[1]}-k{c[2]}-m{int(c[3])}")
+def test_negative_range_matches_oracle(verifier, case):
+    """The negative-integer variant T'(m) = (3m-1)/2, m/2 against the oracle's
+    run-length formulation; the cycle minima count as failures."""
+    from oracle import oracle as O
+    off, size, k, mod9 = case
+    g = verifier(26).verify_range(off, size, k, mod9, negative=True)
+    o = O.range_verify(off, size, k, mod9, method=1, nthreads=NT, negative=True)
+    assert g.errors == 0
+    assert (g.seeds_checked, g.failures) == (o.seeds, o.failures)
+    assert (g.max_stopping_time, g.max_stopping_time_seed) == (o.max_st, o.max_st_seed)
+    assert (g.max_excursion, g.max_excursion_seed) == (o.max_exc, o.max_exc_seed)
+    if off <= 5 and off + size > 17:
+        assert g.failures == 2
+
+
+def test_negative_batch_and_mixed_plan_rules(verifier):
+    import collatz_b200 as cb
+    v = verifier(26)
+    reqs = [((1 << 44) + 7 * i, 5000 + 100 * i, 24, True, True) for i in range(8)]
+    got = v.verify_batch(reqs)
+    for q, g in zip(reqs, got):
+        alone = v.verify_range(*q[:4], negative=True)
+        assert _key(g) == _key(alone)
+    with pytest.raises(cb.CollatzError):  # one sieve (k, sign) per launch
+        v.verify_batch([(1 << 44, 1000, 24, True, True), (1 << 44, 1000, 24, True, False)])
+
+
 def test_batch_equals_alone(verifier):
     """Each request's result is the same alone and in a mixed batch."""
     v = verifier(26)

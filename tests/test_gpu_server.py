@@ -27,6 +27,8 @@ def _mix(rng, n_range, n_traj):
         n = rng.choice([1, 3, 100, 1000])
         reqs.append(("traj", [rng.getrandbits(rng.randint(64, 256)) | 1 for _ in range(n)]))
     reqs.append(("range", (5, 1 << 16, 24)))        # starts below 2^k (unsieved part)
+    reqs.append(("range", (2, 1 << 14, 16, True, True)))          # negative integers (cycle minima)
+    reqs.append(("range", ((1 << 45) + 3, 1 << 18, 24, True, True)))
     reqs.append(("range", (1 << 40, 0, 24)))        # empty
     reqs.append(("traj", [0, 1, 2, 27, (1 << 256) - 1]))
     rng.shuffle(reqs)
@@ -34,13 +36,15 @@ def _mix(rng, n_range, n_traj):
 
 
 def _submit(srv, kind, arg):
-    return srv.submit_range(*arg) if kind == "range" else srv.submit_trajectory(arg)
+    if kind != "range":
+        return srv.submit_trajectory(arg)
+    return srv.submit_range(*arg[:4], negative=len(arg) > 4 and arg[4])
 
 
 def _check(verifier, kind, arg, resp):
     assert resp.status == 0, resp
     if kind == "range":
-        alone = verifier.verify_range(*arg)
+        alone = verifier.verify_range(*arg[:4], negative=len(arg) > 4 and arg[4])
         assert _range_key(resp.range) == _range_key(alone), (arg, resp.range, alone)
     else:
         assert resp.trajectory() == verifier.trajectory(arg)

@@ -187,6 +187,80 @@ def test_range_k34_bruteforce():
     assert (o.max_exc, o.max_exc_seed) == (best_e[0], -best_e[1])
 
 
+def T_neg(m):
+    """T acting on -m, written for m: (3m-1)/2 for odd m, m/2 for even m."""
+    return (3 * m - 1) // 2 if m & 1 else m // 2
+
+
+def brute_neg(m, cap=10000):
+    """(stopping time, excursion), or None when m returns to itself or runs cap steps."""
+    x, E, k = m, m, 0
+    while True:
+        x = T_neg(x)
+        k += 1
+        E = max(E, x)
+        if x < m:
+            return k, E
+        if x == m or k >= cap:
+            return None
+
+
+def test_negative_merge_rules():
+    """The negative variant's mod-9 sieve drops m = 1 (mod 3), m > 1, and
+    m = 5 (mod 9), m > 5, because a smaller seed reaches them first."""
+    for m in range(2, 3000):
+        if m % 3 == 1:
+            p = (2 * m + 1) // 3
+            assert (2 * m + 1) % 3 == 0 and p % 2 == 1 and T_neg(p) == m and p < m
+        if m % 9 == 5 and m > 5:
+            x = (8 * m + 5) // 9
+            assert (8 * m + 5) % 9 == 0 and T_neg(T_neg(T_neg(x))) == m and x < m
+
+
+@pytest.mark.parametrize("case", [(2, 4000, 8, True), (2, 3000, 12, False), ((1 << 30) + 17, 3000, 12, True),
+                                  ((1 << 34) + 5, 2000, 16, True)])
+def test_range_negative_bruteforce(case):
+    from oracle import oracle as O
+    off, size, k, mod9 = case
+    o = O.range_verify(off, size, k, mod9, method=0, negative=True)
+    best_st, best_e, seeds, fails = (-1, 0), (-1, 0), 0, 0
+    for m in range(off, off + size):
+        if m < 2 or (mod9 and not (m % 9 in (0, 2, 3, 6, 8) or m == 5)):
+            continue
+        if m >= (1 << k):
+            x, f, ok = m % (1 << k), 0, True
+            for j in range(1, k + 1):
+                if x & 1:
+                    f += 1
+                x = T_neg(x)
+                if 3 ** f < 2 ** j:
+                    ok = False
+                    break
+            if not ok:
+                continue
+        seeds += 1
+        b = brute_neg(m)
+        if b is None:
+            fails += 1
+            continue
+        best_st = max(best_st, (b[0], -m))
+        best_e = max(best_e, (b[1], -m))
+    assert (o.seeds, o.failures) == (seeds, fails)
+    assert (o.max_st, o.max_st_seed) == (best_st[0], -best_st[1])
+    assert (o.max_exc, o.max_exc_seed) == (best_e[0], -best_e[1])
+    if off <= 17 < off + size:
+        assert fails == 2  # the cycle minima 5 and 17
+
+
+@pytest.mark.parametrize("case", [(2, 1 << 18, 16), ((1 << 40) + 3, 1 << 18, 20), ((1 << 62) - 999, 1 << 16, 24)])
+def test_range_negative_methods_agree(case):
+    from oracle import oracle as O
+    off, size, k = case
+    rs = [O.range_verify(off, size, k, True, method=m, nthreads=4, negative=True) for m in (0, 1, 2)]
+    keys = [(r.seeds, r.failures, r.max_st, r.max_st_seed, r.max_exc, r.max_exc_seed) for r in rs]
+    assert keys[0] == keys[1] == keys[2]
+
+
 def test_trajectory_bruteforce():
     from oracle import oracle as O
     rng = random.Random(3)
