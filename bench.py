@@ -54,6 +54,9 @@ K_RANGE_DRAM_BYTES = 5.339648e6 + 0.219904e6
 # 5.406020352e9 and wrote 9.036032e6 bytes, so traffic per launch = blocks x
 # this figure.
 K_RANGE_FRONTIER_DRAM_BYTES_PER_BLOCK = (5.406020352e9 + 9.036032e6) / 4
+# Issue-slot utilisation of k_range measured with ncu (2^33 block, k = 24;
+# 2^36 frontier, k = 34).
+K_RANGE_ISSUE_NCU = {"block": 0.6921, "frontier": 0.7632}
 
 
 def dist_env():
@@ -507,7 +510,14 @@ def main():
                                   f"({OPS_JUMP} + {OPS_ODD} x {odd_per:.2f} odd runs + {OPS_EVEN} x "
                                   f"{even_per:.2f} even runs) x {res.seeds_checked} seeds per launch",
                          "peak_basis": f"issue peak {sm_count} SMs x 4 SMSP x 32 lanes x {sm_mhz:.0f} MHz "
-                                       "(sampled median SM clock); no integer peak in MEASURED_PEAKS.json"},
+                                       "(sampled median SM clock); no integer peak in MEASURED_PEAKS.json",
+                         # issue-slot utilisation of the same kernel, measured with ncu on a smaller
+                         # launch of this workload: achieved/peak counts only the algorithmic ops, this
+                         # counts every issued instruction (work distribution included)
+                         "issue_slots_busy_ncu": K_RANGE_ISSUE_NCU[args.workload],
+                         "issue_basis": "sm__inst_issued.avg.pct_of_peak_sustained_active of one k_range "
+                                        "launch (profiles/k_range_2p38_block.md, "
+                                        "profiles/k_range_frontier_2p36.md)"},
             # request (32 B) + its work list: an aligned range of many blocks lowers to 55
             # 64-byte segments (5 kept mod-9 classes of the first and last block, 9 x 5 for the
             # blocks between)

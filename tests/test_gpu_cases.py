@@ -94,6 +94,35 @@ def test_case_maxima_match_oracle(verifier, oracle_tables, n, tup):
     assert (r.max_excursion, r.max_excursion_seed) == (o.max_exc, o.max_exc_seed)
 
 
+@pytest.mark.parametrize("variant", range(4))
+def test_every_cases_variant_matches_reference(verifier, oracle_tables, variant):
+    """Each cases-kernel variant reproduces the reference's pair batches
+    (overflow reports included), search2 pairs, and the oracle's maxima."""
+    import collatz_b200 as cb
+    assert cb.lib().collatz_variant_count(0) == 4
+    v = verifier(45)
+    v.set_variant(0, variant)
+    try:
+        fx = load_golden("pairs_N45.json")
+        for b in fx["batches"]:
+            r = v.launchkernel(b["bigindex"], [(int(x), int(y)) for x, y in b["pairs"]])
+            assert f"{r.hash:X}" == b["hash"] and r.seeds_checked == b["seeds"], (variant, b["kind"])
+            assert sorted(r.overflow) == sorted(int(x) for x in b["overflow"])
+        for d in fx["search2"]:
+            r = v.launchkernel(d["bigindex"], [(int(d["base"]), int(d["number"]))])
+            assert f"{r.hash:X}" == d["hash"], (variant, d)
+        v36 = verifier(36)
+        v36.set_variant(0, variant)
+        r = v36.run_case(27, 10, 8, 183, 0, 0)
+        o = oracle_tables(36).run_case(27, 10, 8, 183, 0, 0)
+        assert (r.hash, r.seeds_checked) == (o.hash, o.seeds)
+        assert (r.max_stopping_time, r.max_stopping_time_seed) == (o.max_st, o.max_st_seed)
+        assert (r.max_excursion, r.max_excursion_seed) == (o.max_exc, o.max_exc_seed)
+    finally:
+        v.set_variant(0, 1)
+        verifier(36).set_variant(0, 1)
+
+
 def test_pair_maxima_match_oracle(verifier, oracle_tables):
     fx = load_golden("pairs_N26.json")
     v, T = verifier(26), oracle_tables(26)
@@ -144,3 +173,19 @@ def test_cli_drop_in_output():
     assert lines[0] == "Number of kernel launches = 6. Spot checks = 0. Complete hash = 86E5527C."
     assert lines[1].startswith("# results {") and '"seeds_checked": 142133' in lines[1]
     assert p.stdout == ""
+
+
+def test_iteration_cap_reports_instead_of_running_on():
+    """A per-seed checkpoint cap that real seeds exceed ends those seeds with
+    the ERR_ITER_CAP bit and a failure count (status COLLATZ_E_DEVICE); the
+    launch finishes and the context stays usable."""
+    import collatz_b200 as cb
+    with cb.Verifier(26, iter_cap=2) as v:
+        r = v.run_case(3, 2, 2, 9, 1, 0, check=False)
+        assert r.errors & 0x2
+        with pytest.raises(cb.CollatzError) as e:
+            v.run_case(3, 2, 2, 9, 1, 0)
+        assert e.value.status == cb.E_DEVICE
+        assert v.trajectory([27, 97])[0][0] == 3  # trajectory queries: status 3, iteration cap
+    # a fresh context computes the reference's answer
+    assert f"{cb.Verifier(26).run_case(3, 2, 2, 9, 1, 0).hash:X}" == "86E5527C"
