@@ -340,16 +340,22 @@ __device__ __forceinline__ bool expand_one(WT& W, const RangeArgs& A, const uint
     const u32 t0 = q0 << kb, t1 = __funnelshift_l(q0, q1, kb), t2 = __funnelshift_l(q1, q2, kb);
     const u32 qk0 = (k >= 32) ? 0u : t0, qk1 = (k >= 32) ? t0 : t1, qk2 = (k >= 32) ? t1 : t2;
     const u32 nbl = (q2 ? 96u - __clz(q2) : (q1 ? 64u - __clz(q1) : 32u - __clz(q0))) + k;
-    const u32 b9 = (mod9_96(q0, q1, q2) * k9) % 9u;
     const u32 meta_item = (slot << 8) | (nbl << 16);
     const bool jump_ok_base = true;
+    if (it.mod9) {  // segments of whole kept classes (the usual case) need no per-entry test
+      const u32 b9 = (mod9_96(q0, q1, q2) * k9) % 9u;
 #pragma unroll
-    for (u32 j = 0; j < RANGE_ITEM / 32; j++) {
-      if (it.sbase + j * 32 + lane < it.send) {
-        u32 x = b9 + ((e[j].y >> 16) & 0xFFu);
-        x = (x >= 9u) ? x - 9u : x;
-        if (!it.mod9 || (((NEG ? KEEP9N : KEEP9) >> x) & 1u)) mask |= 1u << j;
+      for (u32 j = 0; j < RANGE_ITEM / 32; j++) {
+        if (it.sbase + j * 32 + lane < it.send) {
+          u32 x = b9 + ((e[j].y >> 16) & 0xFFu);
+          x = (x >= 9u) ? x - 9u : x;
+          if (((NEG ? KEEP9N : KEEP9) >> x) & 1u) mask |= 1u << j;
+        }
       }
+    } else {
+#pragma unroll
+      for (u32 j = 0; j < RANGE_ITEM / 32; j++)
+        if (it.sbase + j * 32 + lane < it.send) mask |= 1u << j;
     }
     pos = tail + warp_excl_scan(__popc(mask), &total);
 #pragma unroll
