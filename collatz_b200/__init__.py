@@ -36,7 +36,11 @@ class CollatzError(RuntimeError):
 
 class Config(C.Structure):
     _fields_ = [("maxbits", C.c_uint32), ("range_k", C.c_uint32), ("device", C.c_int32),
-                ("variant", C.c_uint32), ("iter_cap", C.c_uint32), ("reserved", C.c_uint32 * 11)]
+                ("variant", C.c_uint32), ("iter_cap", C.c_uint32), ("flags", C.c_uint32),
+                ("reserved", C.c_uint32 * 10)]
+
+
+CFG_HOST_STEP1 = 0x1  # collatz_run_case: Step 1 on the host threads instead of the device
 
 
 class Case(C.Structure):
@@ -129,6 +133,8 @@ def lib() -> C.CDLL:
             "collatz_verify_pairs": (C.c_int, [P, C.c_uint32, P, C.c_uint32, C.POINTER(CaseResultC)]),
             "collatz_step1_pairs": (C.c_int, [C.c_uint32, C.POINTER(Case), P, C.c_uint64,
                                               C.POINTER(C.c_uint64)]),
+            "collatz_step1_pairs_device": (C.c_int, [P, C.POINTER(Case), P, C.c_uint64,
+                                                     C.POINTER(C.c_uint64)]),
             "collatz_case_tables": (C.c_int, [P, P, P]),
             "collatz_range_sieve": (C.c_int, [P, C.c_uint32, P, C.POINTER(C.c_uint64)]),
             "collatz_verify_range": (C.c_int, [P, C.POINTER(Range), C.POINTER(RangeResultC)]),
@@ -290,11 +296,14 @@ class Verifier:
     """One device context (tables resident in HBM)."""
 
     def __init__(self, maxbits: int = 45, range_k: int = 24, device: int = 0,
-                 variant: int | None = None, iter_cap: int = 0):
+                 variant: int | None = None, iter_cap: int = 0, host_step1: bool = False):
+        """host_step1: run_case runs Step 1 on the host threads (the default
+        is the device)."""
         cfg = Config()
         lib().collatz_config_default(C.byref(cfg))
         cfg.maxbits, cfg.range_k, cfg.device = maxbits, range_k, device
         cfg.iter_cap = iter_cap
+        cfg.flags = CFG_HOST_STEP1 if host_step1 else 0
         if variant is not None:
             cfg.variant = variant
         h = C.c_void_p()
@@ -363,6 +372,24 @@ class Verifier:
         if check:
             self._check(rc, "run_case")
         return _case_result(r, ov, overflow_cap)
+
+    def step1_pairs_device(self, base, sigfig, threepower, number, doubleeven, numevens, cap=None):
+        """Step-1 leaves [(bigindex, base, number)] from the device Step 1, in
+        no particular order (compare with step1_pairs as sorted lists)."""
+        c = make_case(base, sigfig, threepower, number, doubleeven, numevens)
+        cnt = C.c_uint64()
+        self._check(lib().collatz_step1_pairs_device(self._h, C.byref(c), None, 0, C.byref(cnt)),
+                    "step1_pairs_device")
+        n = cnt.value if cap is None else min(cap, cnt.value)
+        import numpy as np
+        buf = np.zeros((max(1, n), 8), dtype=np.uint32)
+        self._check(lib().collatz_step1_pairs_device(self._h, C.byref(c), buf.ctypes.data, n, C.byref(cnt)),
+                    "step1_pairs_device")
+        out = []
+        for w in buf[:n].tolist():
+            out.append((w[3], w[0] | (w[1] << 32) | (w[2] << 64),
+                        w[4] | (w[5] << 32) | (w[6] << 64) | (w[7] << 96)))
+        return out
 
     def launchkernel(self, bigindex: int, pairs, overflow_cap: int = 1 << 16,
                      check: bool = True) -> CaseResult:

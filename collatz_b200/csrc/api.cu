@@ -303,10 +303,12 @@ extern "C" void collatz_destroy(collatz_ctx* c) {
   for (auto& kv : c->rt) free_range_table(&kv.second.dev);
   DevBuf* bufs[] = {&c->d_rec, &c->d_counter, &c->d_overflow, &c->d_ovcount, &c->d_pairs[0], &c->d_pairs[1],
                     &c->d_segs, &c->d_widen, &c->d_widen2, &c->d_wcount, &c->t_seeds, &c->t_st, &c->t_exc,
-                    &c->t_status, &c->t_idx[0], &c->t_idx[1], &c->t_cnt};
+                    &c->t_status, &c->t_idx[0], &c->t_idx[1], &c->t_cnt, &c->s1_front[0], &c->s1_front[1],
+                    &c->s1_off, &c->s1_cnt, &c->s1_scal, &c->s1_stk_num, &c->s1_stk_meta};
   for (DevBuf* b : bufs) b->release();
   c->h_rec.release();
   c->h_pairs.release();
+  c->h_s1.release();
   for (auto& ev : c->ev)
     if (ev) cudaEventDestroy(ev);
   if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
@@ -468,6 +470,17 @@ extern "C" int collatz_step1_pairs(uint32_t maxbits, const collatz_case* cs, uin
   return COLLATZ_OK;
 }
 
+// The reference's counters from the leaves per bigindex (counts[16]: bigindex
+// >= 16, the CPU path of cu:517-519): one launch per full bucket of 2^16
+// pairs plus one per non-empty final flush (cu:532-534, 177-179).
+static void leaf_counts_to_result(const uint64_t counts[17], collatz_case_result* out) {
+  for (int b = 0; b < 16; b++) {
+    out->pairs += counts[b];
+    out->launches += (counts[b] + (1u << 16) - 1) >> 16;
+  }
+  out->cpu_pairs = counts[16];
+}
+
 namespace {
 
 // Host Step 1 on all cores feeding batches of pairs to the GPU.
@@ -522,19 +535,9 @@ struct CaseWorker {
 
 }  // namespace
 
-extern "C" int collatz_run_case(collatz_ctx* c, const collatz_case* cs, collatz_case_result* out) {
-  if (!c || !cs || !out) return COLLATZ_E_ARG;
-  if (cs->sigfig > c->ct.mbi || cs->threepower >= 128) return COLLATZ_E_ARG;  // cu:515 is never reached
-  std::lock_guard<std::recursive_mutex> g(c->mu);
-  uint32_t* ovbuf = out->overflow_seeds;
-  const uint64_t ovcap = out->overflow_cap;
-  std::memset(out, 0, sizeof *out);
-  out->overflow_seeds = ovbuf;
-  out->overflow_cap = ovcap;
-  CK(c, cudaSetDevice(c->device));
-  int rc = case_prepare(c);
-  if (rc) return rc;
-
+// Step 1 on the host threads, batches copied to the device (the pipeline
+// above); COLLATZ_CFG_HOST_STEP1.
+static int run_case_host(collatz_ctx* c, const collatz_case* cs, collatz_case_result* out) {
   Step1 s1(c->ct.mbi, c->ct.tpo);
   const Step1Node root{u128_of(cs->base), cs->sigfig, cs->threepower, u128_of(cs->number), cs->doubleeven,
                        cs->numevens};
@@ -641,13 +644,200 @@ extern "C" int collatz_run_case(collatz_ctx* c, const collatz_case* cs, collatz_
   uint64_t counts[17] = {};
   for (auto& w : ws)
     for (int i = 0; i < 17; i++) counts[i] += w.counts[i];
-  for (int b = 0; b < 16; b++) {
-    out->pairs += counts[b];
-    out->launches += (counts[b] + (1u << 16) - 1) >> 16;  // full buckets + final flush (cu:532-534, 177-179)
-  }
-  out->cpu_pairs = counts[16];
+  leaf_counts_to_result(counts, out);
   out->device_ms = ms;
   return case_finish(c, out);
+}
+
+// ---------------------------------------------------------------------
+// Step 1 on the device (step1_dev.cu).
+// ---------------------------------------------------------------------
+
+namespace {
+
+constexpr uint32_t S1_ROOTS = 2048;               // subtree roots cut on the host
+constexpr uint64_t S1_FRONTIER_CAP = 1ull << 21;  // nodes of the last breadth-first level
+constexpr uint64_t S1_CHUNK = 1ull << 22;         // pairs per emit pass and cases launch
+
+struct S1Run {
+  uint32_t nroots = 0, levels = 0, s0 = 0;
+  const S1Node* front = nullptr;
+  const uint32_t* front_count = nullptr;
+  uint64_t total = 0;
+  uint64_t hist[17] = {};
+  float ms = 0;  // device time of the breadth-first levels and the count pass
+};
+
+Step1Args s1_args(collatz_ctx* c) {
+  Step1Args a;
+  std::memset(&a, 0, sizeof a);
+  S1Scalars* sc = c->s1_scal.as<S1Scalars>();
+  a.mbi = c->ct.mbi;
+  a.tpo = c->ct.tpo;
+  a.off = c->s1_off.as<unsigned long long>();
+  a.cnt = c->s1_cnt.as<unsigned long long>();
+  a.total = &sc->total;
+  a.hist = sc->hist;
+  a.stk_num = c->s1_stk_num.as<ulonglong2>();
+  a.stk_meta = c->s1_stk_meta.as<uint4>();
+  a.nthreads = (uint32_t)c->sm_count * STEP1_WALK_BLOCKS_PER_SM * 128u;
+  return a;
+}
+
+}  // namespace
+
+// Step 1 down to the leaf count of every frontier node: the host cuts the
+// tree at the first level with >= S1_ROOTS nodes, the device expands as many
+// levels as the frontier buffer bounds (each level at most doubles), then the
+// count pass walks every frontier node's subtree.  Ends with the stream idle.
+static int s1_count(collatz_ctx* c, const collatz_case* cs, S1Run& R) {
+  const uint32_t mbi = c->ct.mbi;
+  Step1 s1(mbi, c->ct.tpo);
+  const Step1Node root{u128_of(cs->base), cs->sigfig, cs->threepower, u128_of(cs->number), cs->doubleeven,
+                       cs->numevens};
+  std::vector<Step1Node> roots;
+  uint32_t cut = cs->sigfig;
+  for (;;) {
+    roots.clear();
+    s1.split(root, cut, roots);
+    if (roots.size() >= S1_ROOTS || roots.empty() || cut >= mbi) break;
+    cut++;
+  }
+  R.nroots = (uint32_t)roots.size();
+  if (roots.empty()) return COLLATZ_OK;
+  uint64_t bound = R.nroots;
+  uint32_t d = 0;
+  while (cut + d < mbi && bound * 2 <= S1_FRONTIER_CAP) {
+    bound *= 2;
+    d++;
+  }
+  R.levels = d;
+  R.s0 = cut + d;
+  Step1Args a = s1_args(c);
+  const uint64_t depth = mbi - R.s0;
+  CK(c, c->s1_front[0].ensure(sizeof(S1Node) * bound));
+  CK(c, c->s1_front[1].ensure(sizeof(S1Node) * bound));
+  CK(c, c->s1_off.ensure(8 * bound));
+  CK(c, c->s1_cnt.ensure(8 * bound));
+  CK(c, c->s1_scal.ensure(sizeof(S1Scalars)));
+  if (depth) {
+    CK(c, c->s1_stk_num.ensure(16 * depth * a.nthreads));
+    CK(c, c->s1_stk_meta.ensure(16 * depth * a.nthreads));
+  }
+  CK(c, c->h_s1.ensure(std::max(sizeof(S1Scalars), sizeof(S1Node) * (size_t)R.nroots + 4)));
+  a = s1_args(c);  // buffers may have moved
+  S1Node* hn = c->h_s1.as<S1Node>();
+  for (uint32_t i = 0; i < R.nroots; i++) {
+    const Step1Node& r = roots[i];
+    hn[i] = S1Node{(unsigned long long)r.base, (unsigned long long)(r.base >> 64), (unsigned long long)r.number,
+                   (unsigned long long)(r.number >> 64), r.sigfig, r.threepower, r.doubleeven, r.numevens};
+  }
+  uint32_t* hcount = reinterpret_cast<uint32_t*>(hn + R.nroots);
+  *hcount = R.nroots;
+  S1Scalars* sc = c->s1_scal.as<S1Scalars>();
+  CK(c, cudaEventRecord(c->ev[2], c->stream));
+  CK(c, cudaMemsetAsync(sc, 0, sizeof(S1Scalars), c->stream));
+  CK(c, cudaMemcpyAsync(c->s1_front[0].p, hn, sizeof(S1Node) * R.nroots, cudaMemcpyHostToDevice, c->stream));
+  CK(c, cudaMemcpyAsync(&sc->level[0], hcount, 4, cudaMemcpyHostToDevice, c->stream));
+  for (uint32_t l = 0; l < d; l++) {
+    a.in = c->s1_front[l & 1].as<S1Node>();
+    a.in_count = &sc->level[l];
+    a.out = c->s1_front[(l + 1) & 1].as<S1Node>();
+    a.out_count = &sc->level[l + 1];
+    CK(c, launch_step1_expand(a, (uint32_t)((uint64_t)R.nroots << l), c->stream));
+  }
+  R.front = c->s1_front[d & 1].as<S1Node>();
+  R.front_count = &sc->level[d];
+  a.in = R.front;
+  a.in_count = R.front_count;
+  a.cursor = &sc->cursor[0];
+  CK(c, launch_step1_walk(a, false, c->stream));
+  CK(c, cudaEventRecord(c->ev[3], c->stream));
+  S1Scalars* hs = c->h_s1.as<S1Scalars>();
+  CK(c, cudaMemcpyAsync(&hs->total, &sc->total, 8 * 18, cudaMemcpyDeviceToHost, c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  R.total = hs->total;
+  std::memcpy(R.hist, hs->hist, sizeof R.hist);
+  CK(c, cudaEventElapsedTime(&R.ms, c->ev[2], c->ev[3]));
+  return COLLATZ_OK;
+}
+
+// Emit pass: the pairs with leaf index in [lo, hi) to dst (device).
+static cudaError_t s1_emit(collatz_ctx* c, const S1Run& R, uint64_t lo, uint64_t hi, uint32_t* dst) {
+  Step1Args a = s1_args(c);
+  S1Scalars* sc = c->s1_scal.as<S1Scalars>();
+  a.in = R.front;
+  a.in_count = R.front_count;
+  a.cursor = &sc->cursor[1];
+  a.pairs = dst;
+  a.w_lo = lo;
+  a.w_hi = hi;
+  cudaError_t e = cudaMemsetAsync(a.cursor, 0, 4, c->stream);
+  if (e == cudaSuccess) e = launch_step1_walk(a, true, c->stream);
+  return e;
+}
+
+static int run_case_device(collatz_ctx* c, const collatz_case* cs, collatz_case_result* out) {
+  S1Run R;
+  int rc = s1_count(c, cs, R);
+  if (rc) return rc;
+  double ms = R.ms;
+  if (R.total) {
+    CK(c, c->d_pairs[0].ensure(32 * std::min<uint64_t>(R.total, S1_CHUNK)));
+    uint32_t* dp = c->d_pairs[0].as<uint32_t>();
+    CK(c, cudaEventRecord(c->ev[0], c->stream));
+    for (uint64_t lo = 0; lo < R.total; lo += S1_CHUNK) {
+      const uint64_t hi = std::min<uint64_t>(R.total, lo + S1_CHUNK);
+      CK(c, s1_emit(c, R, lo, hi, dp));
+      CK(c, cudaMemsetAsync(c->d_counter.p, 0, sizeof(uint32_t), c->stream));
+      CasesArgs a = case_args(c, dp, (uint32_t)(hi - lo), -1);
+      CK(c, launch_cases(a, c->cases_variant, grid_for(c, 0, c->cases_variant), c->stream));
+    }
+    CK(c, cudaEventRecord(c->ev[1], c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    float x = 0;
+    CK(c, cudaEventElapsedTime(&x, c->ev[0], c->ev[1]));
+    ms += x;
+  }
+  leaf_counts_to_result(R.hist, out);
+  out->device_ms = ms;
+  return case_finish(c, out);
+}
+
+extern "C" int collatz_run_case(collatz_ctx* c, const collatz_case* cs, collatz_case_result* out) {
+  if (!c || !cs || !out) return COLLATZ_E_ARG;
+  if (cs->sigfig > c->ct.mbi || cs->threepower >= 128) return COLLATZ_E_ARG;  // cu:515 is never reached
+  std::lock_guard<std::recursive_mutex> g(c->mu);
+  uint32_t* ovbuf = out->overflow_seeds;
+  const uint64_t ovcap = out->overflow_cap;
+  std::memset(out, 0, sizeof *out);
+  out->overflow_seeds = ovbuf;
+  out->overflow_cap = ovcap;
+  CK(c, cudaSetDevice(c->device));
+  int rc = case_prepare(c);
+  if (rc) return rc;
+  return (c->cfg.flags & COLLATZ_CFG_HOST_STEP1) ? run_case_host(c, cs, out) : run_case_device(c, cs, out);
+}
+
+extern "C" int collatz_step1_pairs_device(collatz_ctx* c, const collatz_case* cs, uint32_t* pairs, uint64_t cap,
+                                          uint64_t* count) {
+  if (!c || !cs || !count || (cap && !pairs)) return COLLATZ_E_ARG;
+  if (cs->sigfig > c->ct.mbi || cs->threepower >= 128) return COLLATZ_E_ARG;
+  std::lock_guard<std::recursive_mutex> g(c->mu);
+  CK(c, cudaSetDevice(c->device));
+  S1Run R;
+  int rc = s1_count(c, cs, R);
+  if (rc) return rc;
+  *count = R.total;
+  const uint64_t want = std::min<uint64_t>(cap, R.total);
+  if (want) CK(c, c->d_pairs[0].ensure(32 * std::min<uint64_t>(want, S1_CHUNK)));
+  for (uint64_t lo = 0; lo < want; lo += S1_CHUNK) {
+    const uint64_t hi = std::min<uint64_t>(want, lo + S1_CHUNK);
+    CK(c, s1_emit(c, R, lo, hi, c->d_pairs[0].as<uint32_t>()));
+    CK(c, cudaMemcpyAsync(pairs + 8 * lo, c->d_pairs[0].p, 32 * (hi - lo), cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+  }
+  return COLLATZ_OK;
 }
 
 // =====================================================================

@@ -29,6 +29,44 @@ int cases_variants();
 cudaError_t launch_cases(const CasesArgs& a, int variant, uint32_t grid, cudaStream_t st);
 cudaError_t cases_occupancy(int variant, int* blocks_per_sm);
 
+// ---------------- device Step 1 (step1_dev.cu) ----------------
+// A node of search1's tree (cu:497-505): base and number as little-endian
+// 64-bit halves; sigfig, threepower, doubleeven, numevens.
+struct S1Node {
+  unsigned long long base_lo, base_hi, num_lo, num_hi;
+  uint32_t sig, tp, de, ne;
+};
+static_assert(sizeof(S1Node) == 48, "S1Node layout");
+
+// Counters of one device Step 1 run (zeroed before it starts).
+struct S1Scalars {
+  uint32_t level[128];  // frontier size after each breadth-first level
+  uint32_t cursor[32];  // [0] count pass, [1 + chunk % 31] emit passes
+  unsigned long long total;
+  unsigned long long hist[17];  // leaves per bigindex; [16] = bigindex >= 16
+};
+
+struct Step1Args {
+  uint32_t mbi, tpo;
+  const S1Node* in;          // frontier
+  const uint32_t* in_count;  // its size (device)
+  S1Node* out;               // expand: children
+  uint32_t* out_count;
+  unsigned long long* off;   // walk: per frontier node, first leaf index
+  unsigned long long* cnt;   // walk: per frontier node, leaves
+  unsigned long long* total;
+  unsigned long long* hist;
+  uint32_t* cursor;          // walk: zero before the launch
+  ulonglong2* stk_num;       // walk: pending siblings, [level][thread]
+  uint4* stk_meta;
+  uint32_t nthreads;         // walk: threads of the launch (grid x 128)
+  uint32_t* pairs;           // emit: pairs with leaf index in [w_lo, w_hi)
+  unsigned long long w_lo, w_hi;
+};
+constexpr uint32_t STEP1_WALK_BLOCKS_PER_SM = 8;
+cudaError_t launch_step1_expand(const Step1Args& a, uint32_t bound, cudaStream_t st);
+cudaError_t launch_step1_walk(const Step1Args& a, bool emit, cudaStream_t st);
+
 // ---------------- range mode (range.cu) ----------------
 constexpr uint32_t RANGE_ITEM = 64;     // survivor-table entries per work item
 constexpr uint32_t DENSE_ITEM = 64;     // consecutive integers per dense work item

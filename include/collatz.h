@@ -58,9 +58,13 @@ typedef struct {
   int32_t device;       /* CUDA device ordinal; default 0 */
   uint32_t variant;     /* kernel variant, COLLATZ_VARIANT_AUTO = tuned default */
   uint32_t iter_cap;    /* per-seed loop cap in checkpoints / run pairs (0 = default 1<<16) */
-  uint32_t reserved[11];
+  uint32_t flags;       /* COLLATZ_CFG_* bits; default 0 */
+  uint32_t reserved[10];
 } collatz_config;
 #define COLLATZ_VARIANT_AUTO 0xFFFFFFFFu
+/* collatz_run_case runs Step 1 (search1, cu:497-563) on the host threads
+ * and copies the pairs to the device, instead of on the device. */
+#define COLLATZ_CFG_HOST_STEP1 0x1u
 
 void collatz_config_default(collatz_config *cfg);
 /* Builds the reference's sieve tables for cfg->maxbits on the device
@@ -105,11 +109,14 @@ typedef struct {
   uint32_t max_stopping_time_seed[4];
   uint32_t errors;          /* COLLATZ_ERR_* bits */
   uint32_t reserved;
-  double device_ms;         /* device time of the Step 2/3 kernels */
+  double device_ms;         /* device time of the kernels (Steps 2/3, and Step 1 when on the device) */
 } collatz_case_result;
 
-/* Whole run from one 6-tuple (replaces main, cu:95-183): host Step 1
- * (search1, cu:497-563) on all host threads feeding the GPU. */
+/* Whole run from one 6-tuple (replaces main, cu:95-183).  Step 1
+ * (search1, cu:497-563) runs on the device and writes the pairs into
+ * device memory, where Steps 2-3 read them; with COLLATZ_CFG_HOST_STEP1 it
+ * runs on all host threads feeding batches to the GPU instead.  Both give
+ * the same result. */
 int collatz_run_case(collatz_ctx *ctx, const collatz_case *c, collatz_case_result *out);
 
 /* One batch of Step-1 pairs of one bucket (replaces launchkernel,
@@ -145,6 +152,14 @@ int collatz_verify_pairs_noalloc(collatz_ctx *ctx, uint32_t bigindex, const uint
  * written up to cap).  Host-only: needs no device. */
 int collatz_step1_pairs(uint32_t maxbits, const collatz_case *c, uint32_t *pairs, uint64_t cap,
                         uint64_t *count);
+
+/* No counterpart in the reference.  The Step-1 leaves of a case computed by
+ * the device Step 1 of collatz_run_case, for the context's N, in no
+ * particular order (the same multiset as collatz_step1_pairs).  *count
+ * receives the number of leaves; pairs (8 uint32 each, base limb 3 =
+ * bigindex) are written up to cap. */
+int collatz_step1_pairs_device(collatz_ctx *ctx, const collatz_case *c, uint32_t *pairs, uint64_t cap,
+                               uint64_t *count);
 
 /* ---- Cases driver: many cases_* lines with a resume journal ---- */
 /* The reference is run as one process per cases_* line and the results are
