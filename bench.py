@@ -221,29 +221,37 @@ def run_batched(v, n_req: int = 4096, seed: int = 4096, lo_log2: int = 20, hi_lo
 
 
 def run_cases() -> dict:
-    """Cases mode, the reference's own verification run (Algorithm 1: host
-    Step 1, GPU Steps 2-3), end to end through collatz_run_case on the golden
-    tuples with more than 10^7 seeds (N = 36 root case; N = 45 cases_tiny
-    lines 1-3), each checked against the reference's hash and launch count.
-    CPU: the oracle's restatement of the reference, one thread like the
-    reference's host program, on the N = 36 root case."""
+    """Cases mode, the reference's own verification run (Algorithm 1: Step 1
+    on the device, Steps 2-3), end to end through collatz_run_case on the
+    golden tuples with more than 10^7 seeds (N = 36 root case; N = 45
+    cases_tiny lines 1-3), each checked against the reference's hash and
+    launch count.  `host_step1_s`: the same call with Step 1 on the host
+    threads (COLLATZ_CFG_HOST_STEP1).  CPU: the oracle's restatement of the
+    reference, one thread like the reference's host program, on the N = 36
+    root case."""
     import collatz_b200 as cb
     from oracle import oracle as O
     with open(os.path.join(ROOT, "tests", "golden", "cases_runs.json")) as f:
         runs = [r for r in json.load(f)["runs"] if r["N"] in (36, 45) and r["seeds"] > 10 ** 7]
     verifiers, out = {}, []
-    for r in runs:
-        if r["N"] not in verifiers:
-            verifiers[r["N"]] = cb.Verifier(r["N"])
-        v = verifiers[r["N"]]
-        v.run_case(*r["tuple"])  # warm-up (host pools, first launches)
+
+    def timed(v, tup):
+        v.run_case(*tup)  # warm-up (buffers, first launches)
         t0 = time.perf_counter()
-        res = v.run_case(*r["tuple"])
-        dt = time.perf_counter() - t0
+        res = v.run_case(*tup)
+        return res, time.perf_counter() - t0
+
+    for r in runs:
+        for host in (False, True):
+            if (r["N"], host) not in verifiers:
+                verifiers[(r["N"], host)] = cb.Verifier(r["N"], host_step1=host)
+        res, dt = timed(verifiers[(r["N"], False)], r["tuple"])
+        hres, hdt = timed(verifiers[(r["N"], True)], r["tuple"])
         out.append({"N": r["N"], "tuple": r["tuple"], "seeds": res.seeds_checked, "s": dt,
-                    "seeds_per_s": res.seeds_checked / dt, "device_ms": res.device_ms,
-                    "hash_ok": f"{res.hash:X}" == r["hash"], "launches_ok": res.launches == r["launches"],
-                    "seeds_ok": res.seeds_checked == r["seeds"]})
+                    "seeds_per_s": res.seeds_checked / dt, "device_ms": res.device_ms, "host_step1_s": hdt,
+                    "hash_ok": f"{res.hash:X}" == r["hash"] and hres.hash == res.hash,
+                    "launches_ok": res.launches == r["launches"] == hres.launches,
+                    "seeds_ok": res.seeds_checked == r["seeds"] == hres.seeds_checked})
     for v in verifiers.values():
         v.close()
     T = O.Tables(36)
@@ -251,7 +259,7 @@ def run_cases() -> dict:
     c = T.run_case(3, 2, 2, 9, 1, 0)
     cdt = time.perf_counter() - t0
     n45 = [o for o in out if o["N"] == 45]
-    return {"workload": "collatz_run_case (host Step 1 + GPU Steps 2-3) on the reference's golden tuples",
+    return {"workload": "collatz_run_case (Step 1 and Steps 2-3 on the GPU) on the reference's golden tuples",
             "runs": out,
             "n45_seeds_per_s": sum(o["seeds"] for o in n45) / max(1e-9, sum(o["s"] for o in n45)),
             "all_match_reference": all(o["hash_ok"] and o["launches_ok"] and o["seeds_ok"] for o in out),

@@ -17,6 +17,9 @@
 // all lines, then the summary line with the summed launch count and the XOR
 // of the lines' hashes (the hash of the whole tree).  With --journal, each
 // finished line is recorded and a rerun resumes after the last finished one.
+//
+// Step 1 (search1, cu:497-563) runs on the GPU; --host-step1 runs it on the
+// host threads instead (same outputs).
 #include <cinttypes>
 #include <fstream>
 #include <cstdio>
@@ -51,9 +54,12 @@ int main(int argc, char** argv) {
   uint32_t maxbits = 45;
   if (const char* e = std::getenv("COLLATZ_MAXBITS")) maxbits = (uint32_t)std::atoi(e);
   std::string cases_file, journal;
+  bool host_step1 = false;
   for (int i = 1; i < argc; i++) {
     const std::string a = argv[i];
-    if (a == "--cases" && i + 1 < argc) {
+    if (a == "--host-step1") {
+      host_step1 = true;
+    } else if (a == "--cases" && i + 1 < argc) {
       cases_file = argv[++i];
     } else if (a == "--journal" && i + 1 < argc) {
       journal = argv[++i];
@@ -84,6 +90,7 @@ int main(int argc, char** argv) {
   collatz_config cfg;
   collatz_config_default(&cfg);
   cfg.maxbits = maxbits;
+  if (host_step1) cfg.flags |= COLLATZ_CFG_HOST_STEP1;
   collatz_ctx* ctx = nullptr;
   int rc = collatz_create(&cfg, &ctx);
   if (rc) {

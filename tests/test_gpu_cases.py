@@ -160,14 +160,15 @@ def test_bad_case_rejected(verifier):
         v.run_case(3, 17, 12, 9, 1, 0)  # sigfig > N - A: the reference never terminates
 
 
-def test_cli_drop_in_output():
+@pytest.mark.parametrize("flags", [[], ["--host-step1"]], ids=["device-step1", "host-step1"])
+def test_cli_drop_in_output(flags):
     """The CLI prints the reference's stderr summary (cu:181-182) and the
     overflow list on stdout (cu:298 format) for one stdin 6-tuple."""
     import os
     import subprocess
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     cli = os.path.join(root, "collatz_b200", "collatz_b200")
-    p = subprocess.run([cli, "26"], input="3 2 2 9 1 0\n", capture_output=True, text=True, timeout=300)
+    p = subprocess.run([cli] + flags + ["26"], input="3 2 2 9 1 0\n", capture_output=True, text=True, timeout=300)
     assert p.returncode == 0, p.stderr
     lines = p.stderr.splitlines()
     assert lines[0] == "Number of kernel launches = 6. Spot checks = 0. Complete hash = 86E5527C."

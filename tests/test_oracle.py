@@ -80,7 +80,9 @@ def test_step1_leaves_match_product(oracle_tables):
     in the same order as the oracle's restatement of search1."""
     import collatz_b200 as cb
     from oracle import oracle as O
-    for n, tup in ((26, (3, 2, 2, 9, 1, 0)), (36, (27, 10, 8, 183, 0, 0)), (45, (27, 25, 18, 335, 0, 1))):
+    for n, tup in ((26, (3, 2, 2, 9, 1, 0)), (36, (27, 10, 8, 183, 0, 0)), (45, (27, 25, 18, 335, 0, 1)),
+                   (26, (0, 5, 0, 1, 0, 0)), (26, (3, 16, 12, 9, 0, 0)), (30, (3, 2, 2, 9, 5, 0)),
+                   (30, (3, 2, 2, 9, 0, 7)), (30, (3, 2, 2, 9, 0, 0xFFFFFFFF))):
         assert cb.step1_pairs(n, *tup) == O.leaves(n, tup)
 
 
