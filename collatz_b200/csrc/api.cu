@@ -304,11 +304,14 @@ extern "C" void collatz_destroy(collatz_ctx* c) {
   DevBuf* bufs[] = {&c->d_rec, &c->d_counter, &c->d_overflow, &c->d_ovcount, &c->d_pairs[0], &c->d_pairs[1],
                     &c->d_segs, &c->d_widen, &c->d_widen2, &c->d_wcount, &c->t_seeds, &c->t_st, &c->t_exc,
                     &c->t_status, &c->t_idx[0], &c->t_idx[1], &c->t_cnt, &c->s1_front[0], &c->s1_front[1],
-                    &c->s1_off, &c->s1_cnt, &c->s1_scal, &c->s1_stk_num, &c->s1_stk_meta};
+                    &c->s1_off, &c->s1_cnt, &c->s1_scal, &c->s1_stk_num, &c->s1_stk_meta, &c->d_recs,
+                    &c->d_rcursor};
   for (DevBuf* b : bufs) b->release();
   c->h_rec.release();
   c->h_pairs.release();
   c->h_s1.release();
+  c->h_segs.release();
+  c->h_recs.release();
   for (auto& ev : c->ev)
     if (ev) cudaEventDestroy(ev);
   if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
@@ -858,25 +861,95 @@ struct collatz_plan {
   float last_ms = 0;
 };
 
-static int plan_build(collatz_ctx* c, const collatz_range* r, uint32_t n, collatz_plan* p) {
+// Checks that a batch uses one sieve (k, sign), fetches (or builds) its
+// tables and lowers every request into segments.
+static int range_lower_batch(collatz_ctx* c, const collatz_range* r, uint32_t n, RangeTables** T, uint32_t* k_out,
+                             bool* neg_out, std::vector<RangeSeg>& segs, unsigned long long& items) {
   const uint32_t k = r[0].k ? r[0].k : c->cfg.range_k;
   const bool neg = (r[0].flags & COLLATZ_RANGE_NEGATIVE) != 0;
   for (uint32_t i = 0; i < n; i++)  // one sieve (k, sign) per launch
     if ((r[i].k ? r[i].k : c->cfg.range_k) != k || ((r[i].flags & COLLATZ_RANGE_NEGATIVE) != 0) != neg)
       return COLLATZ_E_ARG;
   if (k < 8 || k > 34) return COLLATZ_E_ARG;
-  p->negative = neg;
-  int rc = get_range_tables(c, k, &p->T, neg);
+  int rc = get_range_tables(c, k, T, neg);
   if (rc) return rc;
   for (uint32_t i = 0; i < n; i++) {
-    rc = lower_range(c, r[i], i, *p->T, p->segs, p->items);
+    rc = lower_range(c, r[i], i, **T, segs, items);
     if (rc) return rc;
   }
-  if (p->segs.empty()) {  // keep the kernel's segment search well-defined
+  if (segs.empty()) {  // keep the kernel's segment search well-defined
     RangeSeg g{};
     g.kind = 1;
-    p->segs.push_back(g);
+    segs.push_back(g);
   }
+  *k_out = k;
+  *neg_out = neg;
+  return COLLATZ_OK;
+}
+
+// Device buffers of one range launch.
+struct RangeBufs {
+  RangeSeg* segs;
+  uint32_t nsegs;
+  unsigned long long items;
+  ReqRec* recs;
+  void* h_recs;  // pinned: the records come back here
+  uint32_t n;
+  unsigned long long* cursor;
+  WidenEntry* widen;
+  WidenEntry* widen2;
+  uint32_t* wcount;  // 2 counters
+  unsigned long long* stats;
+};
+
+static RangeArgs range_args(collatz_ctx* c, const RangeTables& T, uint32_t k, bool neg, const RangeBufs& b) {
+  RangeArgs a;
+  a.table = T.dev.table;
+  a.k = k;
+  a.segs = b.segs;
+  a.nsegs = b.nsegs;
+  a.item_cursor = b.cursor;
+  a.item_limit = b.items;
+  a.recs = b.recs;
+  a.widen = b.widen;
+  a.widen_cap = WIDEN_CAP;
+  a.widen_count = b.wcount;
+  a.iter_cap = c->iter_cap;
+  a.stats = b.stats;
+  a.negative = neg ? 1u : 0u;
+  return a;
+}
+
+// One range launch on stream s: record and counter reset, k_range, the
+// 192- and 256-bit widening passes, the record copy-back.  Captured into a
+// graph by plans; issued directly by collatz_verify_batch.
+static cudaError_t range_enqueue(collatz_ctx* c, const RangeArgs& a, const RangeBufs& b, cudaStream_t s) {
+  const size_t rb = sizeof(ReqRec) * std::max(1u, b.n);
+  const uint32_t grid = (uint32_t)grid_for(c, 1, c->range_variant);
+  cudaError_t e = cudaMemsetAsync(b.recs, 0, rb, s);
+  if (!e) e = cudaMemsetAsync(b.cursor, 0, sizeof(unsigned long long), s);
+  if (!e) e = cudaMemsetAsync(b.wcount, 0, sizeof(uint32_t) * 2, s);
+  if (!e && b.stats) e = cudaMemsetAsync(b.stats, 0, 16 * sizeof(unsigned long long), s);
+  if (!e) e = (b.stats && !a.negative) ? launch_range_stats(a, grid, s) : launch_range(a, c->range_variant, grid, s);
+  if (!e)
+    e = launch_range_wide(b.widen, b.wcount, WIDEN_CAP, 6, b.recs, b.widen2, WIDEN_CAP, b.wcount + 1, c->iter_cap, s,
+                          a.negative != 0);
+  if (!e)
+    e = launch_range_wide(b.widen2, b.wcount + 1, WIDEN_CAP, 8, b.recs, nullptr, 0, nullptr, c->iter_cap, s,
+                          a.negative != 0);
+  if (!e) e = cudaMemcpyAsync(b.h_recs, b.recs, rb, cudaMemcpyDeviceToHost, s);
+  return e;
+}
+
+static bool range_stats_requested() {
+  const char* dbg = getenv("COLLATZ_RANGE_STATS");
+  return dbg && dbg[0] == '1';
+}
+
+static int plan_build(collatz_ctx* c, const collatz_range* r, uint32_t n, collatz_plan* p) {
+  uint32_t k = 0;
+  int rc = range_lower_batch(c, r, n, &p->T, &k, &p->negative, p->segs, p->items);
+  if (rc) return rc;
   p->n = n;
   CK(c, p->d_segs.ensure(sizeof(RangeSeg) * p->segs.size()));
   CK(c, cudaMemcpy(p->d_segs.p, p->segs.data(), sizeof(RangeSeg) * p->segs.size(), cudaMemcpyHostToDevice));
@@ -886,44 +959,17 @@ static int plan_build(collatz_ctx* c, const collatz_range* r, uint32_t n, collat
   CK(c, p->d_widen.ensure(sizeof(WidenEntry) * WIDEN_CAP));
   CK(c, p->d_widen2.ensure(sizeof(WidenEntry) * WIDEN_CAP));
   CK(c, p->d_wcount.ensure(sizeof(uint32_t) * 2));
-
-  RangeArgs a;
-  a.table = p->T->dev.table;
-  a.k = k;
-  a.segs = p->d_segs.as<RangeSeg>();
-  a.nsegs = (uint32_t)p->segs.size();
-  a.item_cursor = p->d_cursor.as<unsigned long long>();
-  a.item_limit = p->items;
-  a.recs = p->d_recs.as<ReqRec>();
-  a.widen = p->d_widen.as<WidenEntry>();
-  a.widen_cap = WIDEN_CAP;
-  a.widen_count = p->d_wcount.as<uint32_t>();
-  a.iter_cap = c->iter_cap;
-  a.stats = nullptr;
-  a.negative = p->negative ? 1u : 0u;
-  const char* dbg = getenv("COLLATZ_RANGE_STATS");
-  p->stats = dbg && dbg[0] == '1';
-  if (p->stats) {
-    CK(c, p->d_stats.ensure(16 * sizeof(unsigned long long)));
-    a.stats = p->d_stats.as<unsigned long long>();
-  }
-  const uint32_t grid = (uint32_t)grid_for(c, 1, c->range_variant);
+  p->stats = range_stats_requested();
+  if (p->stats) CK(c, p->d_stats.ensure(16 * sizeof(unsigned long long)));
+  const RangeBufs b{p->d_segs.as<RangeSeg>(), (uint32_t)p->segs.size(), p->items, p->d_recs.as<ReqRec>(),
+                    p->h_recs.p, n, p->d_cursor.as<unsigned long long>(), p->d_widen.as<WidenEntry>(),
+                    p->d_widen2.as<WidenEntry>(), p->d_wcount.as<uint32_t>(),
+                    p->stats ? p->d_stats.as<unsigned long long>() : nullptr};
+  const RangeArgs a = range_args(c, *p->T, k, p->negative, b);
   cudaStream_t s = c->own_stream;
   CK(c, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-  cudaError_t e = cudaMemsetAsync(p->d_recs.p, 0, sizeof(ReqRec) * std::max(1u, n), s);
-  if (!e) e = cudaMemsetAsync(p->d_cursor.p, 0, sizeof(unsigned long long), s);
-  if (!e) e = cudaMemsetAsync(p->d_wcount.p, 0, sizeof(uint32_t) * 2, s);
-  if (!e && p->stats) e = cudaMemsetAsync(p->d_stats.p, 0, 16 * sizeof(unsigned long long), s);
-  if (!e) e = (p->stats && !p->negative) ? launch_range_stats(a, grid, s) : launch_range(a, c->range_variant, grid, s);
-  if (!e)
-    e = launch_range_wide(p->d_widen.as<WidenEntry>(), p->d_wcount.as<uint32_t>(), WIDEN_CAP, 6, a.recs,
-                          p->d_widen2.as<WidenEntry>(), WIDEN_CAP, p->d_wcount.as<uint32_t>() + 1, c->iter_cap, s,
-                          p->negative);
-  if (!e)
-    e = launch_range_wide(p->d_widen2.as<WidenEntry>(), p->d_wcount.as<uint32_t>() + 1, WIDEN_CAP, 8, a.recs,
-                          nullptr, 0, nullptr, c->iter_cap, s, p->negative);
-  if (!e) e = cudaMemcpyAsync(p->h_recs.p, p->d_recs.p, sizeof(ReqRec) * std::max(1u, n), cudaMemcpyDeviceToHost, s);
-  cudaError_t e2 = cudaStreamEndCapture(s, &p->graph);
+  const cudaError_t e = range_enqueue(c, a, b, s);
+  const cudaError_t e2 = cudaStreamEndCapture(s, &p->graph);
   if (e) return set_cuda_error(c, e, "plan capture");
   if (e2) return set_cuda_error(c, e2, "cudaStreamEndCapture");
   CK(c, cudaGraphInstantiate(&p->exec, p->graph, 0));
@@ -997,15 +1043,59 @@ extern "C" void collatz_plan_destroy(collatz_plan* p) {
   delete p;
 }
 
+// One-shot batches run directly on the context's grow-only scratch: no
+// allocation, graph capture or free per call (each of those costs about a
+// millisecond of host time, and cudaFree synchronises the device).
 extern "C" int collatz_verify_batch(collatz_ctx* c, const collatz_range* r, uint32_t n, collatz_range_result* out) {
   if (!c || !r || !n || !out) return COLLATZ_E_ARG;
-  collatz_plan* p = nullptr;
-  int rc = collatz_plan_create(c, r, n, &p);
+  if (range_stats_requested()) {  // diagnostics go through a plan
+    collatz_plan* p = nullptr;
+    int rc = collatz_plan_create(c, r, n, &p);
+    if (rc) return rc;
+    rc = collatz_plan_launch(p);
+    if (!rc) rc = collatz_plan_results(p, out);
+    collatz_plan_destroy(p);
+    return rc;
+  }
+  std::lock_guard<std::recursive_mutex> g(c->mu);
+  CK(c, cudaSetDevice(c->device));
+  std::vector<RangeSeg>& segs = c->range_segs;
+  segs.clear();
+  unsigned long long items = 0;
+  RangeTables* T = nullptr;
+  uint32_t k = 0;
+  bool neg = false;
+  int rc = range_lower_batch(c, r, n, &T, &k, &neg, segs, items);
   if (rc) return rc;
-  rc = collatz_plan_launch(p);
-  if (!rc) rc = collatz_plan_results(p, out);
-  collatz_plan_destroy(p);
-  return rc;
+  const size_t sb = sizeof(RangeSeg) * segs.size(), rb = sizeof(ReqRec) * n;
+  CK(c, c->d_segs.ensure(sb));
+  CK(c, c->h_segs.ensure(sb));
+  CK(c, c->d_recs.ensure(rb));
+  CK(c, c->h_recs.ensure(rb));
+  CK(c, c->d_rcursor.ensure(sizeof(unsigned long long)));
+  CK(c, c->d_widen.ensure(sizeof(WidenEntry) * WIDEN_CAP));
+  CK(c, c->d_widen2.ensure(sizeof(WidenEntry) * WIDEN_CAP));
+  CK(c, c->d_wcount.ensure(sizeof(uint32_t) * 2));
+  std::memcpy(c->h_segs.p, segs.data(), sb);
+  const RangeBufs b{c->d_segs.as<RangeSeg>(), (uint32_t)segs.size(), items, c->d_recs.as<ReqRec>(), c->h_recs.p, n,
+                    c->d_rcursor.as<unsigned long long>(), c->d_widen.as<WidenEntry>(),
+                    c->d_widen2.as<WidenEntry>(), c->d_wcount.as<uint32_t>(), nullptr};
+  const RangeArgs a = range_args(c, *T, k, neg, b);
+  CK(c, cudaMemcpyAsync(c->d_segs.p, c->h_segs.p, sb, cudaMemcpyHostToDevice, c->stream));
+  CK(c, cudaEventRecord(c->ev[2], c->stream));
+  CK(c, range_enqueue(c, a, b, c->stream));
+  CK(c, cudaEventRecord(c->ev[3], c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);
+  const ReqRec* h = c->h_recs.as<ReqRec>();
+  int status = COLLATZ_OK;
+  for (uint32_t i = 0; i < n; i++) {
+    rec_to_range_result(h[i], &out[i]);
+    out[i].device_ms = ms;
+    if (out[i].status) status = out[i].status;
+  }
+  return status;
 }
 
 extern "C" int collatz_verify_range(collatz_ctx* c, const collatz_range* r, collatz_range_result* out) {

@@ -85,6 +85,10 @@ struct collatz_ctx {
   // scratch for the synchronous calls
   cz::DevBuf d_rec, d_counter, d_overflow, d_ovcount, d_pairs[2], d_segs, d_widen, d_widen2, d_wcount;
   cz::HostBuf h_rec, h_pairs;
+  // one-shot range batches (collatz_verify_batch / collatz_verify_range)
+  cz::DevBuf d_recs, d_rcursor;
+  cz::HostBuf h_segs, h_recs;
+  std::vector<cz::RangeSeg> range_segs;
   cz::DevBuf t_seeds, t_st, t_exc, t_status, t_idx[2], t_cnt;
   // device Step 1: frontier (ping-pong), per-node leaf offsets and counts,
   // counters, pending-sibling stack
