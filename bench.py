@@ -252,6 +252,33 @@ def run_cases() -> dict:
                     "hash_ok": f"{res.hash:X}" == r["hash"] and hres.hash == res.hash,
                     "launches_ok": res.launches == r["launches"] == hres.launches,
                     "seeds_ok": res.seeds_checked == r["seeds"] == hres.seeds_checked})
+    # many small lines, the shape of the reference's cases_big file: the whole
+    # N = 45 tree cut at sigfig 24, run through the line-batched driver
+    v45 = verifiers[(45, False)]
+    lines = cb.split_cases(45, (3, 2, 2, 9, 1, 0), 24)
+    t0 = time.perf_counter()
+    whole = v45.run_case(3, 2, 2, 9, 1, 0)
+    t_whole = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    comb, _, _ = v45.run_cases(lines, per_case=False)
+    t_lines = time.perf_counter() - t0
+    sample = 1000
+    t0 = time.perf_counter()
+    for c in lines[:sample]:
+        v45.run_case(*cb.case_tuple(c))
+    per_line_s = (time.perf_counter() - t0) / sample
+    many = {"workload": f"N=45 root case (3 2 2 9 1 0) cut at sigfig 24 into {len(lines)} lines "
+                        "(collatz_step1_split; the shape of the reference's cases_big), one collatz_run_cases "
+                        "call (groups of 8192 lines per device pass)",
+            "lines": len(lines), "seeds": comb.seeds_checked, "s": t_lines,
+            "seeds_per_s": comb.seeds_checked / t_lines, "lines_per_s": len(lines) / t_lines,
+            "device_s": comb.device_ms / 1e3, "xor_of_lines_equals_whole_run": comb.hash == whole.hash
+            and comb.seeds_checked == whole.seeds_checked,
+            "whole_run": {"hash": f"{whole.hash:X}", "seeds": whole.seeds_checked, "s": t_whole,
+                          "seeds_per_s": whole.seeds_checked / t_whole},
+            "one_call_per_line_ms": per_line_s * 1e3,
+            "vs_one_call_per_line": per_line_s * len(lines) / t_lines,
+            "one_call_per_line_sample": f"first {sample} lines, collatz_run_case each"}
     for v in verifiers.values():
         v.close()
     T = O.Tables(36)
@@ -263,6 +290,7 @@ def run_cases() -> dict:
             "runs": out,
             "n45_seeds_per_s": sum(o["seeds"] for o in n45) / max(1e-9, sum(o["s"] for o in n45)),
             "all_match_reference": all(o["hash_ok"] and o["launches_ok"] and o["seeds_ok"] for o in out),
+            "many_lines": many,
             "cpu_baseline": {"value": c.seeds / cdt, "unit": UNIT, "cores": 1, "kind": "port",
                              "sample": f"N=36 root case (3 2 2 9 1 0), {c.seeds} seeds in {cdt:.1f} s "
                                        "(oracle/collatz_oracle.c orc_run_case, the reference's kernel "
@@ -531,7 +559,7 @@ def main():
             # blocks between)
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 32 + 64 * 55,
                     "d2h_bytes_per_step": 136,
-                    "call": "collatz_verify_range (lower + upload work list + graph + result copy)"},
+                    "call": "collatz_verify_range (lower + upload work list + launches + result copy)"},
             "clocks": clocks,
             "gpu_launches": 3 * args.steps,
             "wall_s_timed": wall,

@@ -154,6 +154,9 @@ def lib() -> C.CDLL:
             "collatz_combine_case_results": (C.c_int, [P, C.c_uint32, C.POINTER(CaseResultC)]),
             "collatz_run_cases": (C.c_int, [P, P, C.c_uint32, C.c_char_p, P, C.POINTER(CaseResultC),
                                             C.POINTER(C.c_uint32)]),
+            "collatz_run_case_batch": (C.c_int, [P, P, C.c_uint32, P, P, C.c_uint64]),
+            "collatz_step1_split": (C.c_int, [C.c_uint32, C.POINTER(Case), C.c_uint32, P, C.c_uint64,
+                                              C.POINTER(C.c_uint64)]),
             "collatz_journal_load": (C.c_int, [C.c_char_p, P, C.c_uint32, P, P]),
             "collatz_variant_count": (C.c_int, [C.c_int]),
             "collatz_set_variant": (C.c_int, [P, C.c_int, C.c_int]),
@@ -273,6 +276,26 @@ def journal_load(journal: str, tuples, overflow_cap: int = 1 << 10):
     return {i: _case_result(res[i], bufs[i], overflow_cap) for i in range(n) if done[i]}
 
 
+def split_cases(maxbits: int, case, cut: int):
+    """The Step-1 tree nodes of `case` (a 6-tuple) at sigfig = cut, in the reference's
+    order (collatz_step1_split), as a ctypes Case array for Verifier.run_cases."""
+    c = make_case(*case)
+    cnt = C.c_uint64()
+    rc = lib().collatz_step1_split(maxbits, C.byref(c), cut, None, 0, C.byref(cnt))
+    if rc:
+        raise CollatzError(rc, "step1_split")
+    arr = (Case * max(1, cnt.value))()
+    rc = lib().collatz_step1_split(maxbits, C.byref(c), cut, arr, cnt.value, C.byref(cnt))
+    if rc:
+        raise CollatzError(rc, "step1_split")
+    return arr if cnt.value else (Case * 0)()
+
+
+def case_tuple(c: Case) -> tuple:
+    return (c.base[0] | (c.base[1] << 64), c.sigfig, c.threepower, c.number[0] | (c.number[1] << 64),
+            c.doubleeven, c.numevens)
+
+
 def step1_pairs(maxbits: int, base, sigfig, threepower, number, doubleeven, numevens, cap=None):
     """Step-1 leaves [(bigindex, base, number)] (host only, no device)."""
     c = make_case(base, sigfig, threepower, number, doubleeven, numevens)
@@ -373,6 +396,31 @@ class Verifier:
             self._check(rc, "run_case")
         return _case_result(r, ov, overflow_cap)
 
+    def run_case_batch(self, tuples, pool_cap: int = 1 << 16, check: bool = True) -> list[CaseResult]:
+        """Cases [(base, sigfig, threepower, number, doubleeven, numevens)] in one
+        device pass (collatz_run_case_batch); one CaseResult per case, as
+        run_case would give it."""
+        n = len(tuples)
+        if n == 0:
+            return []
+        arr = (Case * n)()
+        for i, t in enumerate(tuples):
+            arr[i] = make_case(*t)
+        res = (CaseResultC * n)()
+        pool = (C.c_uint32 * (4 * max(1, pool_cap)))()
+        rc = lib().collatz_run_case_batch(self._h, arr, n, res, pool, pool_cap)
+        if check:
+            self._check(rc, "run_case_batch")
+        out = []
+        for r in res:
+            k = r.overflow_cap if r.overflow_seeds else 0
+            ov = [_limbs(r.overflow_seeds[4 * j:4 * j + 4]) for j in range(k)]
+            out.append(CaseResult(r.hash, r.launches, r.spot_checks, r.seeds_checked, r.pairs, r.cpu_pairs,
+                                  r.n_overflow, ov, _limbs(r.max_excursion), _limbs(r.max_excursion_seed),
+                                  r.max_stopping_time, _limbs(r.max_stopping_time_seed), r.errors,
+                                  r.device_ms))
+        return out
+
     def step1_pairs_device(self, base, sigfig, threepower, number, doubleeven, numevens, cap=None):
         """Step-1 leaves [(bigindex, base, number)] from the device Step 1, in
         no particular order (compare with step1_pairs as sorted lists)."""
@@ -409,14 +457,19 @@ class Verifier:
 
     verify_pairs = launchkernel
 
-    def run_cases(self, tuples, journal: str | None = None, overflow_cap: int = 1 << 16):
-        """Runs cases_* lines [(base, sigfig, threepower, number, doubleeven, numevens)] in one
-        process (collatz_run_cases); returns (combined CaseResult, [per-case CaseResult], run now)."""
-        n = len(tuples)
-        arr = (Case * max(1, n))()
-        for i, t in enumerate(tuples):
-            arr[i] = make_case(*t)
-        per = (CaseResultC * max(1, n))()
+    def run_cases(self, tuples, journal: str | None = None, overflow_cap: int = 1 << 16,
+                  per_case: bool = True):
+        """Runs cases_* lines [(base, sigfig, threepower, number, doubleeven, numevens)], or a
+        ctypes Case array (split_cases), in one process (collatz_run_cases); returns
+        (combined CaseResult, [per-case CaseResult] or None, run now)."""
+        if isinstance(tuples, C.Array):
+            arr, n = tuples, len(tuples)
+        else:
+            n = len(tuples)
+            arr = (Case * max(1, n))()
+            for i, t in enumerate(tuples):
+                arr[i] = make_case(*t)
+        per = (CaseResultC * max(1, n))() if per_case else None
         comb = CaseResultC()
         ov = (C.c_uint32 * (4 * overflow_cap))()
         comb.overflow_seeds = C.cast(ov, C.POINTER(C.c_uint32))
@@ -425,8 +478,8 @@ class Verifier:
         rc = lib().collatz_run_cases(self._h, arr, n, journal.encode() if journal else None, per,
                                      C.byref(comb), C.byref(ran))
         self._check(rc, "run_cases")
-        return (_case_result(comb, ov, overflow_cap), [_case_result(per[i], None, 0) for i in range(n)],
-                ran.value)
+        return (_case_result(comb, ov, overflow_cap),
+                [_case_result(per[i], None, 0) for i in range(n)] if per_case else None, ran.value)
 
     def case_tables(self) -> tuple[bytes, bytes]:
         bv = (C.c_uint32 * (16 * BV_WORDS))()

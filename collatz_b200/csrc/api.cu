@@ -304,7 +304,7 @@ extern "C" void collatz_destroy(collatz_ctx* c) {
   DevBuf* bufs[] = {&c->d_rec, &c->d_counter, &c->d_overflow, &c->d_ovcount, &c->d_pairs[0], &c->d_pairs[1],
                     &c->d_segs, &c->d_widen, &c->d_widen2, &c->d_wcount, &c->t_seeds, &c->t_st, &c->t_exc,
                     &c->t_status, &c->t_idx[0], &c->t_idx[1], &c->t_cnt, &c->s1_front[0], &c->s1_front[1],
-                    &c->s1_off, &c->s1_cnt, &c->s1_scal, &c->s1_stk_num, &c->s1_stk_meta, &c->d_recs,
+                    &c->s1_off, &c->s1_cnt, &c->s1_scal, &c->s1_stk_num, &c->s1_stk_meta, &c->s1_hist, &c->d_recs,
                     &c->d_rcursor};
   for (DevBuf* b : bufs) b->release();
   c->h_rec.release();
@@ -374,6 +374,7 @@ static CasesArgs case_args(collatz_ctx* c, const uint32_t* d_pairs, uint32_t npa
   a.overflow_cap = OVERFLOW_CAP;
   a.overflow_count = c->d_ovcount.as<unsigned long long>();
   a.iter_cap = c->iter_cap;
+  a.multi = 0;
   return a;
 }
 
@@ -482,6 +483,25 @@ static void leaf_counts_to_result(const uint64_t counts[17], collatz_case_result
     out->launches += (counts[b] + (1u << 16) - 1) >> 16;
   }
   out->cpu_pairs = counts[16];
+}
+
+extern "C" int collatz_step1_split(uint32_t maxbits, const collatz_case* cs, uint32_t cut, collatz_case* out,
+                                   uint64_t cap, uint64_t* count) {
+  if (!cs || !count || (cap && !out) || maxbits < 16 || maxbits > 96) return COLLATZ_E_ARG;
+  const uint32_t mbi = maxbits - 10, tpo = mbi * 306 / 485 + 1;
+  if (cs->sigfig > cut || cut > mbi || cs->threepower >= 128) return COLLATZ_E_ARG;
+  Step1 s1(mbi, tpo);
+  const Step1Node root{u128_of(cs->base), cs->sigfig, cs->threepower, u128_of(cs->number), cs->doubleeven,
+                       cs->numevens};
+  std::vector<Step1Node> nodes;
+  s1.split(root, cut, nodes);
+  *count = nodes.size();
+  for (uint64_t i = 0; i < nodes.size() && i < cap; i++) {
+    const Step1Node& r = nodes[i];
+    out[i] = collatz_case{{(uint64_t)r.base, (uint64_t)(r.base >> 64)}, r.sigfig, r.threepower,
+                          {(uint64_t)r.number, (uint64_t)(r.number >> 64)}, r.doubleeven, r.numevens};
+  }
+  return COLLATZ_OK;
 }
 
 namespace {
@@ -689,33 +709,26 @@ Step1Args s1_args(collatz_ctx* c) {
 
 }  // namespace
 
-// Step 1 down to the leaf count of every frontier node: the host cuts the
-// tree at the first level with >= S1_ROOTS nodes, the device expands as many
-// levels as the frontier buffer bounds (each level at most doubles), then the
-// count pass walks every frontier node's subtree.  Ends with the stream idle.
-static int s1_count(collatz_ctx* c, const collatz_case* cs, S1Run& R) {
+// Step 1 down to the leaf count of every frontier node, from the given roots
+// (sigfig of each >= min_sig): the device expands as many breadth-first
+// levels as the frontier buffer bounds (each level at most doubles), then
+// the count pass walks every frontier node's subtree.  hist_lines (device,
+// 17 counters per line, zeroed) receives the leaves per (line, bigindex) of a
+// line batch; null for one case.  Ends with the stream idle.
+static int s1_count_roots(collatz_ctx* c, const std::vector<S1Node>& roots, uint32_t min_sig,
+                          unsigned long long* hist_lines, S1Run& R) {
   const uint32_t mbi = c->ct.mbi;
-  Step1 s1(mbi, c->ct.tpo);
-  const Step1Node root{u128_of(cs->base), cs->sigfig, cs->threepower, u128_of(cs->number), cs->doubleeven,
-                       cs->numevens};
-  std::vector<Step1Node> roots;
-  uint32_t cut = cs->sigfig;
-  for (;;) {
-    roots.clear();
-    s1.split(root, cut, roots);
-    if (roots.size() >= S1_ROOTS || roots.empty() || cut >= mbi) break;
-    cut++;
-  }
   R.nroots = (uint32_t)roots.size();
   if (roots.empty()) return COLLATZ_OK;
+  if (roots.size() > S1_FRONTIER_CAP) return COLLATZ_E_LIMIT;
   uint64_t bound = R.nroots;
   uint32_t d = 0;
-  while (cut + d < mbi && bound * 2 <= S1_FRONTIER_CAP) {
+  while (min_sig + d < mbi && bound * 2 <= S1_FRONTIER_CAP) {
     bound *= 2;
     d++;
   }
   R.levels = d;
-  R.s0 = cut + d;
+  R.s0 = min_sig + d;
   Step1Args a = s1_args(c);
   const uint64_t depth = mbi - R.s0;
   CK(c, c->s1_front[0].ensure(sizeof(S1Node) * bound));
@@ -729,12 +742,9 @@ static int s1_count(collatz_ctx* c, const collatz_case* cs, S1Run& R) {
   }
   CK(c, c->h_s1.ensure(std::max(sizeof(S1Scalars), sizeof(S1Node) * (size_t)R.nroots + 4)));
   a = s1_args(c);  // buffers may have moved
+  a.hist_lines = hist_lines;
   S1Node* hn = c->h_s1.as<S1Node>();
-  for (uint32_t i = 0; i < R.nroots; i++) {
-    const Step1Node& r = roots[i];
-    hn[i] = S1Node{(unsigned long long)r.base, (unsigned long long)(r.base >> 64), (unsigned long long)r.number,
-                   (unsigned long long)(r.number >> 64), r.sigfig, r.threepower, r.doubleeven, r.numevens};
-  }
+  std::memcpy(hn, roots.data(), sizeof(S1Node) * R.nroots);
   uint32_t* hcount = reinterpret_cast<uint32_t*>(hn + R.nroots);
   *hcount = R.nroots;
   S1Scalars* sc = c->s1_scal.as<S1Scalars>();
@@ -763,6 +773,30 @@ static int s1_count(collatz_ctx* c, const collatz_case* cs, S1Run& R) {
   std::memcpy(R.hist, hs->hist, sizeof R.hist);
   CK(c, cudaEventElapsedTime(&R.ms, c->ev[2], c->ev[3]));
   return COLLATZ_OK;
+}
+
+// One case: the host cuts the tree at the first level with >= S1_ROOTS nodes
+// (or at the leaves), then s1_count_roots.
+static int s1_count(collatz_ctx* c, const collatz_case* cs, S1Run& R) {
+  const uint32_t mbi = c->ct.mbi;
+  Step1 s1(mbi, c->ct.tpo);
+  const Step1Node root{u128_of(cs->base), cs->sigfig, cs->threepower, u128_of(cs->number), cs->doubleeven,
+                       cs->numevens};
+  std::vector<Step1Node> cut_nodes;
+  uint32_t cut = cs->sigfig;
+  for (;;) {
+    cut_nodes.clear();
+    s1.split(root, cut, cut_nodes);
+    if (cut_nodes.size() >= S1_ROOTS || cut_nodes.empty() || cut >= mbi) break;
+    cut++;
+  }
+  std::vector<S1Node> roots(cut_nodes.size());
+  for (size_t i = 0; i < cut_nodes.size(); i++) {
+    const Step1Node& r = cut_nodes[i];
+    roots[i] = S1Node{(unsigned long long)r.base, (unsigned long long)(r.base >> 64), (unsigned long long)r.number,
+                      (unsigned long long)(r.number >> 64), r.sigfig, r.threepower, r.doubleeven, r.numevens};
+  }
+  return s1_count_roots(c, roots, cut, nullptr, R);
 }
 
 // Emit pass: the pairs with leaf index in [lo, hi) to dst (device).
@@ -820,6 +854,115 @@ extern "C" int collatz_run_case(collatz_ctx* c, const collatz_case* cs, collatz_
   int rc = case_prepare(c);
   if (rc) return rc;
   return (c->cfg.flags & COLLATZ_CFG_HOST_STEP1) ? run_case_host(c, cs, out) : run_case_device(c, cs, out);
+}
+
+// Entry tests of search1 (cu:507-511) on a case's root, in the reference's
+// 32-bit arithmetic.
+static bool s1_root_pass(const collatz_case& cs) {
+  if (485u * cs.threepower <= 306u * cs.sigfig) return false;
+  if (cs.numevens >= 2u && cs.numevens % 2u == 0u && 306u * (cs.sigfig - 1u) >= 485u * (cs.threepower - 1u))
+    return false;
+  return true;
+}
+
+extern "C" int collatz_run_case_batch(collatz_ctx* c, const collatz_case* cases, uint32_t n,
+                                      collatz_case_result* out, uint32_t* overflow_pool, uint64_t pool_cap) {
+  if (!c || !n || !cases || !out || (pool_cap && !overflow_pool)) return COLLATZ_E_ARG;
+  if (n > COLLATZ_CASE_BATCH_MAX) return COLLATZ_E_LIMIT;
+  for (uint32_t i = 0; i < n; i++)
+    if (cases[i].sigfig > c->ct.mbi || cases[i].threepower >= 128) return COLLATZ_E_ARG;
+  std::lock_guard<std::recursive_mutex> g(c->mu);
+  std::memset(out, 0, sizeof(collatz_case_result) * n);
+  CK(c, cudaSetDevice(c->device));
+  int rc = case_prepare(c);
+  if (rc) return rc;
+  std::vector<S1Node> roots;
+  uint32_t min_sig = 0xFFFFFFFFu;
+  for (uint32_t i = 0; i < n; i++) {
+    const collatz_case& cs = cases[i];
+    if (!s1_root_pass(cs)) continue;  // search1 returns at once: no leaves
+    roots.push_back(S1Node{cs.base[0], cs.base[1], cs.number[0], cs.number[1], cs.sigfig | (i << 8), cs.threepower,
+                           cs.doubleeven, cs.numevens});
+    min_sig = std::min(min_sig, cs.sigfig);
+  }
+  const size_t rb = sizeof(ReqRec) * n, hb = 17 * sizeof(unsigned long long) * n;
+  CK(c, c->d_recs.ensure(rb));
+  CK(c, c->s1_hist.ensure(hb));
+  CK(c, cudaMemsetAsync(c->d_recs.p, 0, rb, c->stream));
+  CK(c, cudaMemsetAsync(c->s1_hist.p, 0, hb, c->stream));
+  S1Run R;
+  rc = s1_count_roots(c, roots, min_sig, c->s1_hist.as<unsigned long long>(), R);
+  if (rc) return rc;
+  double ms = R.ms;
+  if (R.total) {
+    CK(c, c->d_pairs[0].ensure(32 * std::min<uint64_t>(R.total, S1_CHUNK)));
+    uint32_t* dp = c->d_pairs[0].as<uint32_t>();
+    CK(c, cudaEventRecord(c->ev[0], c->stream));
+    for (uint64_t lo = 0; lo < R.total; lo += S1_CHUNK) {
+      const uint64_t hi = std::min<uint64_t>(R.total, lo + S1_CHUNK);
+      CK(c, s1_emit(c, R, lo, hi, dp));
+      CK(c, cudaMemsetAsync(c->d_counter.p, 0, sizeof(uint32_t), c->stream));
+      CasesArgs a = case_args(c, dp, (uint32_t)(hi - lo), -1);
+      a.rec = c->d_recs.as<ReqRec>();
+      a.multi = 1;
+      int bps = 0;
+      if (cases_occupancy(c->cases_variant, &bps, true) != cudaSuccess || bps <= 0) bps = 1;
+      CK(c, launch_cases(a, c->cases_variant, (uint32_t)(bps * c->sm_count), c->stream));
+    }
+    CK(c, cudaEventRecord(c->ev[1], c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    float x = 0;
+    CK(c, cudaEventElapsedTime(&x, c->ev[0], c->ev[1]));
+    ms += x;
+  }
+  std::vector<ReqRec> recs(n);
+  std::vector<uint64_t> hist(17ull * n);
+  unsigned long long nov = 0;
+  CK(c, cudaMemcpy(recs.data(), c->d_recs.p, rb, cudaMemcpyDeviceToHost));
+  CK(c, cudaMemcpy(hist.data(), c->s1_hist.p, hb, cudaMemcpyDeviceToHost));
+  CK(c, cudaMemcpy(&nov, c->d_ovcount.p, sizeof nov, cudaMemcpyDeviceToHost));
+  // overflow seeds (4 words: limbs 0..2, line), grouped by line, ascending
+  const uint64_t have = std::min<uint64_t>(nov, OVERFLOW_CAP);
+  std::vector<uint32_t> ov(4 * have);
+  if (have) CK(c, cudaMemcpy(ov.data(), c->d_overflow.p, 16 * have, cudaMemcpyDeviceToHost));
+  std::vector<std::pair<uint32_t, u128>> tagged(have);
+  for (uint64_t i = 0; i < have; i++)
+    tagged[i] = {ov[4 * i + 3], (u128)ov[4 * i] | ((u128)ov[4 * i + 1] << 32) | ((u128)ov[4 * i + 2] << 64)};
+  std::sort(tagged.begin(), tagged.end());
+  uint64_t total_seeds = 0;
+  for (uint32_t i = 0; i < n; i++) total_seeds += recs[i].seeds;
+  uint64_t used = 0, t = 0;
+  int status = COLLATZ_OK;
+  for (uint32_t i = 0; i < n; i++) {
+    collatz_case_result& o = out[i];
+    const ReqRec& r = recs[i];
+    leaf_counts_to_result(&hist[17ull * i], &o);
+    o.hash = r.hash;
+    o.seeds_checked = r.seeds;
+    o.n_overflow = r.items_done;
+    o.errors = r.errors;
+    if (r.valid & 2u) {
+      std::memcpy(o.max_excursion, r.E, sizeof o.max_excursion);
+      std::memcpy(o.max_excursion_seed, r.E_seed, sizeof o.max_excursion_seed);
+    }
+    if (r.valid & 1u) {
+      o.max_stopping_time = r.st;
+      std::memcpy(o.max_stopping_time_seed, r.st_seed, sizeof o.max_stopping_time_seed);
+    }
+    o.device_ms = total_seeds ? ms * (double)r.seeds / (double)total_seeds : 0.0;
+    const uint64_t first = t;
+    while (t < have && tagged[t].first == i) t++;
+    const uint64_t k = std::min<uint64_t>(t - first, pool_cap - used);
+    if (k) {
+      o.overflow_seeds = overflow_pool + 4 * used;
+      o.overflow_cap = k;
+      for (uint64_t j = 0; j < k; j++) limbs4(tagged[first + j].second, o.overflow_seeds + 4 * j);
+      used += k;
+    }
+    if (r.errors) status = COLLATZ_E_DEVICE;
+  }
+  if (status) c->err = "device error bits in a line of the batch";
+  return status;
 }
 
 extern "C" int collatz_step1_pairs_device(collatz_ctx* c, const collatz_case* cs, uint32_t* pairs, uint64_t cap,

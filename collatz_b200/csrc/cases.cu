@@ -13,6 +13,14 @@
 // XOR hash, the seed count and the overflow list are identical; the order
 // of work does not matter because every output is an XOR, a sum or a max.
 // Stopping time and maximum excursion are tracked on the side.
+//
+// Line batches (MULTI): the pairs of many cases_* lines in one launch.  Base
+// limb 3 of a pair holds bigindex | line << 8 and every line has its own
+// record.  A pair slot keeps its line and that line's prefilter thresholds;
+// a lane folds checkpoint XORs into a register for one line at a time and
+// flushes it to the line's record when it takes a seed of another line.
+// Warps claim pairs 16 at a time, so neighbouring pairs (mostly one line's)
+// stay on one warp.
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -24,20 +32,24 @@ namespace cz {
 constexpr u32 CQ = 1024;  // queue entries per warp (>= 31 + 570 survivors of one pair)
 constexpr u32 CR = 32;    // pair slots per warp (a queue of < 32 entries spans < 32 pairs)
 constexpr u32 CWARPS = 8;
+constexpr u32 MULTI_CLAIM = 16;  // pairs per claim in line batches
 
+template <bool MULTI>
 struct CasesWarp {
-  unsigned short q[CQ];   // (slot << 10) | a
-  u32 ring[CR][12];       // base0..2, number0..3, 3^f limbs 0..3, flags
-  u32 lane[32][8];        // per lane: [0] st, [1..3] seed, [4..7] seed-local max E
-  u32 thr[4];             // excursion threshold (lower bound of the running max)
+  unsigned short q[CQ];             // (slot << 10) | a
+  u32 ring[CR][MULTI ? 17 : 12];    // base0..2, number0..3, 3^f limbs 0..3, flags (bit 0 cpu, line << 1);
+                                    // MULTI: [12] st threshold, [13..16] excursion threshold of the line
+  u32 lane[32][MULTI ? 13 : 8];     // per lane: [0] st, [1..3] seed, [4..7] seed-local max E;
+                                    // MULTI: [8] st threshold, [9..12] excursion threshold of its line
+  u32 thr[4];                       // excursion threshold (lower bound of the running max)
 };
 
-template <int ITERS, int REFILL_MIN>
+template <int ITERS, int REFILL_MIN, bool MULTI>
 __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
-  __shared__ CasesWarp S[CWARPS];
+  __shared__ CasesWarp<MULTI> S[CWARPS];
   __shared__ u32 s_pow3[9];
   const u32 lane = lane_id();
-  CasesWarp& W = S[threadIdx.x >> 5];
+  CasesWarp<MULTI>& W = S[threadIdx.x >> 5];
   if (threadIdx.x < 9) {
     u32 p = 1;
     for (u32 i = 0; i < threadIdx.x; i++) p *= 3;
@@ -52,11 +64,14 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
   bool exhausted = false;
   u32 thr_st = 0, thr3 = 0, thr2 = 0;
   ull warp_seeds = 0;
+  u32 pc = 0, pc_end = 0;  // MULTI: claimed pairs [pc, pc_end)
   // lane state
   bool active = false;
   u32 v0 = 0, v1 = 0, v2 = 0, v3 = 0, n0 = 0, n1 = 0, n2 = 0;
   u32 st = 0, iters = 0, hash = 0;
   u32 found = 0, ovf = 0, cpu = 0, evalid = 0, pend = 0;
+  u32 hline = 0;      // MULTI: the line whose checkpoint XORs `hash` holds (and of the lane's seed)
+  u64 lthr_top = 0;   // MULTI: the lane's line's excursion threshold, bits 64..127
 
   for (;;) {
     // ---- offers of finished seeds, one lane at a time (bounded locks) ----
@@ -66,8 +81,9 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
         const u32 leader = __ffs(pm) - 1;
         if (lane == leader) {
           u32 seed[4] = {W.lane[lane][1], W.lane[lane][2], W.lane[lane][3], 0};
-          if (pend & 1u) rec_offer_st(A.rec, W.lane[lane][0], seed);
-          if (pend & 2u) rec_offer_e<4>(A.rec, &W.lane[lane][4], seed);
+          ReqRec* rec = MULTI ? A.rec + hline : A.rec;
+          if (pend & 1u) rec_offer_st(rec, W.lane[lane][0], seed);
+          if (pend & 2u) rec_offer_e<4>(rec, &W.lane[lane][4], seed);
           pend = 0;
         }
         pm &= pm - 1;
@@ -81,27 +97,27 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
     if (nidle >= (u32)REFILL_MIN || nidle == 32u) {
       while (qcount < nidle && !exhausted) {
         u32 p = 0;
-        if (lane == 0) p = atomicAdd(A.pair_counter, 1u);
-        p = __shfl_sync(FULL, p, 0);
+        if (MULTI) {
+          if (pc >= pc_end) {
+            // 16 pairs per claim while many remain; single pairs for the tail
+            const u32 claim =
+                ((unsigned long long)pc + (unsigned long long)MULTI_CLAIM * gridDim.x * CWARPS < A.npairs)
+                    ? MULTI_CLAIM
+                    : 1u;
+            u32 p0 = 0;
+            if (lane == 0) p0 = atomicAdd(A.pair_counter, claim);
+            p0 = __shfl_sync(FULL, p0, 0);
+            pc = p0;
+            pc_end = (p0 < A.npairs) ? min(A.npairs, p0 + claim) : p0;
+          }
+          p = pc++;
+        } else {
+          if (lane == 0) p = atomicAdd(A.pair_counter, 1u);
+          p = __shfl_sync(FULL, p, 0);
+        }
         if (p >= A.npairs) {
           exhausted = true;
           break;
-        }
-        // thresholds: refreshed once per pair
-        {
-          ull sk = 0, ek = 0;
-          if (lane == 0) {
-            sk = *(volatile ull*)&A.rec->st_key;
-            ek = *(volatile ull*)&A.rec->e_key;
-          }
-          sk = __shfl_sync(FULL, sk, 0);
-          ek = __shfl_sync(FULL, ek, 0);
-          thr_st = (u32)sk;
-          u32 t[4];
-          key_decode<4>(ek, t);
-          if (lane < 4) W.thr[lane] = t[lane];
-          thr3 = t[3];
-          thr2 = t[2];
         }
         // Step 2 (cu:198-235): sieve words for this pair
         const u32* P = A.pairs + 8ull * p;
@@ -109,7 +125,25 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
         const u32 b0 = __shfl_sync(FULL, pw, 0), b1 = __shfl_sync(FULL, pw, 1);
         const u32 b2 = __shfl_sync(FULL, pw, 2), b3 = __shfl_sync(FULL, pw, 3);
         const u32 m0 = __shfl_sync(FULL, pw, 4);
-        u32 bi = (A.bigindex >= 0) ? (u32)A.bigindex : b3;
+        const u32 pline = MULTI ? (b3 >> 8) : 0u;
+        ReqRec* prec = A.rec + pline;
+        // thresholds: refreshed once per pair
+        u32 t[4];
+        {
+          ull sk = 0, ek = 0;
+          if (lane == 0) {
+            sk = *(volatile ull*)&prec->st_key;
+            ek = *(volatile ull*)&prec->e_key;
+          }
+          sk = __shfl_sync(FULL, sk, 0);
+          ek = __shfl_sync(FULL, ek, 0);
+          thr_st = (u32)sk;
+          key_decode<4>(ek, t);
+          if (!MULTI && lane < 4) W.thr[lane] = t[lane];
+          thr3 = t[3];
+          thr2 = t[2];
+        }
+        u32 bi = (A.bigindex >= 0) ? (u32)A.bigindex : (MULTI ? (b3 & 0xFFu) : b3);
         u32 f = A.tpo + bi;
         if (f >= POW3_COUNT) f = POW3_COUNT - 1;
         const u32 red = ((b0 % 9u) + 4u * (b1 % 9u) + 7u * (b2 % 9u)) % 9u;  // 2^32 = 4, 2^64 = 7 (mod 9)
@@ -130,7 +164,12 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
           const u32 rv = __shfl_sync(FULL, pw, lane < 3 ? lane : lane + 1);  // base0..2, number0..3
           if (lane < 7) W.ring[slot][lane] = rv;
           if (lane >= 7 && lane < 11) W.ring[slot][lane] = A.pow3[4u * f + (lane - 7)];
-          if (lane == 11) W.ring[slot][11] = (bi >= 16u) ? 1u : 0u;
+          if (lane == 11) W.ring[slot][11] = ((bi >= 16u) ? 1u : 0u) | (pline << 1);
+          if (MULTI) {
+            if (lane == 12) W.ring[slot][12] = thr_st;
+            if (lane >= 13 && lane < 17) W.ring[slot][lane] = t[lane - 13];
+            if (lane == 0) atomicAdd(&prec->seeds, (ull)total);
+          }
           u32 pos = qhead + qcount + excl;
           while (word) {
             const u32 j = ctz32(word);
@@ -175,7 +214,21 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
           t = (u64)a * R[9] + R[5] + (t >> 32);
           v2 = (u32)t;
           v3 = a * R[10] + R[6] + (u32)(t >> 32);
-          cpu = R[11];
+          cpu = R[11] & 1u;
+          if (MULTI) {
+            const u32 line = R[11] >> 1;
+            if (line != hline) {  // this lane's XORs so far belong to the previous line
+              if (hash) atomicXor(&A.rec[hline].hash, hash);
+              hash = 0;
+              hline = line;
+            }
+            W.lane[lane][8] = R[12];
+            W.lane[lane][9] = R[13];
+            W.lane[lane][10] = R[14];
+            W.lane[lane][11] = R[15];
+            W.lane[lane][12] = R[16];
+            lthr_top = ((u64)R[16] << 32) | R[15];
+          }
           st = mbi;
           iters = 0;
           found = 0;
@@ -183,13 +236,14 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
           evalid = 0;
           if (n2 == 0 && n1 == 0 && n0 < 3u) {
             // v < n can never hold: the reference would loop forever
-            atomicOr(&A.rec->errors, ERR_SEED_SMALL);
+            atomicOr(&(MULTI ? A.rec + hline : A.rec)->errors, ERR_SEED_SMALL);
           } else {
             active = true;
             // E candidate T^(N-A)(n) = v - 1
             const u32 x0 = v0 - 1, x1 = v1 - (v0 == 0), x2 = v2 - ((v0 | v1) == 0), x3 = v3 - ((v0 | v1 | v2) == 0);
-            const bool ge = !lt96(x1, x2, x3, W.thr[1], W.thr[2], W.thr[3]) &&
-                            !((x3 == W.thr[3]) & (x2 == W.thr[2]) & (x1 == W.thr[1]) & (x0 < W.thr[0]));
+            const u32* th = MULTI ? &W.lane[lane][9] : W.thr;
+            const bool ge = !lt96(x1, x2, x3, th[1], th[2], th[3]) &&
+                            !((x3 == th[3]) & (x2 == th[2]) & (x1 == th[1]) & (x0 < th[0]));
             if (ge) {
               W.lane[lane][4] = x0;
               W.lane[lane][5] = x1;
@@ -207,7 +261,7 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
 
     // ---- Step 3 (cu:280-405) ----
     if (active) {
-      const u64 thr_top = ((u64)thr3 << 32) | thr2;
+      const u64 thr_top = MULTI ? lthr_top : (((u64)thr3 << 32) | thr2);
 #pragma unroll 1
       for (int it = 0; it < ITERS; it++) {
 #pragma unroll
@@ -224,8 +278,9 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
                 A.overflow[4 * i + 0] = n0;
                 A.overflow[4 * i + 1] = n1;
                 A.overflow[4 * i + 2] = n2;
-                A.overflow[4 * i + 3] = 0;
+                A.overflow[4 * i + 3] = MULTI ? hline : 0u;
               }
+              if (MULTI) atomicAdd(&A.rec[hline].items_done, 1ull);  // the line's overflow reports
               ovf = 1;
               v0 = 2;
               v1 = v2 = v3 = 0;
@@ -234,7 +289,7 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
           if (!found && !ovf && (((u64)v3 << 32) | v2) >= thr_top) {
             // rare: exact excursion candidate x = v - 1 against the seed max / threshold
             const u32 x0 = v0 - 1, x1 = v1 - (v0 == 0), x2 = v2 - ((v0 | v1) == 0), x3 = v3 - ((v0 | v1 | v2) == 0);
-            const u32* ref = evalid ? &W.lane[lane][4] : W.thr;
+            const u32* ref = evalid ? &W.lane[lane][4] : (MULTI ? &W.lane[lane][9] : W.thr);
             const bool ge = !lt96(x1, x2, x3, ref[1], ref[2], ref[3]) &&
                             !((x3 == ref[3]) & (x2 == ref[2]) & (x1 == ref[1]) & (x0 < ref[0]));
             if (ge) {
@@ -282,13 +337,14 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
         const bool done = (v3 == 0) && lt96(v0, v1, v2, n0, n1, n2);  // cu:362-365
         if (done || iters >= A.iter_cap) {
           if (!done) {
-            atomicOr(&A.rec->errors, ERR_ITER_CAP);
-            atomicAdd(&A.rec->failures, 1ull);
+            ReqRec* rec = MULTI ? A.rec + hline : A.rec;
+            atomicOr(&rec->errors, ERR_ITER_CAP);
+            atomicAdd(&rec->failures, 1ull);
           } else if (!ovf) {
             W.lane[lane][1] = n0;
             W.lane[lane][2] = n1;
             W.lane[lane][3] = n2;
-            if (st >= thr_st) {
+            if (st >= (MULTI ? W.lane[lane][8] : thr_st)) {
               W.lane[lane][0] = st;
               pend |= 1u;
             }
@@ -302,11 +358,15 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
   }
 
   // ---- warp totals ----
+  if (MULTI) {
+    if (hash) atomicXor(&A.rec[hline].hash, hash);
+  } else {
 #pragma unroll
-  for (u32 d = 16; d; d >>= 1) hash ^= __shfl_xor_sync(FULL, hash, d);
-  if (lane == 0) {
-    atomicXor(&A.rec->hash, hash);
-    atomicAdd(&A.rec->seeds, warp_seeds);
+    for (u32 d = 16; d; d >>= 1) hash ^= __shfl_xor_sync(FULL, hash, d);
+    if (lane == 0) {
+      atomicXor(&A.rec->hash, hash);
+      atomicAdd(&A.rec->seeds, warp_seeds);
+    }
   }
 }
 
@@ -316,7 +376,8 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
 
 template <int I, int R>
 static cudaError_t launch_cases_t(const CasesArgs& a, u32 grid, cudaStream_t st) {
-  k_cases<I, R><<<grid, CWARPS * 32, 0, st>>>(a);
+  if (a.multi) k_cases<I, R, true><<<grid, CWARPS * 32, 0, st>>>(a);
+  else k_cases<I, R, false><<<grid, CWARPS * 32, 0, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -331,13 +392,18 @@ cudaError_t launch_cases(const CasesArgs& a, int variant, u32 grid, cudaStream_t
   }
 }
 
-cudaError_t cases_occupancy(int variant, int* blocks_per_sm) {
+template <bool M>
+static cudaError_t occupancy_t(int variant, int* bps) {
   switch (variant) {
-    case 0: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_cases<1, 1>, CWARPS * 32, 0);
-    case 1: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_cases<2, 4>, CWARPS * 32, 0);
-    case 2: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_cases<2, 8>, CWARPS * 32, 0);
-    default: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_cases<4, 8>, CWARPS * 32, 0);
+    case 0: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_cases<1, 1, M>, CWARPS * 32, 0);
+    case 1: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_cases<2, 4, M>, CWARPS * 32, 0);
+    case 2: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_cases<2, 8, M>, CWARPS * 32, 0);
+    default: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_cases<4, 8, M>, CWARPS * 32, 0);
   }
+}
+
+cudaError_t cases_occupancy(int variant, int* blocks_per_sm, bool multi) {
+  return multi ? occupancy_t<true>(variant, blocks_per_sm) : occupancy_t<false>(variant, blocks_per_sm);
 }
 
 }  // namespace cz

@@ -6,10 +6,14 @@
 // of a cases_* file (one Step-1 subtree root each) and combining the
 // per-line outputs: the complete hash of the whole tree is the XOR of the
 // lines' hashes (every checkpoint XOR lands in exactly one subtree), counts
-// add up, and the overflow lists concatenate.  Here the lines run in order
-// on one context; each finished line is appended to a text journal and
-// synced to disk before the next starts, so a run that stops (a crash, a
-// preempted job) resumes from the journal without repeating finished lines.
+// add up, and the overflow lists concatenate.  Here the lines run on one
+// context in groups of up to 8192, each group as one device pass
+// (collatz_run_case_batch: Step 1 from all the group's roots at once, one
+// record per line), so the thousands of small lines of a cases_big file do
+// not each pay a pass's fixed cost.  The group's lines are appended to a
+// text journal and synced to disk before the next group starts, so a run
+// that stops (a crash, a preempted job) resumes from the journal without
+// repeating finished lines.
 //
 // Journal line (one per finished case, whitespace-separated):
 //   case <index> <base lo> <base hi> <sigfig> <threepower> <number lo>
@@ -32,7 +36,8 @@
 
 namespace {
 
-constexpr uint64_t OV_CAP = 1u << 16;  // overflow seeds kept per case
+constexpr uint64_t OV_CAP = 1u << 16;  // overflow seeds kept per case (and per group)
+constexpr uint32_t GROUP = 8192;        // lines per device pass
 
 bool less4(const uint32_t* a, const uint32_t* b) {
   for (int i = 3; i >= 0; i--)
@@ -206,24 +211,34 @@ extern "C" int collatz_run_cases(collatz_ctx* ctx, const collatz_case* cases, ui
   int rc = load(journal, cases, n, res, ovs, done);
   if (rc) return rc;
   uint32_t ran = 0;
-  std::vector<uint32_t> buf(4 * OV_CAP);
-  for (uint32_t i = 0; i < n; i++) {
-    if (done[i]) continue;
-    collatz_case_result r;
-    std::memset(&r, 0, sizeof r);
-    r.overflow_seeds = buf.data();
-    r.overflow_cap = OV_CAP;
-    rc = collatz_run_case(ctx, &cases[i], &r);
-    if (rc && rc != COLLATZ_E_DEVICE) return rc;  // a device error bit is recorded in r.errors
-    const uint64_t nov = std::min(r.n_overflow, OV_CAP);
-    ovs[i].assign(buf.begin(), buf.begin() + 4 * nov);
+  std::vector<uint32_t> todo;
+  for (uint32_t i = 0; i < n; i++)
+    if (!done[i]) todo.push_back(i);
+  std::vector<uint32_t> pool(4 * OV_CAP);
+  std::vector<collatz_case> gc;
+  std::vector<collatz_case_result> gr;
+  for (size_t g0 = 0; g0 < todo.size(); g0 += GROUP) {
+    const uint32_t m = (uint32_t)std::min<size_t>(GROUP, todo.size() - g0);
+    gc.resize(m);
+    gr.resize(m);
+    for (uint32_t j = 0; j < m; j++) gc[j] = cases[todo[g0 + j]];
+    rc = collatz_run_case_batch(ctx, gc.data(), m, gr.data(), pool.data(), OV_CAP);
+    if (rc && rc != COLLATZ_E_DEVICE) return rc;  // a device error bit is recorded in the line's errors
+    std::string text;
+    for (uint32_t j = 0; j < m; j++) {
+      const uint32_t i = todo[g0 + j];
+      const collatz_case_result& r = gr[j];
+      const uint64_t nov = r.overflow_seeds ? r.overflow_cap : 0;
+      ovs[i].assign(r.overflow_seeds, r.overflow_seeds + 4 * nov);
+      if (journal && *journal) text += journal_line(i, cases[i], r, ovs[i].data(), nov);
+      res[i] = r;
+      done[i] = 1;
+      ran++;
+    }
     if (journal && *journal) {
-      const int wrc = append(journal, journal_line(i, cases[i], r, buf.data(), nov));
+      const int wrc = append(journal, text);
       if (wrc) return wrc;
     }
-    res[i] = r;
-    done[i] = 1;
-    ran++;
   }
   for (uint32_t i = 0; i < n; i++) {
     res[i].overflow_seeds = ovs[i].empty() ? nullptr : ovs[i].data();

@@ -24,14 +24,16 @@ struct CasesArgs {
   uint32_t overflow_cap;
   unsigned long long* overflow_count;
   uint32_t iter_cap;       // checkpoints per seed before ERR_ITER_CAP
+  uint32_t multi;          // line batch: base limb 3 = bigindex | line << 8, rec[line] per line
 };
 int cases_variants();
 cudaError_t launch_cases(const CasesArgs& a, int variant, uint32_t grid, cudaStream_t st);
-cudaError_t cases_occupancy(int variant, int* blocks_per_sm);
+cudaError_t cases_occupancy(int variant, int* blocks_per_sm, bool multi = false);
 
 // ---------------- device Step 1 (step1_dev.cu) ----------------
 // A node of search1's tree (cu:497-505): base and number as little-endian
-// 64-bit halves; sigfig, threepower, doubleeven, numevens.
+// 64-bit halves; sigfig | line << 8 (line: the node's cases line in a line
+// batch), threepower, doubleeven, numevens.
 struct S1Node {
   unsigned long long base_lo, base_hi, num_lo, num_hi;
   uint32_t sig, tp, de, ne;
@@ -56,6 +58,7 @@ struct Step1Args {
   unsigned long long* cnt;   // walk: per frontier node, leaves
   unsigned long long* total;
   unsigned long long* hist;
+  unsigned long long* hist_lines;  // line batches: leaves per (line, bigindex), 17 per line; else null
   uint32_t* cursor;          // walk: zero before the launch
   ulonglong2* stk_num;       // walk: pending siblings, [level][thread]
   uint4* stk_meta;

@@ -109,6 +109,7 @@ extern "C" int collatz_verify_pairs_noalloc(collatz_ctx* c, uint32_t bigindex, c
     a.overflow_cap = NOALLOC_OVERFLOW_MAX;
     a.overflow_count = d_ovcount;
     a.iter_cap = c->iter_cap;
+    a.multi = 0;
     int bps = 0;
     if (cases_occupancy(c->cases_variant, &bps) != cudaSuccess || bps <= 0) bps = 1;
     NA_CK(c, cudaEventRecord(c->ev[0], c->stream));

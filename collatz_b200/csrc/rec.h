@@ -21,7 +21,7 @@ struct ReqRec {
   unsigned long long e_key;       // monotone key of the running max excursion (prefilter)
   unsigned long long failures;    // seeds that did not finish (beyond widest limbs / iteration cap)
   unsigned long long widened;     // seeds re-run with wider limbs
-  unsigned long long items_done;  // work items completed (serving progress)
+  unsigned long long items_done;  // work items completed (serving progress); cases line batches: overflow reports
   uint32_t lock;                  // guards the exact maxima below
   uint32_t valid;                 // bit0: st fields set, bit1: E fields set
   uint32_t hash;                  // cases mode: XOR of all checkpoint low limbs (cu:359, 407-409)

@@ -92,7 +92,7 @@ struct collatz_ctx {
   cz::DevBuf t_seeds, t_st, t_exc, t_status, t_idx[2], t_cnt;
   // device Step 1: frontier (ping-pong), per-node leaf offsets and counts,
   // counters, pending-sibling stack
-  cz::DevBuf s1_front[2], s1_off, s1_cnt, s1_scal, s1_stk_num, s1_stk_meta;
+  cz::DevBuf s1_front[2], s1_off, s1_cnt, s1_scal, s1_stk_num, s1_stk_meta, s1_hist;
   cz::HostBuf h_s1;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   std::recursive_mutex mu;

@@ -20,6 +20,12 @@
 // Each lane keeps at most one pending sibling per tree level (the right
 // child, base | 1 << sigfig): its state lives in a global stack laid out
 // [level][thread], and its base is rebuilt from the current path on pop.
+//
+// Line batches: the roots may be many cases_* lines at different sigfigs.
+// A node's sigfig word is sigfig | line << 8; a leaf reached before the last
+// breadth-first level passes through the later levels unchanged; the count
+// pass counts leaves per (line, bigindex); a pair carries bigindex | line << 8
+// in base limb 3.
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -96,29 +102,32 @@ __device__ __forceinline__ void init_pow3(u128d* p3) {
   }
 }
 
+// sig: sigfig (< 256); line: the node's line in a line batch (0 otherwise).
 __device__ __forceinline__ void load_node(const S1Node* p, u128d& base, u128d& num, uint32_t& sig, uint32_t& tp,
-                                          uint32_t& de, uint32_t& ne) {
+                                          uint32_t& de, uint32_t& ne, uint32_t& line) {
   const uint4* q = reinterpret_cast<const uint4*>(p);
   const uint4 x = q[0], y = q[1], z = q[2];
   base = mk(((unsigned long long)x.y << 32) | x.x, ((unsigned long long)x.w << 32) | x.z);
   num = mk(((unsigned long long)y.y << 32) | y.x, ((unsigned long long)y.w << 32) | y.z);
-  sig = z.x;
+  sig = z.x & 0xFFu;
+  line = z.x >> 8;
   tp = z.y;
   de = z.z;
   ne = z.w;
 }
 
-__device__ __forceinline__ void store_node(S1Node* p, u128d base, const Kid& k, uint32_t sig) {
+__device__ __forceinline__ void store_node(S1Node* p, u128d base, u128d num, uint32_t sig, uint32_t tp, uint32_t de,
+                                           uint32_t ne, uint32_t line) {
   uint4* q = reinterpret_cast<uint4*>(p);
   q[0] = make_uint4((uint32_t)base, (uint32_t)(base >> 32), (uint32_t)(base >> 64), (uint32_t)(base >> 96));
-  q[1] = make_uint4((uint32_t)k.num, (uint32_t)(k.num >> 32), (uint32_t)(k.num >> 64), (uint32_t)(k.num >> 96));
-  q[2] = make_uint4(sig, k.tp, k.de, k.ne);
+  q[1] = make_uint4((uint32_t)num, (uint32_t)(num >> 32), (uint32_t)(num >> 64), (uint32_t)(num >> 96));
+  q[2] = make_uint4(sig | (line << 8), tp, de, ne);
 }
 
 }  // namespace
 
 // One breadth-first level: frontier (in, *in_count) -> children (out,
-// *out_count).  Every input node is an inner node (sigfig < N-A).
+// *out_count).  A leaf (sigfig == N-A) is copied through unchanged.
 __global__ void __launch_bounds__(256) k_step1_expand(const Step1Args A) {
   __shared__ u128d p3[128];
   const uint32_t n = *A.in_count;
@@ -130,12 +139,22 @@ __global__ void __launch_bounds__(256) k_step1_expand(const Step1Args A) {
   Kid a, b;
   a.ok = b.ok = false;
   u128d base = 0;
-  uint32_t sig = 0;
+  uint32_t sig = 0, line = 0;
+  bool leaf = false;
   if (i < n) {
     u128d num;
     uint32_t tp, de, ne;
-    load_node(A.in + i, base, num, sig, tp, de, ne);
-    s1_children(num, sig, tp, de, ne, p3, a, b);
+    load_node(A.in + i, base, num, sig, tp, de, ne, line);
+    if (sig == A.mbi) {  // pass the leaf through as the first "child"
+      leaf = true;
+      a.num = num;
+      a.tp = tp;
+      a.de = de;
+      a.ne = ne;
+      a.ok = true;
+    } else {
+      s1_children(num, sig, tp, de, ne, p3, a, b);
+    }
   }
   const uint32_t k = (uint32_t)a.ok + (uint32_t)b.ok;
   uint32_t incl = k;
@@ -148,8 +167,8 @@ __global__ void __launch_bounds__(256) k_step1_expand(const Step1Args A) {
   if (lane == 31u && incl) wbase = atomicAdd(A.out_count, incl);
   wbase = __shfl_sync(FULL, wbase, 31);
   uint32_t o = wbase + incl - k;
-  if (a.ok) store_node(A.out + o++, base, a, sig + 1u);
-  if (b.ok) store_node(A.out + o, base | ((u128d)1 << sig), b, sig + 1u);
+  if (a.ok) store_node(A.out + o++, base, a.num, leaf ? sig : sig + 1u, a.tp, a.de, a.ne, line);
+  if (b.ok) store_node(A.out + o, base | ((u128d)1 << sig), b.num, sig + 1u, b.tp, b.de, b.ne, line);
 }
 
 // Depth-first walk below the frontier; see the file comment.
@@ -178,8 +197,8 @@ __global__ void __launch_bounds__(128) k_step1_walk(const Step1Args A) {
     }
     if (go) {
       u128d base, num;
-      uint32_t sig, tp, de, ne;
-      load_node(A.in + i, base, num, sig, tp, de, ne);
+      uint32_t sig, tp, de, ne, line;
+      load_node(A.in + i, base, num, sig, tp, de, ne, line);
       const uint32_t s0 = sig;
       unsigned long long pend_lo = 0, pend_hi = 0;  // bit l: a pending node at sigfig s0 + 1 + l
       for (;;) {
@@ -190,10 +209,12 @@ __global__ void __launch_bounds__(128) k_step1_walk(const Step1Args A) {
             const unsigned long long idx = off + cnt;
             if (idx >= A.w_lo) {
               uint4* q = reinterpret_cast<uint4*>(A.pairs + 8ull * (idx - A.w_lo));
-              q[0] = make_uint4((uint32_t)base, (uint32_t)(base >> 32), (uint32_t)(base >> 64), bi);
+              q[0] = make_uint4((uint32_t)base, (uint32_t)(base >> 32), (uint32_t)(base >> 64), bi | (line << 8));
               q[1] = make_uint4((uint32_t)num, (uint32_t)(num >> 32), (uint32_t)(num >> 64),
                                 (uint32_t)(num >> 96));
             }
+          } else if (A.hist_lines) {
+            atomicAdd(&A.hist_lines[17ull * line + (bi < 16u ? bi : 16u)], 1ull);
           } else {
             atomicAdd(&hist[bi < 16u ? bi : 16u], 1ull);
           }

@@ -119,6 +119,21 @@ typedef struct {
  * the same result. */
 int collatz_run_case(collatz_ctx *ctx, const collatz_case *c, collatz_case_result *out);
 
+/* No counterpart in the reference.  Runs cases[0..n) together, as one
+ * device pass: Step 1 from all n roots at once, then Steps 2-3 with a
+ * record per case (n <= COLLATZ_CASE_BATCH_MAX).  For a file of many small
+ * lines (cases_big) this replaces n calls of collatz_run_case, whose fixed
+ * cost per call would dominate.  out[i] receives what collatz_run_case gives
+ * for cases[i]: hash, launches, seeds, pairs, maxima, errors, n_overflow;
+ * device_ms is the pass's device time split by seeds.  Overflow seeds go to
+ * one pool (4 uint32 per seed, pool_cap seeds), grouped by case, ascending
+ * within a case: out[i].overflow_seeds / overflow_cap are set to case i's
+ * part of the pool (NULL / 0 when it has none or the pool is full).  At most
+ * 65536 overflow seeds are kept per call; n_overflow counts all of them. */
+#define COLLATZ_CASE_BATCH_MAX (1u << 20)
+int collatz_run_case_batch(collatz_ctx *ctx, const collatz_case *cases, uint32_t n, collatz_case_result *out,
+                           uint32_t *overflow_pool, uint64_t pool_cap);
+
 /* One batch of Step-1 pairs of one bucket (replaces launchkernel,
  * cu:565-649, and compute_kernel, cu:185-411).  pairs: npairs x 8 uint32
  * (base limbs 0..3, number limbs 0..3; base limb 3 is ignored as in
@@ -153,6 +168,15 @@ int collatz_verify_pairs_noalloc(collatz_ctx *ctx, uint32_t bigindex, const uint
 int collatz_step1_pairs(uint32_t maxbits, const collatz_case *c, uint32_t *pairs, uint64_t cap,
                         uint64_t *count);
 
+/* No counterpart in the reference (its cases_* files are cut this way).
+ * The nodes of a case's Step-1 tree at sigfig = cut, c->sigfig <= cut <=
+ * N - A, i.e. the roots of search1's subtrees there (cu:497-563), in the
+ * reference's visiting order, as 6-tuples: run as cases, the XOR of their
+ * hashes and the sums of their counts equal the whole case's.  *count
+ * receives the number of nodes; cases are written up to cap.  Host-only. */
+int collatz_step1_split(uint32_t maxbits, const collatz_case *c, uint32_t cut, collatz_case *out, uint64_t cap,
+                        uint64_t *count);
+
 /* No counterpart in the reference.  The Step-1 leaves of a case computed by
  * the device Step 1 of collatz_run_case, for the context's N, in no
  * particular order (the same multiset as collatz_step1_pairs).  *count
@@ -171,12 +195,13 @@ int collatz_step1_pairs_device(collatz_ctx *ctx, const collatz_case *c, uint32_t
  * Host-only. */
 int collatz_combine_case_results(const collatz_case_result *parts, uint32_t n, collatz_case_result *out);
 
-/* Runs cases[0..n) in order on one context and combines them into
- * *combined.  With a journal path, each finished case is appended to the
- * journal as one text line, flushed and synced before the next case starts;
- * a later call with the same cases and journal takes the finished cases from
- * the journal and runs only the rest, so an interrupted run resumes where it
- * stopped.  A journal line whose tuple differs from the case at its index is
+/* Runs cases[0..n) on one context, in groups of up to 8192 cases per
+ * device pass (collatz_run_case_batch), and combines them into *combined.
+ * With a journal path, each finished case is appended to the journal as one
+ * text line; a group's lines are flushed and synced before the next group
+ * starts.  A later call with the same cases and journal takes the finished
+ * cases from the journal and runs only the rest, so an interrupted run
+ * resumes where it stopped.  A journal line whose tuple differs from the case at its index is
  * rejected (COLLATZ_E_STATE).  per_case (NULL or n entries) receives each
  * case's result without overflow seeds.  *n_run (may be NULL) = cases run by
  * this call. */

@@ -273,3 +273,24 @@ def test_trajectory_bruteforce():
             assert (status, st, E) == (1, 0, s)
         else:
             assert (status, st, E) == (0, *brute(s))
+
+
+def test_split_matches_oracle():
+    """collatz_step1_split (the product's cut of a case into cases_* lines)
+    gives the oracle's nodes in the oracle's order, edge tuples included."""
+    import collatz_b200 as cb
+    from oracle import oracle as O
+    for n, tup, cut in ((36, (3, 2, 2, 9, 1, 0), 12), (36, (3, 2, 2, 9, 1, 0), 20), (45, (27, 10, 8, 183, 0, 0), 23),
+                        (30, (3, 2, 2, 9, 0, 7), 19), (26, (0, 5, 0, 1, 0, 0), 10), (26, (3, 15, 11, 9, 0, 0), 15),
+                        (26, (3, 2, 2, 9, 1, 0), 2)):
+        assert [cb.case_tuple(c) for c in cb.split_cases(n, tup, cut)] == O.split_case(n, tup, cut), (n, tup, cut)
+    # at cut = N - A the nodes are the leaves (the oracle's split stops above them)
+    nodes = [cb.case_tuple(c) for c in cb.split_cases(30, (3, 2, 2, 9, 1, 0), 20)]
+    assert [(b, num) for b, _, _, num, _, _ in nodes] == [(b, num) for _, b, num in O.leaves(30, (3, 2, 2, 9, 1, 0))]
+
+
+def test_split_rejects_bad_cut():
+    import collatz_b200 as cb
+    for n, tup, cut in ((26, (3, 2, 2, 9, 1, 0), 1), (26, (3, 2, 2, 9, 1, 0), 17), (15, (3, 2, 2, 9, 1, 0), 4)):
+        with pytest.raises(cb.CollatzError):
+            cb.split_cases(n, tup, cut)
