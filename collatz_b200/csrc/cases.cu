@@ -69,6 +69,7 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
   bool active = false;
   u32 v0 = 0, v1 = 0, v2 = 0, v3 = 0, n0 = 0, n1 = 0, n2 = 0;
   u32 st = 0, iters = 0, hash = 0;
+  u32 nbl = 0;  // bit length of the seed n
   u32 found = 0, ovf = 0, cpu = 0, evalid = 0, pend = 0;
   u32 hline = 0;      // MULTI: the line whose checkpoint XORs `hash` holds (and of the lane's seed)
   u64 lthr_top = 0;   // MULTI: the lane's line's excursion threshold, bits 64..127
@@ -229,6 +230,7 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
             W.lane[lane][12] = R[16];
             lthr_top = ((u64)R[16] << 32) | R[15];
           }
+          nbl = bitlen96(n0, n1, n2);
           st = mbi;
           iters = 0;
           found = 0;
@@ -239,17 +241,20 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
             atomicOr(&(MULTI ? A.rec + hline : A.rec)->errors, ERR_SEED_SMALL);
           } else {
             active = true;
-            // E candidate T^(N-A)(n) = v - 1
-            const u32 x0 = v0 - 1, x1 = v1 - (v0 == 0), x2 = v2 - ((v0 | v1) == 0), x3 = v3 - ((v0 | v1 | v2) == 0);
-            const u32* th = MULTI ? &W.lane[lane][9] : W.thr;
-            const bool ge = !lt96(x1, x2, x3, th[1], th[2], th[3]) &&
-                            !((x3 == th[3]) & (x2 == th[2]) & (x1 == th[1]) & (x0 < th[0]));
-            if (ge) {
-              W.lane[lane][4] = x0;
-              W.lane[lane][5] = x1;
-              W.lane[lane][6] = x2;
-              W.lane[lane][7] = x3;
-              evalid = 1;
+            // E candidate T^(N-A)(n) = v - 1; (v3:v2) below the threshold's top limbs rejects it at once
+            if ((((u64)v3 << 32) | v2) >= (MULTI ? lthr_top : (((u64)thr3 << 32) | thr2))) {
+              const u32 x0 = v0 - 1, x1 = v1 - (v0 == 0), x2 = v2 - ((v0 | v1) == 0),
+                        x3 = v3 - ((v0 | v1 | v2) == 0);
+              const u32* th = MULTI ? &W.lane[lane][9] : W.thr;
+              const bool ge = !lt96(x1, x2, x3, th[1], th[2], th[3]) &&
+                              !((x3 == th[3]) & (x2 == th[2]) & (x1 == th[1]) & (x0 < th[0]));
+              if (ge) {
+                W.lane[lane][4] = x0;
+                W.lane[lane][5] = x1;
+                W.lane[lane][6] = x2;
+                W.lane[lane][7] = x3;
+                evalid = 1;
+              }
             }
           }
         }
@@ -308,13 +313,7 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
           if (!found && !ovf) {
             if (b != 0 && w3 == 0 && w2 <= n2 && lt96(w0, w1, w2, n0, n1, n2)) {
               // first descent inside this run: smallest i with (v-1) >> i < n
-              u32 i = 1;
-              for (; i < b; i++) {
-                const u32 y0 = __funnelshift_r(v0, v1, i), y1 = __funnelshift_r(v1, v2, i);
-                const u32 y2 = __funnelshift_r(v2, v3, i), y3 = v3 >> i;
-                if (y3 == 0 && lt96(y0, y1, y2, n0, n1, n2)) break;
-              }
-              st += i;
+              st += first_below(v0, v1, v2, v3, n0, n1, n2, nbl);
               found = 1;
             } else {
               st += b;
@@ -341,14 +340,16 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
             atomicOr(&rec->errors, ERR_ITER_CAP);
             atomicAdd(&rec->failures, 1ull);
           } else if (!ovf) {
-            W.lane[lane][1] = n0;
-            W.lane[lane][2] = n1;
-            W.lane[lane][3] = n2;
             if (st >= (MULTI ? W.lane[lane][8] : thr_st)) {
               W.lane[lane][0] = st;
               pend |= 1u;
             }
             if (evalid) pend |= 2u;
+            if (pend) {  // the seed, for the offer
+              W.lane[lane][1] = n0;
+              W.lane[lane][2] = n1;
+              W.lane[lane][3] = n2;
+            }
           }
           active = false;
           break;

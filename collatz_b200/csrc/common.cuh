@@ -49,6 +49,24 @@ __device__ __forceinline__ bool lt96(u32 a0, u32 a1, u32 a2, u32 b0, u32 b1, u32
   return (a2 < b2) | ((a2 == b2) & ((a1 < b1) | ((a1 == b1) & (a0 < b0))));
 }
 
+// Bit length of a 96-bit value.
+__device__ __forceinline__ u32 bitlen96(u32 n0, u32 n1, u32 n2) {
+  return n2 ? 96u - __clz(n2) : (n1 ? 64u - __clz(n1) : 32u - __clz(n0));
+}
+
+// Least i >= 1 with (x >> i) < n, for x = (x3:x2:x1:x0) and a 96-bit n of bit
+// length bln, given that x >> b < n for some b <= 31.  With d = bitlen(x) -
+// bln: x >> i has more bits than n for i < d, fewer for i = d + 1, so the
+// answer is d or d + 1 (1 when d < 1).  Constant time, no loop over i.
+__device__ __forceinline__ u32 first_below(u32 x0, u32 x1, u32 x2, u32 x3, u32 n0, u32 n1, u32 n2, u32 bln) {
+  const u32 bx = x3 ? 128u - __clz(x3) : (x2 ? 96u - __clz(x2) : (x1 ? 64u - __clz(x1) : 32u - __clz(x0)));
+  const int d = (int)bx - (int)bln;
+  if (d < 1) return 1u;
+  const u32 y0 = __funnelshift_r(x0, x1, d), y1 = __funnelshift_r(x1, x2, d);
+  const u32 y2 = __funnelshift_r(x2, x3, d), y3 = x3 >> d;
+  return ((y3 == 0) & lt96(y0, y1, y2, n0, n1, n2)) ? (u32)d : (u32)d + 1u;
+}
+
 // Odd run on 4 limbs: v <- (v >> a) * m with m = 3^a, a <= 8
 // (collatz_cudav7.cu:282-293).  The product is taken mod 2^128.
 __device__ __forceinline__ void odd_run4(u32& v0, u32& v1, u32& v2, u32& v3, u32 a, u32 m) {
