@@ -865,21 +865,23 @@ static bool s1_root_pass(const collatz_case& cs) {
   return true;
 }
 
-extern "C" int collatz_run_case_batch(collatz_ctx* c, const collatz_case* cases, uint32_t n,
-                                      collatz_case_result* out, uint32_t* overflow_pool, uint64_t pool_cap) {
-  if (!c || !n || !cases || !out || (pool_cap && !overflow_pool)) return COLLATZ_E_ARG;
-  if (n > COLLATZ_CASE_BATCH_MAX) return COLLATZ_E_LIMIT;
-  for (uint32_t i = 0; i < n; i++)
-    if (cases[i].sigfig > c->ct.mbi || cases[i].threepower >= 128) return COLLATZ_E_ARG;
-  std::lock_guard<std::recursive_mutex> g(c->mu);
-  std::memset(out, 0, sizeof(collatz_case_result) * n);
-  CK(c, cudaSetDevice(c->device));
+// Lines at least this many levels above the leaves (N-A - sigfig) run alone
+// through the single-case path (host cut, one record): each has >= ~10^7
+// seeds, enough to fill the GPU by itself, and the per-line records of a
+// batch would only add work.  Shallower lines share batched passes.
+constexpr uint32_t BATCH_ALONE_DEPTH = 20;
+
+// One device pass over the lines cases[idx[0..m)] (line j of the pass is
+// cases[idx[j]]); results go to out[idx[j]], overflow seeds to pool[used..).
+static int batch_pass(collatz_ctx* c, const collatz_case* cases, const std::vector<uint32_t>& idx,
+                      collatz_case_result* out, uint32_t* overflow_pool, uint64_t pool_cap, uint64_t& used) {
+  const uint32_t n = (uint32_t)idx.size();
   int rc = case_prepare(c);
   if (rc) return rc;
   std::vector<S1Node> roots;
   uint32_t min_sig = 0xFFFFFFFFu;
   for (uint32_t i = 0; i < n; i++) {
-    const collatz_case& cs = cases[i];
+    const collatz_case& cs = cases[idx[i]];
     if (!s1_root_pass(cs)) continue;  // search1 returns at once: no leaves
     roots.push_back(S1Node{cs.base[0], cs.base[1], cs.number[0], cs.number[1], cs.sigfig | (i << 8), cs.threepower,
                            cs.doubleeven, cs.numevens});
@@ -931,10 +933,10 @@ extern "C" int collatz_run_case_batch(collatz_ctx* c, const collatz_case* cases,
   std::sort(tagged.begin(), tagged.end());
   uint64_t total_seeds = 0;
   for (uint32_t i = 0; i < n; i++) total_seeds += recs[i].seeds;
-  uint64_t used = 0, t = 0;
+  uint64_t t = 0;
   int status = COLLATZ_OK;
   for (uint32_t i = 0; i < n; i++) {
-    collatz_case_result& o = out[i];
+    collatz_case_result& o = out[idx[i]];
     const ReqRec& r = recs[i];
     leaf_counts_to_result(&hist[17ull * i], &o);
     o.hash = r.hash;
@@ -960,6 +962,53 @@ extern "C" int collatz_run_case_batch(collatz_ctx* c, const collatz_case* cases,
       used += k;
     }
     if (r.errors) status = COLLATZ_E_DEVICE;
+  }
+  return status;
+}
+
+extern "C" int collatz_run_case_batch(collatz_ctx* c, const collatz_case* cases, uint32_t n,
+                                      collatz_case_result* out, uint32_t* overflow_pool, uint64_t pool_cap) {
+  if (!c || !n || !cases || !out || (pool_cap && !overflow_pool)) return COLLATZ_E_ARG;
+  if (n > COLLATZ_CASE_BATCH_MAX) return COLLATZ_E_LIMIT;
+  for (uint32_t i = 0; i < n; i++)
+    if (cases[i].sigfig > c->ct.mbi || cases[i].threepower >= 128) return COLLATZ_E_ARG;
+  std::lock_guard<std::recursive_mutex> g(c->mu);
+  std::memset(out, 0, sizeof(collatz_case_result) * n);
+  CK(c, cudaSetDevice(c->device));
+  uint64_t used = 0;
+  int status = COLLATZ_OK;
+  std::vector<uint32_t> shallow;
+  std::vector<uint32_t> tmp;
+  for (uint32_t i = 0; i < n; i++) {
+    if (c->ct.mbi - cases[i].sigfig < BATCH_ALONE_DEPTH || !s1_root_pass(cases[i])) {
+      shallow.push_back(i);
+      continue;
+    }
+    int rc = case_prepare(c);
+    if (rc) return rc;
+    tmp.resize(4ull * OVERFLOW_CAP);
+    collatz_case_result r;
+    std::memset(&r, 0, sizeof r);
+    r.overflow_seeds = tmp.data();
+    r.overflow_cap = OVERFLOW_CAP;
+    rc = run_case_device(c, &cases[i], &r);
+    if (rc && rc != COLLATZ_E_DEVICE) return rc;
+    if (rc) status = rc;
+    const uint64_t k = std::min<uint64_t>(std::min<uint64_t>(r.n_overflow, OVERFLOW_CAP), pool_cap - used);
+    r.overflow_seeds = nullptr;
+    r.overflow_cap = 0;
+    if (k) {
+      r.overflow_seeds = overflow_pool + 4 * used;
+      r.overflow_cap = k;
+      std::memcpy(r.overflow_seeds, tmp.data(), 16 * k);
+      used += k;
+    }
+    out[i] = r;
+  }
+  if (!shallow.empty()) {
+    const int rc = batch_pass(c, cases, shallow, out, overflow_pool, pool_cap, used);
+    if (rc && rc != COLLATZ_E_DEVICE) return rc;
+    if (rc) status = rc;
   }
   if (status) c->err = "device error bits in a line of the batch";
   return status;

@@ -18,9 +18,9 @@
 // limb 3 of a pair holds bigindex | line << 8 and every line has its own
 // record.  A pair slot keeps its line and that line's prefilter thresholds;
 // a lane folds checkpoint XORs into a register for one line at a time and
-// flushes it to the line's record when it takes a seed of another line.
-// Warps claim pairs 16 at a time, so neighbouring pairs (mostly one line's)
-// stay on one warp.
+// flushes it to the line's record when it takes a seed of another line; a
+// warp counts seeds the same way.  Warps claim pairs 16 at a time, so
+// neighbouring pairs (mostly one line's) stay on one warp.
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -65,6 +65,7 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
   u32 thr_st = 0, thr3 = 0, thr2 = 0;
   ull warp_seeds = 0;
   u32 pc = 0, pc_end = 0;  // MULTI: claimed pairs [pc, pc_end)
+  u32 wline = 0;           // MULTI: the line whose seeds warp_seeds counts
   // lane state
   bool active = false;
   u32 v0 = 0, v1 = 0, v2 = 0, v3 = 0, n0 = 0, n1 = 0, n2 = 0;
@@ -169,7 +170,11 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
           if (MULTI) {
             if (lane == 12) W.ring[slot][12] = thr_st;
             if (lane >= 13 && lane < 17) W.ring[slot][lane] = t[lane - 13];
-            if (lane == 0) atomicAdd(&prec->seeds, (ull)total);
+            if (pline != wline) {  // seeds are counted per warp until the line changes
+              if (lane == 0 && warp_seeds) atomicAdd(&A.rec[wline].seeds, warp_seeds);
+              warp_seeds = 0;
+              wline = pline;
+            }
           }
           u32 pos = qhead + qcount + excl;
           while (word) {
@@ -361,6 +366,7 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
   // ---- warp totals ----
   if (MULTI) {
     if (hash) atomicXor(&A.rec[hline].hash, hash);
+    if (lane == 0 && warp_seeds) atomicAdd(&A.rec[wline].seeds, warp_seeds);
   } else {
 #pragma unroll
     for (u32 d = 16; d; d >>= 1) hash ^= __shfl_xor_sync(FULL, hash, d);

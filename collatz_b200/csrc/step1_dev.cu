@@ -24,8 +24,9 @@
 // Line batches: the roots may be many cases_* lines at different sigfigs.
 // A node's sigfig word is sigfig | line << 8; a leaf reached before the last
 // breadth-first level passes through the later levels unchanged; the count
-// pass counts leaves per (line, bigindex); a pair carries bigindex | line << 8
-// in base limb 3.
+// pass counts leaves per (line, bigindex), one line per block in shared
+// memory and the others with global atomics; a pair carries
+// bigindex | line << 8 in base limb 3.
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -176,10 +177,13 @@ template <bool EMIT>
 __global__ void __launch_bounds__(128) k_step1_walk(const Step1Args A) {
   __shared__ u128d p3[128];
   __shared__ unsigned long long hist[17];
+  __shared__ uint32_t s_line;  // line batches: the line whose leaves this block counts in `hist`
   init_pow3(p3);
   if (threadIdx.x < 17u) hist[threadIdx.x] = 0ull;
-  __syncthreads();
   const uint32_t n = *A.in_count;
+  if (threadIdx.x == 0)  // a frontier node's line (one line per block is counted in shared memory)
+    s_line = (!EMIT && A.hist_lines && n) ? (A.in[min(blockIdx.x * 32u, n - 1u)].sig >> 8) : 0u;
+  __syncthreads();
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t T = A.nthreads;
@@ -213,7 +217,7 @@ __global__ void __launch_bounds__(128) k_step1_walk(const Step1Args A) {
               q[1] = make_uint4((uint32_t)num, (uint32_t)(num >> 32), (uint32_t)(num >> 64),
                                 (uint32_t)(num >> 96));
             }
-          } else if (A.hist_lines) {
+          } else if (A.hist_lines && line != s_line) {
             atomicAdd(&A.hist_lines[17ull * line + (bi < 16u ? bi : 16u)], 1ull);
           } else {
             atomicAdd(&hist[bi < 16u ? bi : 16u], 1ull);
@@ -290,7 +294,8 @@ __global__ void __launch_bounds__(128) k_step1_walk(const Step1Args A) {
   }
   if (!EMIT) {
     __syncthreads();
-    if (threadIdx.x < 17u && hist[threadIdx.x]) atomicAdd(A.hist + threadIdx.x, hist[threadIdx.x]);
+    if (threadIdx.x < 17u && hist[threadIdx.x])
+      atomicAdd((A.hist_lines ? A.hist_lines + 17ull * s_line : A.hist) + threadIdx.x, hist[threadIdx.x]);
   }
 }
 

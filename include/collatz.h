@@ -119,11 +119,13 @@ typedef struct {
  * the same result. */
 int collatz_run_case(collatz_ctx *ctx, const collatz_case *c, collatz_case_result *out);
 
-/* No counterpart in the reference.  Runs cases[0..n) together, as one
- * device pass: Step 1 from all n roots at once, then Steps 2-3 with a
- * record per case (n <= COLLATZ_CASE_BATCH_MAX).  For a file of many small
- * lines (cases_big) this replaces n calls of collatz_run_case, whose fixed
- * cost per call would dominate.  out[i] receives what collatz_run_case gives
+/* No counterpart in the reference.  Runs cases[0..n) together
+ * (n <= COLLATZ_CASE_BATCH_MAX): the lines at least 20 levels above the
+ * leaves (N - A - sigfig >= 20, each enough to fill the GPU) run one after
+ * another as in collatz_run_case; all the others share one device pass:
+ * Step 1 from all their roots at once, then Steps 2-3 with a record per
+ * case.  For a file of many small lines (cases_big) this replaces n calls of
+ * collatz_run_case, whose fixed cost per call would dominate.  out[i] receives what collatz_run_case gives
  * for cases[i]: hash, launches, seeds, pairs, maxima, errors, n_overflow;
  * device_ms is the pass's device time split by seeds.  Overflow seeds go to
  * one pool (4 uint32 per seed, pool_cap seeds), grouped by case, ascending
