@@ -47,14 +47,8 @@ struct CasesWarp {
 template <int ITERS, int REFILL_MIN, bool MULTI>
 __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
   __shared__ CasesWarp<MULTI> S[CWARPS];
-  __shared__ u32 s_pow3[9];
   const u32 lane = lane_id();
   CasesWarp<MULTI>& W = S[threadIdx.x >> 5];
-  if (threadIdx.x < 9) {
-    u32 p = 1;
-    for (u32 i = 0; i < threadIdx.x; i++) p *= 3;
-    s_pow3[threadIdx.x] = p;  // THREEPOWERSU16, cu:61
-  }
   if (lane < 4) W.thr[lane] = 0;
   __syncthreads();
 
@@ -276,38 +270,43 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
       for (int it = 0; it < ITERS; it++) {
 #pragma unroll
         for (int half = 0; half < 2; half++) {
-          // odd run
+          // odd run; 3^a from registers.  The stopping time stops counting at the
+          // first descent (found) or after an overflow report (ovf: no maxima).
           const u32 a = ctz32(v0 | (1u << 8));
-          odd_run4(v0, v1, v2, v3, a, s_pow3[a]);
-          if (!found) st += a;
-          if (v3 >= 16u) {  // v >= 2^100 (cu:295, 334); search3 tests > on the second (cu:702)
-            const bool o = !(half == 1 && cpu && v3 == 16u && (v0 | v1 | v2) == 0u);
-            if (o) {
-              const ull i = atomicAdd(A.overflow_count, 1ull);
-              if (i < A.overflow_cap) {
-                A.overflow[4 * i + 0] = n0;
-                A.overflow[4 * i + 1] = n1;
-                A.overflow[4 * i + 2] = n2;
-                A.overflow[4 * i + 3] = MULTI ? hline : 0u;
+          odd_run4(v0, v1, v2, v3, a, pow3_le8(a));
+          st += (found | ovf) ? 0u : a;
+          // one branch for the two rare events of an odd run: overflow, excursion candidate
+          if ((v3 >= 16u) | (!(found | ovf) & ((((u64)v3 << 32) | v2) >= thr_top))) {
+            if (v3 >= 16u) {  // v >= 2^100 (cu:295, 334); search3 tests > on the second (cu:702)
+              const bool o = !(half == 1 && cpu && v3 == 16u && (v0 | v1 | v2) == 0u);
+              if (o) {
+                const ull i = atomicAdd(A.overflow_count, 1ull);
+                if (i < A.overflow_cap) {
+                  A.overflow[4 * i + 0] = n0;
+                  A.overflow[4 * i + 1] = n1;
+                  A.overflow[4 * i + 2] = n2;
+                  A.overflow[4 * i + 3] = MULTI ? hline : 0u;
+                }
+                if (MULTI) atomicAdd(&A.rec[hline].items_done, 1ull);  // the line's overflow reports
+                ovf = 1;
+                v0 = 2;
+                v1 = v2 = v3 = 0;
               }
-              if (MULTI) atomicAdd(&A.rec[hline].items_done, 1ull);  // the line's overflow reports
-              ovf = 1;
-              v0 = 2;
-              v1 = v2 = v3 = 0;
             }
-          }
-          if (!found && !ovf && (((u64)v3 << 32) | v2) >= thr_top) {
-            // rare: exact excursion candidate x = v - 1 against the seed max / threshold
-            const u32 x0 = v0 - 1, x1 = v1 - (v0 == 0), x2 = v2 - ((v0 | v1) == 0), x3 = v3 - ((v0 | v1 | v2) == 0);
-            const u32* ref = evalid ? &W.lane[lane][4] : (MULTI ? &W.lane[lane][9] : W.thr);
-            const bool ge = !lt96(x1, x2, x3, ref[1], ref[2], ref[3]) &&
-                            !((x3 == ref[3]) & (x2 == ref[2]) & (x1 == ref[1]) & (x0 < ref[0]));
-            if (ge) {
-              W.lane[lane][4] = x0;
-              W.lane[lane][5] = x1;
-              W.lane[lane][6] = x2;
-              W.lane[lane][7] = x3;
-              evalid = 1;
+            if (!found && !ovf && (((u64)v3 << 32) | v2) >= thr_top) {
+              // exact excursion candidate x = v - 1 against the seed max / threshold
+              const u32 x0 = v0 - 1, x1 = v1 - (v0 == 0), x2 = v2 - ((v0 | v1) == 0),
+                        x3 = v3 - ((v0 | v1 | v2) == 0);
+              const u32* ref = evalid ? &W.lane[lane][4] : (MULTI ? &W.lane[lane][9] : W.thr);
+              const bool ge = !lt96(x1, x2, x3, ref[1], ref[2], ref[3]) &&
+                              !((x3 == ref[3]) & (x2 == ref[2]) & (x1 == ref[1]) & (x0 < ref[0]));
+              if (ge) {
+                W.lane[lane][4] = x0;
+                W.lane[lane][5] = x1;
+                W.lane[lane][6] = x2;
+                W.lane[lane][7] = x3;
+                evalid = 1;
+              }
             }
           }
           // even run
@@ -315,30 +314,22 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
           const u32 b = ctz32(v0 | 0x80000000u);
           const u32 w0 = __funnelshift_r(v0, v1, b), w1 = __funnelshift_r(v1, v2, b);
           const u32 w2 = __funnelshift_r(v2, v3, b), w3 = v3 >> b;
-          if (!found && !ovf) {
-            if (b != 0 && w3 == 0 && w2 <= n2 && lt96(w0, w1, w2, n0, n1, n2)) {
-              // first descent inside this run: smallest i with (v-1) >> i < n
-              st += first_below(v0, v1, v2, v3, n0, n1, n2, nbl);
-              found = 1;
-            } else {
-              st += b;
-            }
+          if (!(found | ovf) & (b != 0) & (w3 == 0) & lt96c(w0, w1, w2, n0, n1, n2)) {
+            // first descent inside this run: smallest i with (v-1) >> i < n
+            st += first_below(v0, v1, v2, v3, n0, n1, n2, nbl);
+            found = 1;
+          } else {
+            st += (found | ovf) ? 0u : b;
           }
           v0 = w0 + 1;
           v1 = w1;
           v2 = w2;
           v3 = w3;
-          if (v0 == 0 && b != 0) {  // carry of the +1 (cu:310-318)
-            v1 += 1;
-            if (v1 == 0) {
-              v2 += 1;
-              if (v2 == 0) v3 += 1;
-            }
-          }
+          add_carry3(v1, v2, v3, (v0 == 0) & (b != 0));  // carry of the +1 (cu:310-318)
         }
         hash ^= v0;  // cu:359
         iters++;
-        const bool done = (v3 == 0) && lt96(v0, v1, v2, n0, n1, n2);  // cu:362-365
+        const bool done = (v3 == 0) & lt96c(v0, v1, v2, n0, n1, n2);  // cu:362-365
         if (done || iters >= A.iter_cap) {
           if (!done) {
             ReqRec* rec = MULTI ? A.rec + hline : A.rec;

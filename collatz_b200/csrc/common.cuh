@@ -49,6 +49,37 @@ __device__ __forceinline__ bool lt96(u32 a0, u32 a1, u32 a2, u32 b0, u32 b1, u32
   return (a2 < b2) | ((a2 == b2) & ((a1 < b1) | ((a1 == b1) & (a0 < b0))));
 }
 
+// 3^a for a <= 7 from two byte-permute lookups: low bytes 01 03 09 1B 51 F3 D9 8B,
+// high bytes 00 00 00 00 00 00 02 08 (3^6 = 0x2D9, 3^7 = 0x88B).
+__device__ __forceinline__ u32 pow3_le7(u32 a) {
+  return (__byte_perm(0x1B090301u, 0x8BD9F351u, a) & 0xFFu) | __byte_perm(0u, 0x08020000u, a << 4);
+}
+
+// 3^a for a <= 8 (3^8 = 6561), in registers.
+__device__ __forceinline__ u32 pow3_le8(u32 a) { return a == 8u ? 6561u : pow3_le7(a); }
+
+// (a2:a1:a0) < (b2:b1:b0) as one borrow chain.
+__device__ __forceinline__ bool lt96c(u32 a0, u32 a1, u32 a2, u32 b0, u32 b1, u32 b2) {
+  u32 r;
+  asm("{\n\t.reg .u32 t;\n\t"
+      "sub.cc.u32 t, %1, %4;\n\t"
+      "subc.cc.u32 t, %2, %5;\n\t"
+      "subc.cc.u32 t, %3, %6;\n\t"
+      "subc.u32 %0, 0, 0;\n\t}"
+      : "=r"(r)
+      : "r"(a0), "r"(a1), "r"(a2), "r"(b0), "r"(b1), "r"(b2));
+  return r != 0;
+}
+
+// (v3:v2:v1) += c for c in {0, 1}, as one carry chain.
+__device__ __forceinline__ void add_carry3(u32& v1, u32& v2, u32& v3, u32 c) {
+  asm("add.cc.u32 %0, %0, %3;\n\t"
+      "addc.cc.u32 %1, %1, 0;\n\t"
+      "addc.u32 %2, %2, 0;"
+      : "+r"(v1), "+r"(v2), "+r"(v3)
+      : "r"(c));
+}
+
 // Bit length of a 96-bit value.
 __device__ __forceinline__ u32 bitlen96(u32 n0, u32 n1, u32 n2) {
   return n2 ? 96u - __clz(n2) : (n1 ? 64u - __clz(n1) : 32u - __clz(n0));

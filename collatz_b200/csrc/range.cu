@@ -78,25 +78,6 @@ __device__ __forceinline__ u32 bitlen128(unsigned __int128 x) {
   return hi ? 128u - __clzll(hi) : (lo ? 64u - __clzll(lo) : 0u);
 }
 
-// 3^a for a <= 7 from two byte-permute lookups: low bytes 01 03 09 1B 51 F3 D9 8B,
-// high bytes 00 00 00 00 00 00 02 08 (3^6 = 0x2D9, 3^7 = 0x88B).
-__device__ __forceinline__ u32 pow3_le7(u32 a) {
-  return (__byte_perm(0x1B090301u, 0x8BD9F351u, a) & 0xFFu) | __byte_perm(0u, 0x08020000u, a << 4);
-}
-
-// (a2:a1:a0) < (b2:b1:b0) as one borrow chain.
-__device__ __forceinline__ bool lt96c(u32 a0, u32 a1, u32 a2, u32 b0, u32 b1, u32 b2) {
-  u32 r;
-  asm("{\n\t.reg .u32 t;\n\t"
-      "sub.cc.u32 t, %1, %4;\n\t"
-      "subc.cc.u32 t, %2, %5;\n\t"
-      "subc.cc.u32 t, %3, %6;\n\t"
-      "subc.u32 %0, 0, 0;\n\t}"
-      : "=r"(r)
-      : "r"(a0), "r"(a1), "r"(a2), "r"(b0), "r"(b1), "r"(b2));
-  return r != 0;
-}
-
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
