@@ -627,13 +627,7 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
       if (NEG) {
         // t = u + 1 with a full carry (a low limb of all ones gives b = 31 below)
         v0 += 1;
-        if (v0 == 0) {
-          v1 += 1;
-          if (v1 == 0) {
-            v2 += 1;
-            if (v2 == 0) v3 += 1;
-          }
-        }
+        add_carry3(v1, v2, v3, v0 == 0);
       } else {
         v0 -= 1;  // v0 == 0 gives b == 0 below, and the borrow cancels against the +1
       }
@@ -698,13 +692,7 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
         v1 = w1;
         v2 = w2;
         v3 = w3;
-        if ((v0 == 0) & (b != 0)) {
-          v1 += 1;
-          if (v1 == 0) {
-            v2 += 1;
-            if (v2 == 0) v3 += 1;
-          }
-        }
+        add_carry3(v1, v2, v3, (v0 == 0) & (b != 0));
       }
     }
   }
