@@ -991,7 +991,7 @@ extern "C" int collatz_run_case_batch(collatz_ctx* c, const collatz_case* cases,
     std::memset(&r, 0, sizeof r);
     r.overflow_seeds = tmp.data();
     r.overflow_cap = OVERFLOW_CAP;
-    rc = run_case_device(c, &cases[i], &r);
+    rc = (c->cfg.flags & COLLATZ_CFG_HOST_STEP1) ? run_case_host(c, &cases[i], &r) : run_case_device(c, &cases[i], &r);
     if (rc && rc != COLLATZ_E_DEVICE) return rc;
     if (rc) status = rc;
     const uint64_t k = std::min<uint64_t>(std::min<uint64_t>(r.n_overflow, OVERFLOW_CAP), pool_cap - used);
