@@ -65,6 +65,7 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
   u32 v0 = 0, v1 = 0, v2 = 0, v3 = 0, n0 = 0, n1 = 0, n2 = 0;
   u32 st = 0, iters = 0, hash = 0;
   u32 nbl = 0;  // bit length of the seed n
+  u32 sig = 0;  // the stopping time, set at the first descent (st keeps counting)
   u32 found = 0, ovf = 0, cpu = 0, evalid = 0, pend = 0;
   u32 hline = 0;      // MULTI: the line whose checkpoint XORs `hash` holds (and of the lane's seed)
   u64 lthr_top = 0;   // MULTI: the lane's line's excursion threshold, bits 64..127
@@ -266,6 +267,10 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
     // ---- Step 3 (cu:280-405) ----
     if (active) {
       const u64 thr_top = MULTI ? lthr_top : (((u64)thr3 << 32) | thr2);
+      // one compare per odd run finds both rare events: v >= 2^100 (overflow, top limbs
+      // 16:0) and, while the seed still counts, an excursion candidate (top limbs >= thr_top)
+      constexpr u64 OVF_TOP = 16ull << 32;
+      u64 gate = (found | ovf) ? OVF_TOP : min(thr_top, OVF_TOP);
 #pragma unroll 1
       for (int it = 0; it < ITERS; it++) {
 #pragma unroll
@@ -274,9 +279,8 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
           // first descent (found) or after an overflow report (ovf: no maxima).
           const u32 a = ctz32(v0 | (1u << 8));
           odd_run4(v0, v1, v2, v3, a, pow3_le8(a));
-          st += (found | ovf) ? 0u : a;
-          // one branch for the two rare events of an odd run: overflow, excursion candidate
-          if ((v3 >= 16u) | (!(found | ovf) & ((((u64)v3 << 32) | v2) >= thr_top))) {
+          st += a;
+          if ((((u64)v3 << 32) | v2) >= gate) {  // overflow or excursion candidate (rare)
             if (v3 >= 16u) {  // v >= 2^100 (cu:295, 334); search3 tests > on the second (cu:702)
               const bool o = !(half == 1 && cpu && v3 == 16u && (v0 | v1 | v2) == 0u);
               if (o) {
@@ -289,6 +293,7 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
                 }
                 if (MULTI) atomicAdd(&A.rec[hline].items_done, 1ull);  // the line's overflow reports
                 ovf = 1;
+                gate = OVF_TOP;
                 v0 = 2;
                 v1 = v2 = v3 = 0;
               }
@@ -316,11 +321,11 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
           const u32 w2 = __funnelshift_r(v2, v3, b), w3 = v3 >> b;
           if (!(found | ovf) & (b != 0) & (w3 == 0) & lt96c(w0, w1, w2, n0, n1, n2)) {
             // first descent inside this run: smallest i with (v-1) >> i < n
-            st += first_below(v0, v1, v2, v3, n0, n1, n2, nbl);
+            sig = st + first_below(v0, v1, v2, v3, n0, n1, n2, nbl);
             found = 1;
-          } else {
-            st += (found | ovf) ? 0u : b;
+            gate = OVF_TOP;
           }
+          st += b;
           v0 = w0 + 1;
           v1 = w1;
           v2 = w2;
@@ -336,8 +341,9 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
             atomicOr(&rec->errors, ERR_ITER_CAP);
             atomicAdd(&rec->failures, 1ull);
           } else if (!ovf) {
-            if (st >= (MULTI ? W.lane[lane][8] : thr_st)) {
-              W.lane[lane][0] = st;
+            const u32 sigma = found ? sig : st;  // done implies found: an odd run only rises
+            if (sigma >= (MULTI ? W.lane[lane][8] : thr_st)) {
+              W.lane[lane][0] = sigma;
               pend |= 1u;
             }
             if (evalid) pend |= 2u;
