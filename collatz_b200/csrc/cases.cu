@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
       // 16:0) and, while the seed still counts, an excursion candidate (top limbs >= thr_top)
       constexpr u64 OVF_TOP = 16ull << 32;
       u64 gate = (found | ovf) ? OVF_TOP : min(thr_top, OVF_TOP);
-#pragma unroll 1
+#pragma unroll
       for (int it = 0; it < ITERS; it++) {
 #pragma unroll
         for (int half = 0; half < 2; half++) {
