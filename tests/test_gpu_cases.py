@@ -118,9 +118,9 @@ def test_every_cases_variant_matches_reference(verifier, oracle_tables, variant)
         assert (r.hash, r.seeds_checked) == (o.hash, o.seeds)
         assert (r.max_stopping_time, r.max_stopping_time_seed) == (o.max_st, o.max_st_seed)
         assert (r.max_excursion, r.max_excursion_seed) == (o.max_exc, o.max_exc_seed)
-    finally:
-        v.set_variant(0, 1)
-        verifier(36).set_variant(0, 1)
+    finally:  # back to the default variant
+        v.set_variant(0, 3)
+        verifier(36).set_variant(0, 3)
 
 
 def test_pair_maxima_match_oracle(verifier, oracle_tables):
