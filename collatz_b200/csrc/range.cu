@@ -575,7 +575,7 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
     if (exhausted && tail == head && __ballot_sync(FULL, active) == 0) break;
 
     // ---- lanes: R times (take a seed if idle, one odd run and one even run) ----
-#pragma unroll 1
+#pragma unroll
     for (int r = 0; r < R; r++) {
       {
         // idle lanes take the next queued seeds (a pending offer keeps its scratch until the next pass)
