@@ -26,7 +26,8 @@ namespace cz {
 constexpr u32 RQ = 128;          // queue entries per warp, power of two (>= 32 R + one item)
 constexpr u32 RR = 32;           // item slots per warp (one per lane; see expand_one)
 constexpr u32 RWARPS = 7;
-constexpr u32 CLAIM = 8;         // items claimed per atomic
+constexpr u32 CLAIM = 8;         // items claimed per atomic near the end of a launch
+constexpr u32 CLAIM_BIG = 32;    // ... and while at least 128 items per warp remain
 constexpr u32 KEEP9 = 0xCBu;     // n mod 9 in {0,1,3,6,7} survives (cu:488)
 // Negative variant T'(m) = (3m-1)/2, m/2: m = 1 mod 3 (m > 1) is T' of the smaller
 // (2m+1)/3 and m = 5 mod 9 (m > 5) is T'^3 of the smaller (8m+5)/9, so m mod 9 in
@@ -128,8 +129,11 @@ __device__ __forceinline__ void stage_next(WT& W, uint4* dst, const RangeArgs& A
   ull next = W.item + 1;
   bool fresh = false;
   if (next >= W.claim_hi) {
+    // the warp's last claim end stands in for the cursor: big claims while far from the end
+    const u32 claim =
+        (W.claim_hi + (ull)gridDim.x * RWARPS * 128u < A.item_limit) ? CLAIM_BIG : CLAIM;
     ull c = 0;
-    if (lane == 0) c = atomicAdd(A.item_cursor, (ull)CLAIM);
+    if (lane == 0) c = atomicAdd(A.item_cursor, (ull)claim);
     c = __shfl_sync(FULL, c, 0);
     if (c >= A.item_limit) {
       __syncwarp();
@@ -140,7 +144,7 @@ __device__ __forceinline__ void stage_next(WT& W, uint4* dst, const RangeArgs& A
     next = c;
     fresh = true;
     __syncwarp();
-    if (lane == 0) W.claim_hi = min(c + CLAIM, A.item_limit);
+    if (lane == 0) W.claim_hi = min(c + claim, A.item_limit);
   }
   if (next < W.seg_lo || next >= W.seg_hi) {
     u32 si = 0;
