@@ -103,3 +103,19 @@ def test_batch_argument_checks(verifier):
     with pytest.raises(cb.CollatzError):
         v.run_case_batch([(3, 2, 2, 9, 1, 0), (3, 17, 12, 9, 1, 0)])  # sigfig > N - A
     assert v.run_case_batch([]) == []
+
+
+def test_overflow_pool_smaller_than_the_reports(verifier):
+    """With an overflow pool of 500 seeds for 1 242 reports, every line still
+    counts all its reports (n_overflow), the pool is filled line by line, and
+    each line's part is a subset of its full list."""
+    v = verifier(40)
+    lines = [(5, 28, 20, (1 << 99) - 12345, 0, 0), (7, 27, 19, (1 << 98) + 999, 0, 0),
+             (3, 29, 21, (1 << 99) + (1 << 97), 0, 1)]
+    part = v.run_case_batch(lines, pool_cap=500)
+    full = v.run_case_batch(lines)
+    assert [r.n_overflow for r in part] == [432, 529, 281]
+    assert [len(r.overflow) for r in part] == [432, 68, 0]
+    for p, f in zip(part, full):
+        assert set(p.overflow) <= set(f.overflow)
+        assert (p.hash, p.seeds_checked) == (f.hash, f.seeds_checked)
