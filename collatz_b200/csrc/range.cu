@@ -248,10 +248,11 @@ struct ExpandStats {
 // request and thresholds from their item's slot when they are popped, so a
 // slot is reused only after the last seed of its previous item has left the
 // queue; the queue is then not empty).  Warp-uniform.
-template <bool STATS, bool NEG, class WT>
+template <bool STATS, bool NEG, bool WIN, class WT>
 __device__ __forceinline__ bool expand_one(WT& W, const RangeArgs& A, const uint4* __restrict__ T, u32 lane, u32 k,
-                                           u32 k9, const unsigned long long* s_p3, u32 head, u32& tail,
-                                           bool& exhausted, u32& w_thr_st, u32& w_req, u64& w_gate, ExpandStats& X) {
+                                           u32 k9, const unsigned long long* s_p3, const u32* s_win, u32 head,
+                                           u32& tail, bool& exhausted, u32& w_thr_st, u32& w_req, u64& w_gate,
+                                           ExpandStats& X) {
   if ((int)(W.ring_end[W.ring_seq & (RR - 1)] - head) > 0) return false;
   if (STATS) X.t_sub = clock64();
   cp_async_wait_all();  // this lane's copies of the staged item
@@ -369,6 +370,32 @@ __device__ __forceinline__ bool expand_one(WT& W, const RangeArgs& A, const uint
             V3 += q2 * p1 + (u32)(ee >> 32);
           }
           s0 = k;
+          if (WIN && !NEG) {
+            // 8 more steps at once when they can neither descend nor reach the
+            // excursion threshold: x = T^k(n) = a 2^8 + r gives T^i(x) = a 2^(8-i) 3^f_i +
+            // T^i(r) for i <= 8, so a g(r) <= T^i(x) < (a + 1) h(r) (g, h: the least and
+            // largest 2^(8-i) 3^f_i); bit lengths test both bounds
+            const u32 x0 = V0 - 1, x1 = V1 - (V0 == 0), x2 = V2 - ((V0 | V1) == 0), x3 = V3 - ((V0 | V1 | V2) == 0);
+            const u32 e8 = s_win[x0 & 255u];
+            const u32 xb = x3 ? 128u - __clz(x3) : (x2 ? 96u - __clz(x2) : (x1 ? 64u - __clz(x1) : 32u - __clz(x0)));
+            const u32 glen = (e8 >> 20) & 31u, hlen = (e8 >> 25) & 31u;
+            if ((xb + glen >= nbl + 10u) & (xb + hlen < w_thr_bl + 8u) & (xb <= 100u)) {
+              u32 y0 = x0, y1 = x1, y2 = x2, y3 = x3;
+              odd_run4(y0, y1, y2, y3, 8u, pow3_le8((e8 >> 16) & 15u));  // (x >> 8) 3^f_8
+              // + T^8(r) + 1 (back to v space)
+              asm("add.cc.u32 %0, %0, %4;\n\t"
+                  "addc.cc.u32 %1, %1, 0;\n\t"
+                  "addc.cc.u32 %2, %2, 0;\n\t"
+                  "addc.u32 %3, %3, 0;"
+                  : "+r"(y0), "+r"(y1), "+r"(y2), "+r"(y3)
+                  : "r"((e8 & 0xFFFFu) + 1u));
+              V0 = y0;
+              V1 = y1;
+              V2 = y2;
+              V3 = y3;
+              s0 = k + 8u;
+            }
+          }
           if (STATS) X.c_jump++;
         } else {
           if (NEG) {  // u = n - 1 (n >= 2^k: no borrow out of 96 bits)
@@ -431,7 +458,7 @@ __device__ __forceinline__ bool expand_one(WT& W, const RangeArgs& A, const uint
   return true;
 }
 
-template <int R, int MINB, bool STATS = false, bool NEG = false>
+template <int R, int MINB, bool STATS = false, bool NEG = false, bool WIN = false>
 __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) {
   // diagnostics (STATS variant only): run pairs, excursion slow paths, replays, jumps, pops,
   // expansions, passes, offers; clock64 cycles per phase (lane 0)
@@ -442,6 +469,25 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
   RangeWarp* S = reinterpret_cast<RangeWarp*>(range_smem);
   __shared__ unsigned long long s_p3[41];
   __shared__ u32 s_pow3[9], s_keep9[9];
+  __shared__ u32 s_win[WIN ? 256 : 1];  // per r < 2^8: T^8(r) | f_8 << 16 | bitlen(g) << 20 | bitlen(h) << 25
+  if (WIN) {
+    for (u32 r = threadIdx.x; r < 256u; r += blockDim.x) {
+      u32 x = r, f = 0, g = 0xFFFFFFFFu, h = 0;
+      for (u32 i = 1; i <= 8u; i++) {
+        if (x & 1u) {
+          x = (3u * x + 1u) >> 1;
+          f++;
+        } else {
+          x >>= 1;
+        }
+        u32 t = 1u << (8u - i);
+        for (u32 j = 0; j < f; j++) t *= 3u;
+        g = min(g, t);
+        h = max(h, t);
+      }
+      s_win[r] = x | (f << 16) | ((32u - __clz(g)) << 20) | ((32u - __clz(h)) << 25);
+    }
+  }
   const u32 lane = lane_id();
   RangeWarp& W = S[threadIdx.x >> 5];
   if (threadIdx.x < 41) {
@@ -567,7 +613,8 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
     }
     // ---- refill: keep 32 R seeds queued (each lane pops at most R per pass) ----
     while (tail - head < 32u * R && !exhausted) {
-      if (!expand_one<STATS, NEG>(W, A, T, lane, k, k9, s_p3, head, tail, exhausted, w_thr_st, w_req, w_gate, X))
+      if (!expand_one<STATS, NEG, WIN>(W, A, T, lane, k, k9, s_p3, s_win, head, tail, exhausted, w_thr_st, w_req,
+                                       w_gate, X))
         break;
     }
     __syncwarp();
@@ -814,7 +861,7 @@ __global__ void __launch_bounds__(128) k_range_wide(const WidenEntry* __restrict
 // ------------------------------------------------------------------
 // Launchers.
 // ------------------------------------------------------------------
-int range_variants() { return 4; }
+int range_variants() { return 6; }
 
 constexpr size_t RANGE_SMEM = sizeof(RangeWarp) * RWARPS;
 
@@ -823,17 +870,17 @@ cudaError_t launch_range_stats(const RangeArgs& a, u32 grid, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-// (run pairs per pass, minimum resident blocks per SM)
-#define CZ_RANGE_VARIANTS(X) X(0, 1, 3) X(1, 2, 3) X(2, 2, 4) X(3, 1, 4)
+// (run pairs per pass, minimum resident blocks per SM, 8-step window after the k-step jump)
+#define CZ_RANGE_VARIANTS(X) X(0, 1, 3, 0) X(1, 2, 3, 0) X(2, 2, 4, 0) X(3, 1, 4, 0) X(4, 2, 4, 1) X(5, 2, 3, 1)
 
 cudaError_t launch_range(const RangeArgs& a, int variant, u32 grid, cudaStream_t st) {
   switch (variant) {
-#define X(id, rm, mb)                                                                 \
+#define X(id, rm, mb, win)                                                            \
   case id:                                                                            \
     if (a.negative)                                                                   \
       k_range<rm, mb, false, true><<<grid, RWARPS * 32, RANGE_SMEM, st>>>(a);         \
     else                                                                              \
-      k_range<rm, mb><<<grid, RWARPS * 32, RANGE_SMEM, st>>>(a);                      \
+      k_range<rm, mb, false, false, win><<<grid, RWARPS * 32, RANGE_SMEM, st>>>(a);   \
     break;
     CZ_RANGE_VARIANTS(X)
 #undef X
@@ -844,9 +891,9 @@ cudaError_t launch_range(const RangeArgs& a, int variant, u32 grid, cudaStream_t
 
 cudaError_t range_occupancy(int variant, int* bps) {
   switch (variant) {
-#define X(id, rm, mb) \
-  case id:            \
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_range<rm, mb>, RWARPS * 32, RANGE_SMEM);
+#define X(id, rm, mb, win) \
+  case id:                 \
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_range<rm, mb, false, false, win>, RWARPS * 32, RANGE_SMEM);
     CZ_RANGE_VARIANTS(X)
 #undef X
     default: return cudaErrorInvalidValue;
@@ -856,9 +903,10 @@ cudaError_t range_occupancy(int variant, int* bps) {
 // Opts every range kernel into RANGE_SMEM (> 48 KB) of dynamic shared memory.
 cudaError_t range_init() {
   cudaError_t e = cudaSuccess;
-#define X(id, rm, mb)                                                                                          \
+#define X(id, rm, mb, win)                                                                                     \
   if (e == cudaSuccess)                                                                                        \
-    e = cudaFuncSetAttribute(k_range<rm, mb>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RANGE_SMEM);    \
+    e = cudaFuncSetAttribute(k_range<rm, mb, false, false, win>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                             (int)RANGE_SMEM);                                                                 \
   if (e == cudaSuccess)                                                                                        \
     e = cudaFuncSetAttribute(k_range<rm, mb, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,         \
                              (int)RANGE_SMEM);

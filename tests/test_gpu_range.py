@@ -54,12 +54,13 @@ def test_range_matches_oracle(verifier, case):
 VARIANT_CASES = [CASES[i] for i in (0, 3, 4, 5, 6, 7, 8, 10)]
 
 
-@pytest.mark.parametrize("variant", range(4))
+@pytest.mark.parametrize("variant", range(6))
 def test_range_variants_match_oracle(verifier, variant):
-    """Every range-kernel variant (block shape) gives the oracle's results."""
+    """Every range-kernel variant (block shape; 4 and 5 add the 8-step window
+    after the k-step jump) gives the oracle's results."""
     import collatz_b200 as cb
     from oracle import oracle as O
-    assert cb.lib().collatz_variant_count(1) == 4
+    assert cb.lib().collatz_variant_count(1) == 6
     v = verifier(26)
     v.set_variant(1, variant)
     try:
@@ -73,7 +74,7 @@ def test_range_variants_match_oracle(verifier, variant):
             o = O.range_verify(*q, method=1, nthreads=NT)
             _cmp(m, o)
     finally:
-        v.set_variant(1, 2)
+        v.set_variant(1, 4)  # the default
 
 
 def test_batch_of_tiny_requests(verifier):
@@ -184,3 +185,22 @@ def test_limits_rejected(verifier):
         v.verify_range((1 << 96) - 10, 100, 24)
     with pytest.raises(cb.CollatzError):
         v.verify_range(1 << 40, 1 << 49, 24)
+
+
+@pytest.mark.parametrize("off,size,k", [((1 << 40) + 12345, 1 << 32, 24), ((1 << 60) + (5 << 34), 1 << 34, 34),
+                                        ((1 << 90) + 777, 1 << 30, 24)])
+def test_window_variant_equals_plain(verifier, off, size, k):
+    """The 8-step window after the k-step jump (variant 4) leaves every output
+    unchanged on large ranges, where most seeds take it: seeds, maxima with
+    their seeds, failures and widened seeds equal the plain variant's."""
+    v = verifier(26, range_k=k)
+    try:
+        v.set_variant(1, 4)
+        w = v.verify_range(off, size, k)
+        v.set_variant(1, 2)
+        p = v.verify_range(off, size, k)
+    finally:
+        v.set_variant(1, 4)  # the default
+    assert (w.seeds_checked, w.failures, w.widened, w.errors) == (p.seeds_checked, p.failures, p.widened, p.errors)
+    assert (w.max_stopping_time, w.max_stopping_time_seed) == (p.max_stopping_time, p.max_stopping_time_seed)
+    assert (w.max_excursion, w.max_excursion_seed) == (p.max_excursion, p.max_excursion_seed)
