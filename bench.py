@@ -51,12 +51,12 @@ OPS_JUMP, OPS_ODD, OPS_EVEN = 16, 14, 12
 K_RANGE_DRAM_BYTES = 5.339648e6 + 0.219904e6
 # Frontier (k = 34): every block of 2^34 seeds streams the 5 mod-9 classes
 # of the 2.43 GB survivor table that it keeps; ncu on a 4-block launch read
-# 5.406020352e9 and wrote 9.036032e6 bytes, so traffic per launch = blocks x
+# 5.421552640e9 and wrote 9.596928e6 bytes, so traffic per launch = blocks x
 # this figure.
-K_RANGE_FRONTIER_DRAM_BYTES_PER_BLOCK = (5.406020352e9 + 9.036032e6) / 4
+K_RANGE_FRONTIER_DRAM_BYTES_PER_BLOCK = (5.421552640e9 + 9.596928e6) / 4
 # Issue-slot utilisation of k_range measured with ncu (2^33 block, k = 24;
 # 2^36 frontier, k = 34).
-K_RANGE_ISSUE_NCU = {"block": 0.6921, "frontier": 0.7632}
+K_RANGE_ISSUE_NCU = {"block": 0.6921, "frontier": 0.7416}
 
 
 def dist_env():
