@@ -48,15 +48,18 @@ UNIT = "seeds/s"
 # shifts, increment with carry, descent test).
 OPS_JUMP, OPS_ODD, OPS_EVEN = 16, 14, 12
 # DRAM bytes (read + write) of one k_range launch, measured with ncu.
-K_RANGE_DRAM_BYTES = 5.339648e6 + 0.219904e6
+K_RANGE_DRAM_BYTES = 5.366272e6 + 0.226048e6
 # Frontier (k = 34): every block of 2^34 seeds streams the 5 mod-9 classes
 # of the 2.43 GB survivor table that it keeps; ncu on a 4-block launch read
 # 5.421552640e9 and wrote 9.596928e6 bytes, so traffic per launch = blocks x
 # this figure.
 K_RANGE_FRONTIER_DRAM_BYTES_PER_BLOCK = (5.421552640e9 + 9.596928e6) / 4
-# Issue-slot utilisation of k_range measured with ncu (2^33 block, k = 24;
-# 2^36 frontier, k = 34).
-K_RANGE_ISSUE_NCU = {"block": 0.6921, "frontier": 0.7416}
+# Issue-slot and ALU-pipe utilisation of k_range measured with ncu (2^33
+# block, k = 24; 2^36 frontier, k = 34).  The ALU pipe is the one that
+# saturates first for this instruction mix (collatz_int_peak mix 1 reaches
+# its limit at 77 % of the issue slots).
+K_RANGE_ISSUE_NCU = {"block": 0.6703, "frontier": 0.7416}
+K_RANGE_ALU_PIPE_NCU = {"block": 0.5913, "frontier": 0.6560}
 
 
 def dist_env():
@@ -509,7 +512,11 @@ def main():
         mean_ms = sum(ms) / len(ms)
         achieved = ops_step / (mean_ms / 1e3) / 1e12
         sm_mhz = clocks.get("sm_mhz") or 1965.0
-        peak = sm_count * 128 * sm_mhz * 1e6 / 1e12
+        issue_peak = sm_count * 128 * sm_mhz * 1e6 / 1e12
+        # measured integer peak (collatz_int_peak, after the timed region): the
+        # kernel mix's operations per SM clock, scaled to the clock sampled under load
+        ipk = {m: v.int_peak(m) for m in (1, 0)}
+        peak = ipk[1]["ops_per_clk_sm"] * sm_count * sm_mhz * 1e6 / 1e12
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * dev_s / args.steps, "higher_is_better": True,
@@ -545,15 +552,28 @@ def main():
                          "model": f"{ops_per_seed:.1f} algorithmic 32-bit ops per surviving seed "
                                   f"({OPS_JUMP} + {OPS_ODD} x {odd_per:.2f} odd runs + {OPS_EVEN} x "
                                   f"{even_per:.2f} even runs) x {res.seeds_checked} seeds per launch",
-                         "peak_basis": f"issue peak {sm_count} SMs x 4 SMSP x 32 lanes x {sm_mhz:.0f} MHz "
-                                       "(sampled median SM clock); no integer peak in MEASURED_PEAKS.json",
+                         "peak_basis": f"measured integer peak (collatz_int_peak mix 1: funnel shift, 3-input "
+                                       f"add, multiply-add chains on every SM): {ipk[1]['ops_per_clk_sm']:.1f} "
+                                       f"ops per SM clock x {sm_count} SMs x {sm_mhz:.0f} MHz (sampled median "
+                                       "SM clock); MEASURED_PEAKS.json has no integer peak",
+                         "int_peak_measured": {
+                             "mix1_kernel_mix": {"tops": ipk[1]["ops_per_s"] / 1e12,
+                                                 "ops_per_clk_sm": ipk[1]["ops_per_clk_sm"],
+                                                 "sm_mhz": ipk[1]["sm_mhz"]},
+                             "mix0_alu_only": {"tops": ipk[0]["ops_per_s"] / 1e12,
+                                               "ops_per_clk_sm": ipk[0]["ops_per_clk_sm"],
+                                               "sm_mhz": ipk[0]["sm_mhz"]}},
+                         "issue_peak": issue_peak,
+                         "frac_of_issue_peak": achieved / issue_peak,
                          # issue-slot utilisation of the same kernel, measured with ncu on a smaller
                          # launch of this workload: achieved/peak counts only the algorithmic ops, this
                          # counts every issued instruction (work distribution included)
                          "issue_slots_busy_ncu": K_RANGE_ISSUE_NCU[args.workload],
-                         "issue_basis": "sm__inst_issued.avg.pct_of_peak_sustained_active of one k_range "
-                                        "launch (profiles/k_range_2p38_block.md, "
-                                        "profiles/k_range_frontier_2p36.md)"},
+                         "alu_pipe_busy_ncu": K_RANGE_ALU_PIPE_NCU[args.workload],
+                         "issue_basis": "sm__inst_issued.avg.pct_of_peak_sustained_active and "
+                                        "sm__pipe_alu_cycles_active.avg.pct_of_peak_sustained_active of one "
+                                        "k_range launch (profiles/k_range_2p38_block.md, "
+                                        "profiles/k_range_frontier_2p36.md, profiles/int_peak_mixes.md)"},
             # request (32 B) + its work list: an aligned range of many blocks lowers to 55
             # 64-byte segments (5 kept mod-9 classes of the first and last block, 9 x 5 for the
             # blocks between)

@@ -79,6 +79,11 @@ class TuneResultC(C.Structure):
                 ("range_ms", C.c_float * 8), ("cases_ms", C.c_float * 8)]
 
 
+class IntPeakC(C.Structure):
+    _fields_ = [("ops", C.c_uint64), ("ms", C.c_float), ("mix", C.c_uint32), ("sm_count", C.c_uint32),
+                ("ops_per_s", C.c_double), ("sm_mhz", C.c_double), ("ops_per_clk_sm", C.c_double)]
+
+
 class ServerConfig(C.Structure):
     _fields_ = [("max_active", C.c_uint32), ("slice_items", C.c_uint32), ("hbm_reserve", C.c_uint64),
                 ("traj_batch_seeds", C.c_uint32), ("reserved", C.c_uint32 * 7)]
@@ -151,6 +156,7 @@ def lib() -> C.CDLL:
             "collatz_server_info": (C.c_int, [P, C.POINTER(ServerInfoC)]),
             "collatz_server_stop": (C.c_int, [P]),
             "collatz_autotune": (C.c_int, [P, C.c_uint32, C.POINTER(TuneResultC)]),
+            "collatz_int_peak": (C.c_int, [P, C.c_int, C.POINTER(IntPeakC)]),
             "collatz_combine_case_results": (C.c_int, [P, C.c_uint32, C.POINTER(CaseResultC)]),
             "collatz_run_cases": (C.c_int, [P, P, C.c_uint32, C.c_char_p, P, C.POINTER(CaseResultC),
                                             C.POINTER(C.c_uint32)]),
@@ -382,6 +388,14 @@ class Verifier:
         self._check(lib().collatz_autotune(self._h, flags, C.byref(r)), "autotune")
         return {"range_variant": r.range_variant, "cases_variant": r.cases_variant,
                 "range_ms": [x for x in r.range_ms if x >= 0], "cases_ms": [x for x in r.cases_ms if x >= 0]}
+
+    def int_peak(self, mix: int = 1) -> dict:
+        """Measured 32-bit integer peak of this device (collatz_int_peak): mix 0 is
+        ALU-pipe operations only, mix 1 two ALU operations to one multiply-add."""
+        r = IntPeakC()
+        self._check(lib().collatz_int_peak(self._h, mix, C.byref(r)), "int_peak")
+        return {"mix": r.mix, "ops": r.ops, "ms": r.ms, "ops_per_s": r.ops_per_s, "sm_mhz": r.sm_mhz,
+                "ops_per_clk_sm": r.ops_per_clk_sm, "sm_count": r.sm_count}
 
     # ---- cases mode ----
     def run_case(self, base, sigfig, threepower, number, doubleeven, numevens,

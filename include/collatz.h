@@ -380,6 +380,24 @@ typedef struct {
 #define COLLATZ_TUNE_NO_CACHE 0x4u /* do not record the choice in the cache */
 int collatz_autotune(collatz_ctx *ctx, uint32_t flags, collatz_tune_result *out);
 
+/* Measured 32-bit integer peak of the context's device (no counterpart in
+ * the reference; the roofline denominator of the integer-issue-bound
+ * kernels).  Every SM runs 8 blocks of 256 threads, each thread 8
+ * independent chains of dependent operations; the fastest of 3 timed
+ * launches after a warm-up is kept.  mix 0: funnel shift, 3-input add and
+ * 3-input logic op per link (ALU pipe only); mix 1: funnel shift, 3-input
+ * add and multiply-add per link (two ALU operations to one FMA-pipe
+ * multiply-add, the proportion of the run arithmetic).  About 0.2 s. */
+typedef struct {
+  uint64_t ops;          /* 32-bit operations of one launch */
+  float ms;              /* its CUDA-event time */
+  uint32_t mix, sm_count;
+  double ops_per_s;      /* whole device */
+  double sm_mhz;         /* SM clock during the launch (clock64 / global timer) */
+  double ops_per_clk_sm; /* ops_per_s / (sm_mhz x sm_count): scales to other clocks */
+} collatz_int_peak_t;
+int collatz_int_peak(collatz_ctx *ctx, int mix, collatz_int_peak_t *out);
+
 #ifdef __cplusplus
 }
 #endif
