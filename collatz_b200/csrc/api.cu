@@ -1056,7 +1056,8 @@ struct collatz_plan {
 // Checks that a batch uses one sieve (k, sign), fetches (or builds) its
 // tables and lowers every request into segments.
 static int range_lower_batch(collatz_ctx* c, const collatz_range* r, uint32_t n, RangeTables** T, uint32_t* k_out,
-                             bool* neg_out, std::vector<RangeSeg>& segs, unsigned long long& items) {
+                             bool* neg_out, std::vector<RangeSeg>& segs, unsigned long long& items,
+                             uint32_t* seed_bits) {
   const uint32_t k = r[0].k ? r[0].k : c->cfg.range_k;
   const bool neg = (r[0].flags & COLLATZ_RANGE_NEGATIVE) != 0;
   for (uint32_t i = 0; i < n; i++)  // one sieve (k, sign) per launch
@@ -1065,9 +1066,11 @@ static int range_lower_batch(collatz_ctx* c, const collatz_range* r, uint32_t n,
   if (k < 8 || k > 34) return COLLATZ_E_ARG;
   int rc = get_range_tables(c, k, T, neg);
   if (rc) return rc;
+  *seed_bits = 0;
   for (uint32_t i = 0; i < n; i++) {
     rc = lower_range(c, r[i], i, **T, segs, items);
     if (rc) return rc;
+    *seed_bits = std::max(*seed_bits, range_seed_bits(r[i]));
   }
   if (segs.empty()) {  // keep the kernel's segment search well-defined
     RangeSeg g{};
@@ -1094,8 +1097,10 @@ struct RangeBufs {
   unsigned long long* stats;
 };
 
-static RangeArgs range_args(collatz_ctx* c, const RangeTables& T, uint32_t k, bool neg, const RangeBufs& b) {
+static RangeArgs range_args(collatz_ctx* c, const RangeTables& T, uint32_t k, bool neg, const RangeBufs& b,
+                            uint32_t seed_bits) {
   RangeArgs a;
+  a.seed_bits = seed_bits;
   a.table = T.dev.table;
   a.k = k;
   a.segs = b.segs;
@@ -1139,8 +1144,8 @@ static bool range_stats_requested() {
 }
 
 static int plan_build(collatz_ctx* c, const collatz_range* r, uint32_t n, collatz_plan* p) {
-  uint32_t k = 0;
-  int rc = range_lower_batch(c, r, n, &p->T, &k, &p->negative, p->segs, p->items);
+  uint32_t k = 0, seed_bits = 0;
+  int rc = range_lower_batch(c, r, n, &p->T, &k, &p->negative, p->segs, p->items, &seed_bits);
   if (rc) return rc;
   p->n = n;
   CK(c, p->d_segs.ensure(sizeof(RangeSeg) * p->segs.size()));
@@ -1157,7 +1162,7 @@ static int plan_build(collatz_ctx* c, const collatz_range* r, uint32_t n, collat
                     p->h_recs.p, n, p->d_cursor.as<unsigned long long>(), p->d_widen.as<WidenEntry>(),
                     p->d_widen2.as<WidenEntry>(), p->d_wcount.as<uint32_t>(),
                     p->stats ? p->d_stats.as<unsigned long long>() : nullptr};
-  const RangeArgs a = range_args(c, *p->T, k, p->negative, b);
+  const RangeArgs a = range_args(c, *p->T, k, p->negative, b, seed_bits);
   cudaStream_t s = c->own_stream;
   CK(c, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   const cudaError_t e = range_enqueue(c, a, b, s);
@@ -1255,9 +1260,9 @@ extern "C" int collatz_verify_batch(collatz_ctx* c, const collatz_range* r, uint
   segs.clear();
   unsigned long long items = 0;
   RangeTables* T = nullptr;
-  uint32_t k = 0;
+  uint32_t k = 0, seed_bits = 0;
   bool neg = false;
-  int rc = range_lower_batch(c, r, n, &T, &k, &neg, segs, items);
+  int rc = range_lower_batch(c, r, n, &T, &k, &neg, segs, items, &seed_bits);
   if (rc) return rc;
   const size_t sb = sizeof(RangeSeg) * segs.size(), rb = sizeof(ReqRec) * n;
   CK(c, c->d_segs.ensure(sb));
@@ -1272,7 +1277,7 @@ extern "C" int collatz_verify_batch(collatz_ctx* c, const collatz_range* r, uint
   const RangeBufs b{c->d_segs.as<RangeSeg>(), (uint32_t)segs.size(), items, c->d_recs.as<ReqRec>(), c->h_recs.p, n,
                     c->d_rcursor.as<unsigned long long>(), c->d_widen.as<WidenEntry>(),
                     c->d_widen2.as<WidenEntry>(), c->d_wcount.as<uint32_t>(), nullptr};
-  const RangeArgs a = range_args(c, *T, k, neg, b);
+  const RangeArgs a = range_args(c, *T, k, neg, b, seed_bits);
   CK(c, cudaMemcpyAsync(c->d_segs.p, c->h_segs.p, sb, cudaMemcpyHostToDevice, c->stream));
   CK(c, cudaEventRecord(c->ev[2], c->stream));
   CK(c, range_enqueue(c, a, b, c->stream));

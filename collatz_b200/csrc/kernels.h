@@ -115,7 +115,14 @@ struct RangeArgs {
   uint32_t iter_cap;              // odd/even run pairs per seed before ERR_ITER_CAP
   uint32_t negative;              // 1: the negative-integer variant (a table built for it)
   unsigned long long* stats;      // diagnostics counters (stats variant only), may be null
+  uint32_t seed_bits;             // bit length of the launch's largest seed (0: not known)
 };
+// Variants 4 and 5 run the 64-bit body (variants 6 and 7) when every seed of
+// the launch lies below 2^RANGE_NARROW_MAX_BITS: its values then stay below
+// 2^59 for most steps.  For seeds from 2^52 on, the 128-bit body alone is
+// faster (measured on B200: 2^34 seeds at 2^51 take 5.20 ms with the 64-bit
+// body and 5.21 ms without; at 2^52, 5.29 ms and 5.21 ms).
+constexpr uint32_t RANGE_NARROW_MAX_BITS = 52;
 int range_variants();
 cudaError_t range_init();  // once per device, before the first launch
 // Diagnostics variant: counts run pairs, slow paths, replays, jumps, pops,

@@ -458,7 +458,7 @@ __device__ __forceinline__ bool expand_one(WT& W, const RangeArgs& A, const uint
   return true;
 }
 
-template <int R, int MINB, bool STATS = false, bool NEG = false, bool WIN = false>
+template <int R, int MINB, bool STATS = false, bool NEG = false, bool WIN = false, bool N64 = false>
 __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) {
   // diagnostics (STATS variant only): run pairs, excursion slow paths, replays, jumps, pops,
   // expansions, passes, offers; clock64 cycles per phase (lane 0)
@@ -570,6 +570,27 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
     }                                                                                \
   } while (0)
 
+// The value T^s(n) = v -/+ 1 at or above the excursion threshold window: keep
+// it as the seed's maximum when it is the largest so far.
+#define EXC_CANDIDATE()                                                                  \
+  do {                                                                                   \
+    if (STATS) c_slow++;                                                                 \
+    u32 xv_[4];                                                                          \
+    value_of<NEG>(v0, v1, v2, v3, xv_);                                                  \
+    bool take_ = !evalid;                                                                \
+    if (evalid)                                                                          \
+      take_ = lt96c(W.e[0][lane], W.e[1][lane], W.e[2][lane], xv_[0], xv_[1], xv_[2])    \
+                  ? (W.e[3][lane] <= xv_[3])                                             \
+                  : (W.e[3][lane] < xv_[3]);                                             \
+    if (take_) {                                                                         \
+      W.e[0][lane] = xv_[0];                                                             \
+      W.e[1][lane] = xv_[1];                                                             \
+      W.e[2][lane] = xv_[2];                                                             \
+      W.e[3][lane] = xv_[3];                                                             \
+      evalid = true;                                                                     \
+    }                                                                                    \
+  } while (0)
+
   if (STATS) t_mark = clock64();
   for (;;) {
     if (STATS) {
@@ -640,53 +661,84 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
           head += take;
         }
       }
+      // 64-bit body while every active lane's value is below 2^59: an odd run of at most 7
+      // steps multiplies by less than 2^5, so the value stays below 2^64 (a warp-uniform
+      // choice made again at every step; the 128-bit body below is the general one)
+      const bool narrow = N64 && !NEG && __all_sync(FULL, !active || (((v2 | v3) == 0) & (v1 < (1u << 27))));
       if (!active) continue;
-      {
-        // odd run capped at 7 steps (a longer run continues in the next pass, after an empty
-        // even run); 3^a from byte lookups in registers keeps shared memory off this path
+      u32 b;
+      bool fin;
+      if (N64 && !NEG && narrow) {
+        u64 v = ((u64)v1 << 32) | v0;
         const u32 a = ctz32(v0 | (1u << 7));
-        odd_run4(v0, v1, v2, v3, a, pow3_le7(a));
+        v = (v >> a) * pow3_le7(a);
         st += a;
         if (STATS) c_iter++;
-      }
-      // excursion / overflow gate: (v3:v2:v1) >= (0:gate) (T': >= gate - 1, since the
-      // value v + 1 has a window at most 1 above v's)
-      const u64 g_eff = NEG ? gate - (gate != 0) : gate;
-      if (!lt96c(v1, v2, v3, (u32)g_eff, (u32)(g_eff >> 32), 0u)) {
-        if (v3 >= OVF3) {
-          // the next odd run could leave 128 bits: re-run this seed with wider limbs
-          widen_seed(A, req, n0, n1, n2);
-          active = false;
-          continue;
-        }
-        // excursion candidate (bits 32..95 at or above the threshold)
-        if (STATS) c_slow++;
-        u32 xv[4];
-        value_of<NEG>(v0, v1, v2, v3, xv);
-        const u32 x0 = xv[0], x1 = xv[1], x2 = xv[2], x3 = xv[3];
-        bool take_it = !evalid;
-        if (evalid) take_it = lt96c(W.e[0][lane], W.e[1][lane], W.e[2][lane], x0, x1, x2) ? (W.e[3][lane] <= x3)
-                                                                                           : (W.e[3][lane] < x3);
-        if (take_it) {
-          W.e[0][lane] = x0;
-          W.e[1][lane] = x1;
-          W.e[2][lane] = x2;
-          W.e[3][lane] = x3;
-          evalid = true;
-        }
-      }
-      if (NEG) {
-        // t = u + 1 with a full carry (a low limb of all ones gives b = 31 below)
-        v0 += 1;
-        add_carry3(v1, v2, v3, v0 == 0);
+        v0 = (u32)v;
+        v1 = (u32)(v >> 32);
+        if ((v >> 32) >= gate) EXC_CANDIDATE();  // v2 = v3 = 0
+        const u64 x = v - 1;
+        b = ctz32((u32)x | 0x80000000u);
+        const u64 w = x >> b;
+        st += b;
+        fin = ((b != 0) & ((n2 != 0) | (w < (((u64)n1 << 32) | n0)))) | (st > ST_CAP);
+        const u64 y = fin ? x : w + 1;  // the finish reads v - 1; else the next state w + 1
+        v0 = (u32)y;
+        v1 = (u32)(y >> 32);
       } else {
-        v0 -= 1;  // v0 == 0 gives b == 0 below, and the borrow cancels against the +1
+        {
+          // odd run capped at 7 steps (a longer run continues in the next pass, after an empty
+          // even run); 3^a from byte lookups in registers keeps shared memory off this path
+          const u32 a = ctz32(v0 | (1u << 7));
+          odd_run4(v0, v1, v2, v3, a, pow3_le7(a));
+          st += a;
+          if (STATS) c_iter++;
+        }
+        // excursion / overflow gate: (v3:v2:v1) >= (0:gate) (T': >= gate - 1, since the
+        // value v + 1 has a window at most 1 above v's)
+        const u64 g_eff = NEG ? gate - (gate != 0) : gate;
+        if (!lt96c(v1, v2, v3, (u32)g_eff, (u32)(g_eff >> 32), 0u)) {
+          if (v3 >= OVF3) {
+            // the next odd run could leave 128 bits: re-run this seed with wider limbs
+            widen_seed(A, req, n0, n1, n2);
+            active = false;
+            continue;
+          }
+          EXC_CANDIDATE();  // bits 32..95 at or above the threshold
+        }
+        if (NEG) {
+          // t = u + 1 with a full carry (a low limb of all ones gives b = 31 below)
+          v0 += 1;
+          add_carry3(v1, v2, v3, v0 == 0);
+        } else {
+          v0 -= 1;  // v0 == 0 gives b == 0 below, and the borrow cancels against the +1
+        }
+        b = ctz32(v0 | 0x80000000u);
+        const u32 w0 = __funnelshift_r(v0, v1, b), w1 = __funnelshift_r(v1, v2, b);
+        const u32 w2 = __funnelshift_r(v2, v3, b), w3 = v3 >> b;
+        st += b;
+        fin = ((w3 == 0) & (b != 0) & lt96c(w0, w1, w2, n0, n1, n2)) | (st > ST_CAP);
+        if (fin) {
+          // the finish below reads v (the value before the even run)
+        } else if (NEG && (w3 == 0) & (w0 == n0) & (w1 == n1) & (w2 == n2)) {
+          // T': back at the seed -- it lies on a cycle and never descends (the minima 5, 17)
+          atomicAdd(&A.recs[req].failures, 1ull);
+          active = false;
+        } else if (NEG) {
+          // u = w - 1 (w >= 1)
+          v0 = w0 - 1;
+          v1 = w1 - (w0 == 0);
+          v2 = w2 - ((w0 | w1) == 0);
+          v3 = w3 - ((w0 | w1 | w2) == 0);
+        } else {
+          v0 = w0 + 1;
+          v1 = w1;
+          v2 = w2;
+          v3 = w3;
+          add_carry3(v1, v2, v3, (v0 == 0) & (b != 0));
+        }
       }
-      const u32 b = ctz32(v0 | 0x80000000u);
-      const u32 w0 = __funnelshift_r(v0, v1, b), w1 = __funnelshift_r(v1, v2, b);
-      const u32 w2 = __funnelshift_r(v2, v3, b), w3 = v3 >> b;
-      st += b;
-      if (((w3 == 0) & (b != 0) & lt96c(w0, w1, w2, n0, n1, n2)) | (st > ST_CAP)) {
+      if (fin) {
         if (st > ST_CAP) {
           atomicOr(&A.recs[req].errors, ERR_ITER_CAP);
           atomicAdd(&A.recs[req].failures, 1ull);
@@ -728,25 +780,10 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
         }
         active = false;
         // a lane with a pending offer waits for the next pass (its scratch is in use)
-      } else if (NEG && (w3 == 0) & (w0 == n0) & (w1 == n1) & (w2 == n2)) {
-        // T': back at the seed -- it lies on a cycle and never descends (the minima 5, 17)
-        atomicAdd(&A.recs[req].failures, 1ull);
-        active = false;
-      } else if (NEG) {
-        // u = w - 1 (w >= 1)
-        v0 = w0 - 1;
-        v1 = w1 - (w0 == 0);
-        v2 = w2 - ((w0 | w1) == 0);
-        v3 = w3 - ((w0 | w1 | w2) == 0);
-      } else {
-        v0 = w0 + 1;
-        v1 = w1;
-        v2 = w2;
-        v3 = w3;
-        add_carry3(v1, v2, v3, (v0 == 0) & (b != 0));
       }
     }
   }
+#undef EXC_CANDIDATE
 #undef POP_NEXT
   if (STATS && A.stats && lane == 0) {
     atomicAdd(&A.stats[8], t_offer);
@@ -861,7 +898,7 @@ __global__ void __launch_bounds__(128) k_range_wide(const WidenEntry* __restrict
 // ------------------------------------------------------------------
 // Launchers.
 // ------------------------------------------------------------------
-int range_variants() { return 6; }
+int range_variants() { return 8; }
 
 constexpr size_t RANGE_SMEM = sizeof(RangeWarp) * RWARPS;
 
@@ -870,17 +907,22 @@ cudaError_t launch_range_stats(const RangeArgs& a, u32 grid, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-// (run pairs per pass, minimum resident blocks per SM, 8-step window after the k-step jump)
-#define CZ_RANGE_VARIANTS(X) X(0, 1, 3, 0) X(1, 2, 3, 0) X(2, 2, 4, 0) X(3, 1, 4, 0) X(4, 2, 4, 1) X(5, 2, 3, 1)
+// (run pairs per pass, minimum resident blocks per SM, 8-step window after the k-step jump,
+// 64-bit body while the warp's values are below 2^59)
+#define CZ_RANGE_VARIANTS(X)                                                                   \
+  X(0, 1, 3, 0, 0) X(1, 2, 3, 0, 0) X(2, 2, 4, 0, 0) X(3, 1, 4, 0, 0) X(4, 2, 4, 1, 0) X(5, 2, 3, 1, 0) \
+  X(6, 2, 4, 1, 1) X(7, 2, 3, 1, 1)
 
 cudaError_t launch_range(const RangeArgs& a, int variant, u32 grid, cudaStream_t st) {
+  if (!a.negative && a.seed_bits && a.seed_bits <= RANGE_NARROW_MAX_BITS && (variant == 4 || variant == 5))
+    variant += 2;  // the same shape with the 64-bit body
   switch (variant) {
-#define X(id, rm, mb, win)                                                            \
-  case id:                                                                            \
-    if (a.negative)                                                                   \
-      k_range<rm, mb, false, true><<<grid, RWARPS * 32, RANGE_SMEM, st>>>(a);         \
-    else                                                                              \
-      k_range<rm, mb, false, false, win><<<grid, RWARPS * 32, RANGE_SMEM, st>>>(a);   \
+#define X(id, rm, mb, win, n64)                                                          \
+  case id:                                                                               \
+    if (a.negative)                                                                      \
+      k_range<rm, mb, false, true><<<grid, RWARPS * 32, RANGE_SMEM, st>>>(a);            \
+    else                                                                                 \
+      k_range<rm, mb, false, false, win, n64><<<grid, RWARPS * 32, RANGE_SMEM, st>>>(a); \
     break;
     CZ_RANGE_VARIANTS(X)
 #undef X
@@ -891,9 +933,10 @@ cudaError_t launch_range(const RangeArgs& a, int variant, u32 grid, cudaStream_t
 
 cudaError_t range_occupancy(int variant, int* bps) {
   switch (variant) {
-#define X(id, rm, mb, win) \
-  case id:                 \
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_range<rm, mb, false, false, win>, RWARPS * 32, RANGE_SMEM);
+#define X(id, rm, mb, win, n64) \
+  case id:                      \
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_range<rm, mb, false, false, win, n64>, RWARPS * 32, \
+                                                         RANGE_SMEM);
     CZ_RANGE_VARIANTS(X)
 #undef X
     default: return cudaErrorInvalidValue;
@@ -903,10 +946,10 @@ cudaError_t range_occupancy(int variant, int* bps) {
 // Opts every range kernel into RANGE_SMEM (> 48 KB) of dynamic shared memory.
 cudaError_t range_init() {
   cudaError_t e = cudaSuccess;
-#define X(id, rm, mb, win)                                                                                     \
-  if (e == cudaSuccess)                                                                                        \
-    e = cudaFuncSetAttribute(k_range<rm, mb, false, false, win>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
-                             (int)RANGE_SMEM);                                                                 \
+#define X(id, rm, mb, win, n64)                                                                                 \
+  if (e == cudaSuccess)                                                                                         \
+    e = cudaFuncSetAttribute(k_range<rm, mb, false, false, win, n64>,                                          \
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RANGE_SMEM);                    \
   if (e == cudaSuccess)                                                                                        \
     e = cudaFuncSetAttribute(k_range<rm, mb, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,         \
                              (int)RANGE_SMEM);

@@ -101,6 +101,18 @@ struct collatz_ctx {
 
 namespace cz {
 int set_cuda_error(collatz_ctx* c, cudaError_t e, const char* where);
+
+// Bit length of the largest seed of a range request (of its offset when it is empty).
+inline uint32_t range_seed_bits(const collatz_range& r) {
+  unsigned __int128 top = ((unsigned __int128)r.offset[1] << 64) | r.offset[0];
+  if (r.size) top += r.size - 1;
+  uint32_t b = 0;
+  while (top) {
+    top >>= 1;
+    b++;
+  }
+  return b;
+}
 int get_range_tables(collatz_ctx* c, uint32_t k, RangeTables** out, bool negative = false);
 int lower_range(collatz_ctx* c, const collatz_range& r, uint32_t req, const RangeTables& T,
                 std::vector<RangeSeg>& segs, unsigned long long& items);

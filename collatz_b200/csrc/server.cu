@@ -326,9 +326,11 @@ int launch_slice(collatz_server* s, int si) {
   S.finishing.clear();
   std::vector<RangeSeg> segs;
   unsigned long long slice_items = 0, budget = s->cfg.slice_items;
+  uint32_t seed_bits = 0;
   for (size_t i = 0; i < want.size(); i++) {
     const unsigned long long share = std::max<unsigned long long>(1, budget / (want.size() - i));
     const unsigned long long q = std::min(want[i].first, share);
+    if (q) seed_bits = std::max(seed_bits, range_seed_bits(want[i].second->q.range));
     take_items(want[i].second, q, segs, slice_items);
     budget -= std::min(budget, q);
     if (want[i].second->cursor == want[i].second->items) S.finishing.push_back(want[i].second);
@@ -358,6 +360,7 @@ int launch_slice(collatz_server* s, int si) {
   a.iter_cap = c->iter_cap;
   a.stats = nullptr;
   a.negative = neg ? 1u : 0u;
+  a.seed_bits = seed_bits;
   cudaStream_t st = s->sa;
   e = cudaMemcpyAsync(S.d_segs.p, S.h_segs.p, sb, cudaMemcpyHostToDevice, st);
   if (!e) e = cudaMemsetAsync(S.d_cursor.p, 0, sizeof(unsigned long long), st);

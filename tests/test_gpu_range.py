@@ -23,6 +23,7 @@ CASES = [
     ((1 << 60) + (3 << 34), 1 << 22, 34, True),  # frontier sieve (2 GiB bit array), aligned
     ((1 << 60) + (5 << 34) - 100000, 300000, 34, True),  # crosses a 2^34 block boundary
     ((1 << 60) + 77777, 1 << 21, 30, True),     # k = 30, unaligned
+    ((1 << 57) + 3, 1 << 20, 20, True),         # values cross 2^59 (the 64-bit body's limit) both ways
 ]
 
 
@@ -51,16 +52,16 @@ def test_range_matches_oracle(verifier, case):
     _cmp(g, o)
 
 
-VARIANT_CASES = [CASES[i] for i in (0, 3, 4, 5, 6, 7, 8, 10)]
+VARIANT_CASES = [CASES[i] for i in (0, 3, 4, 5, 6, 7, 8, 10, 12)]
 
 
-@pytest.mark.parametrize("variant", range(6))
+@pytest.mark.parametrize("variant", range(8))
 def test_range_variants_match_oracle(verifier, variant):
     """Every range-kernel variant (block shape; 4 and 5 add the 8-step window
     after the k-step jump) gives the oracle's results."""
     import collatz_b200 as cb
     from oracle import oracle as O
-    assert cb.lib().collatz_variant_count(1) == 6
+    assert cb.lib().collatz_variant_count(1) == 8
     v = verifier(26)
     v.set_variant(1, variant)
     try:
@@ -196,6 +197,26 @@ def test_window_variant_equals_plain(verifier, off, size, k):
     v = verifier(26, range_k=k)
     try:
         v.set_variant(1, 4)
+        w = v.verify_range(off, size, k)
+        v.set_variant(1, 2)
+        p = v.verify_range(off, size, k)
+    finally:
+        v.set_variant(1, 4)  # the default
+    assert (w.seeds_checked, w.failures, w.widened, w.errors) == (p.seeds_checked, p.failures, p.widened, p.errors)
+    assert (w.max_stopping_time, w.max_stopping_time_seed) == (p.max_stopping_time, p.max_stopping_time_seed)
+    assert (w.max_excursion, w.max_excursion_seed) == (p.max_excursion, p.max_excursion_seed)
+
+
+@pytest.mark.parametrize("off,size,k", [((1 << 40) + 777, 1 << 33, 24), ((1 << 56) + 12345, 1 << 30, 24),
+                                        ((1 << 58) + (7 << 24), 1 << 30, 24), ((1 << 63) + 5, 1 << 28, 24)])
+def test_narrow_variant_equals_plain(verifier, off, size, k):
+    """The 64-bit body (variant 6: taken while every active lane's value is below
+    2^59) leaves every output unchanged: at 2^40 nearly all steps take it, at
+    2^56-2^58 warps switch between the bodies, at 2^63 the seeds start above
+    its limit."""
+    v = verifier(26, range_k=k)
+    try:
+        v.set_variant(1, 6)
         w = v.verify_range(off, size, k)
         v.set_variant(1, 2)
         p = v.verify_range(off, size, k)
