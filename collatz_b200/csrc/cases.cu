@@ -44,7 +44,25 @@ struct CasesWarp {
   u32 thr[4];                       // excursion threshold (lower bound of the running max)
 };
 
-template <int ITERS, int REFILL_MIN, bool MULTI>
+// Exact excursion candidate x = v - 1 against the seed's maximum so far (or the
+// threshold): kept as the seed's maximum when it is at least as large.
+#define CASES_EXC_CANDIDATE()                                                                    \
+  do {                                                                                           \
+    const u32 x0 = v0 - 1, x1 = v1 - (v0 == 0), x2 = v2 - ((v0 | v1) == 0),                      \
+              x3 = v3 - ((v0 | v1 | v2) == 0);                                                   \
+    const u32* ref = evalid ? &W.lane[lane][4] : (MULTI ? &W.lane[lane][9] : W.thr);             \
+    const bool ge = !lt96(x1, x2, x3, ref[1], ref[2], ref[3]) &&                                 \
+                    !((x3 == ref[3]) & (x2 == ref[2]) & (x1 == ref[1]) & (x0 < ref[0]));         \
+    if (ge) {                                                                                    \
+      W.lane[lane][4] = x0;                                                                      \
+      W.lane[lane][5] = x1;                                                                      \
+      W.lane[lane][6] = x2;                                                                      \
+      W.lane[lane][7] = x3;                                                                      \
+      evalid = 1;                                                                                \
+    }                                                                                            \
+  } while (0)
+
+template <int ITERS, int REFILL_MIN, bool MULTI, bool N64 = false>
 __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
   __shared__ CasesWarp<MULTI> S[CWARPS];
   const u32 lane = lane_id();
@@ -275,62 +293,76 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
       for (int it = 0; it < ITERS; it++) {
 #pragma unroll
         for (int half = 0; half < 2; half++) {
-          // odd run; 3^a from registers.  The stopping time stops counting at the
-          // first descent (found) or after an overflow report (ovf: no maxima).
-          const u32 a = ctz32(v0 | (1u << 8));
-          odd_run4(v0, v1, v2, v3, a, pow3_le8(a));
-          st += a;
-          if ((((u64)v3 << 32) | v2) >= gate) {  // overflow or excursion candidate (rare)
-            if (v3 >= 16u) {  // v >= 2^100 (cu:295, 334); search3 tests > on the second (cu:702)
-              const bool o = !(half == 1 && cpu && v3 == 16u && (v0 | v1 | v2) == 0u);
-              if (o) {
-                const ull i = atomicAdd(A.overflow_count, 1ull);
-                if (i < A.overflow_cap) {
-                  A.overflow[4 * i + 0] = n0;
-                  A.overflow[4 * i + 1] = n1;
-                  A.overflow[4 * i + 2] = n2;
-                  A.overflow[4 * i + 3] = MULTI ? hline : 0u;
+          // 64-bit body while every lane of the group is below 2^59: an odd run of at most 8
+          // steps multiplies by less than 2^5, so the value stays below 2^64 (the choice is
+          // the same for all lanes that run this step together; lanes done have left the loop)
+          const bool narrow = N64 && __all_sync(__activemask(), ((v2 | v3) == 0) & (v1 < (1u << 27)));
+          if (N64 && narrow) {
+            u64 v = ((u64)v1 << 32) | v0;
+            const u32 a = ctz32(v0 | (1u << 8));
+            v = (v >> a) * pow3_le8(a);
+            st += a;
+            v0 = (u32)v;
+            v1 = (u32)(v >> 32);
+            // (v3:v2) = 0 reaches the gate only when it is 0: no overflow, and the threshold
+            // is below 2^64 while the seed still counts -- an excursion candidate
+            if (gate == 0) CASES_EXC_CANDIDATE();
+            const u64 x = v - 1;
+            const u32 b = ctz32((u32)x | 0x80000000u);
+            const u64 w = x >> b;
+            if (!(found | ovf) & (b != 0) & ((n2 != 0) | (w < (((u64)n1 << 32) | n0)))) {
+              sig = st + first_below((u32)x, (u32)(x >> 32), 0u, 0u, n0, n1, n2, nbl);
+              found = 1;
+              gate = OVF_TOP;
+            }
+            st += b;
+            const u64 y = w + 1;
+            v0 = (u32)y;
+            v1 = (u32)(y >> 32);
+          } else {
+            // odd run; 3^a from registers.  The stopping time stops counting at the
+            // first descent (found) or after an overflow report (ovf: no maxima).
+            const u32 a = ctz32(v0 | (1u << 8));
+            odd_run4(v0, v1, v2, v3, a, pow3_le8(a));
+            st += a;
+            if ((((u64)v3 << 32) | v2) >= gate) {  // overflow or excursion candidate (rare)
+              if (v3 >= 16u) {  // v >= 2^100 (cu:295, 334); search3 tests > on the second (cu:702)
+                const bool o = !(half == 1 && cpu && v3 == 16u && (v0 | v1 | v2) == 0u);
+                if (o) {
+                  const ull i = atomicAdd(A.overflow_count, 1ull);
+                  if (i < A.overflow_cap) {
+                    A.overflow[4 * i + 0] = n0;
+                    A.overflow[4 * i + 1] = n1;
+                    A.overflow[4 * i + 2] = n2;
+                    A.overflow[4 * i + 3] = MULTI ? hline : 0u;
+                  }
+                  if (MULTI) atomicAdd(&A.rec[hline].items_done, 1ull);  // the line's overflow reports
+                  ovf = 1;
+                  gate = OVF_TOP;
+                  v0 = 2;
+                  v1 = v2 = v3 = 0;
                 }
-                if (MULTI) atomicAdd(&A.rec[hline].items_done, 1ull);  // the line's overflow reports
-                ovf = 1;
-                gate = OVF_TOP;
-                v0 = 2;
-                v1 = v2 = v3 = 0;
               }
+              if (!found && !ovf && (((u64)v3 << 32) | v2) >= thr_top) CASES_EXC_CANDIDATE();
             }
-            if (!found && !ovf && (((u64)v3 << 32) | v2) >= thr_top) {
-              // exact excursion candidate x = v - 1 against the seed max / threshold
-              const u32 x0 = v0 - 1, x1 = v1 - (v0 == 0), x2 = v2 - ((v0 | v1) == 0),
-                        x3 = v3 - ((v0 | v1 | v2) == 0);
-              const u32* ref = evalid ? &W.lane[lane][4] : (MULTI ? &W.lane[lane][9] : W.thr);
-              const bool ge = !lt96(x1, x2, x3, ref[1], ref[2], ref[3]) &&
-                              !((x3 == ref[3]) & (x2 == ref[2]) & (x1 == ref[1]) & (x0 < ref[0]));
-              if (ge) {
-                W.lane[lane][4] = x0;
-                W.lane[lane][5] = x1;
-                W.lane[lane][6] = x2;
-                W.lane[lane][7] = x3;
-                evalid = 1;
-              }
+            // even run
+            v0 -= 1;
+            const u32 b = ctz32(v0 | 0x80000000u);
+            const u32 w0 = __funnelshift_r(v0, v1, b), w1 = __funnelshift_r(v1, v2, b);
+            const u32 w2 = __funnelshift_r(v2, v3, b), w3 = v3 >> b;
+            if (!(found | ovf) & (b != 0) & (w3 == 0) & lt96c(w0, w1, w2, n0, n1, n2)) {
+              // first descent inside this run: smallest i with (v-1) >> i < n
+              sig = st + first_below(v0, v1, v2, v3, n0, n1, n2, nbl);
+              found = 1;
+              gate = OVF_TOP;
             }
+            st += b;
+            v0 = w0 + 1;
+            v1 = w1;
+            v2 = w2;
+            v3 = w3;
+            add_carry3(v1, v2, v3, (v0 == 0) & (b != 0));  // carry of the +1 (cu:310-318)
           }
-          // even run
-          v0 -= 1;
-          const u32 b = ctz32(v0 | 0x80000000u);
-          const u32 w0 = __funnelshift_r(v0, v1, b), w1 = __funnelshift_r(v1, v2, b);
-          const u32 w2 = __funnelshift_r(v2, v3, b), w3 = v3 >> b;
-          if (!(found | ovf) & (b != 0) & (w3 == 0) & lt96c(w0, w1, w2, n0, n1, n2)) {
-            // first descent inside this run: smallest i with (v-1) >> i < n
-            sig = st + first_below(v0, v1, v2, v3, n0, n1, n2, nbl);
-            found = 1;
-            gate = OVF_TOP;
-          }
-          st += b;
-          v0 = w0 + 1;
-          v1 = w1;
-          v2 = w2;
-          v3 = w3;
-          add_carry3(v1, v2, v3, (v0 == 0) & (b != 0));  // carry of the +1 (cu:310-318)
         }
         hash ^= v0;  // cu:359
         iters++;
@@ -374,24 +406,31 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
   }
 }
 
+#undef CASES_EXC_CANDIDATE
+
 // ------------------------------------------------------------------
 // Host launcher.
 // ------------------------------------------------------------------
 
-template <int I, int R>
+template <int I, int R, bool N64 = false>
 static cudaError_t launch_cases_t(const CasesArgs& a, u32 grid, cudaStream_t st) {
-  if (a.multi) k_cases<I, R, true><<<grid, CWARPS * 32, 0, st>>>(a);
-  else k_cases<I, R, false><<<grid, CWARPS * 32, 0, st>>>(a);
+  if (a.multi) k_cases<I, R, true, N64><<<grid, CWARPS * 32, 0, st>>>(a);
+  else k_cases<I, R, false, N64><<<grid, CWARPS * 32, 0, st>>>(a);
   return cudaGetLastError();
 }
 
-int cases_variants() { return 4; }
+// Variants: checkpoints per pass and refill threshold; variant 4 adds the 64-bit body
+// (for N <= 52; variant 3 above).
+int cases_variants() { return 5; }
 
 cudaError_t launch_cases(const CasesArgs& a, int variant, u32 grid, cudaStream_t st) {
+  // seeds n = base | a << (N - A) lie below 2^N (A = 10): above 2^52 the 128-bit body alone is faster
+  if (variant == 4 && a.mbi + 10u > RANGE_NARROW_MAX_BITS) variant = 3;
   switch (variant) {
     case 0: return launch_cases_t<1, 1>(a, grid, st);
     case 1: return launch_cases_t<2, 4>(a, grid, st);
     case 2: return launch_cases_t<2, 8>(a, grid, st);
+    case 4: return launch_cases_t<4, 8, true>(a, grid, st);
     default: return launch_cases_t<4, 8>(a, grid, st);
   }
 }
@@ -402,6 +441,7 @@ static cudaError_t occupancy_t(int variant, int* bps) {
     case 0: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_cases<1, 1, M>, CWARPS * 32, 0);
     case 1: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_cases<2, 4, M>, CWARPS * 32, 0);
     case 2: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_cases<2, 8, M>, CWARPS * 32, 0);
+    case 4: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_cases<4, 8, M, true>, CWARPS * 32, 0);
     default: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_cases<4, 8, M>, CWARPS * 32, 0);
   }
 }

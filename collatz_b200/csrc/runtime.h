@@ -80,7 +80,7 @@ struct collatz_ctx {
   cudaStream_t own_stream = nullptr, stream = nullptr, copy_stream = nullptr;
   cz::CaseTables ct;
   std::map<uint32_t, cz::RangeTables> rt;
-  int cases_variant = 3, range_variant = 4;
+  int cases_variant = 4, range_variant = 4;
   uint32_t iter_cap = 1u << 16;
   // scratch for the synchronous calls
   cz::DevBuf d_rec, d_counter, d_overflow, d_ovcount, d_pairs[2], d_segs, d_widen, d_widen2, d_wcount;

@@ -94,12 +94,12 @@ def test_case_maxima_match_oracle(verifier, oracle_tables, n, tup):
     assert (r.max_excursion, r.max_excursion_seed) == (o.max_exc, o.max_exc_seed)
 
 
-@pytest.mark.parametrize("variant", range(4))
+@pytest.mark.parametrize("variant", range(5))
 def test_every_cases_variant_matches_reference(verifier, oracle_tables, variant):
     """Each cases-kernel variant reproduces the reference's pair batches
     (overflow reports included), search2 pairs, and the oracle's maxima."""
     import collatz_b200 as cb
-    assert cb.lib().collatz_variant_count(0) == 4
+    assert cb.lib().collatz_variant_count(0) == 5
     v = verifier(45)
     v.set_variant(0, variant)
     try:
@@ -119,8 +119,8 @@ def test_every_cases_variant_matches_reference(verifier, oracle_tables, variant)
         assert (r.max_stopping_time, r.max_stopping_time_seed) == (o.max_st, o.max_st_seed)
         assert (r.max_excursion, r.max_excursion_seed) == (o.max_exc, o.max_exc_seed)
     finally:  # back to the default variant
-        v.set_variant(0, 3)
-        verifier(36).set_variant(0, 3)
+        v.set_variant(0, 4)
+        verifier(36).set_variant(0, 4)
 
 
 def test_pair_maxima_match_oracle(verifier, oracle_tables):

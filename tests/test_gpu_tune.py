@@ -29,7 +29,7 @@ def test_every_variant_same_results(verifier):
         assert ref_case is None or got == ref_case, var
         ref_case = got
     v.set_variant(1, 4)  # the defaults
-    v.set_variant(0, 3)
+    v.set_variant(0, 4)
 
 
 def test_autotune_records_and_reuses(tmp_path, monkeypatch):
