@@ -48,7 +48,7 @@ UNIT = "seeds/s"
 # shifts, increment with carry, descent test).
 OPS_JUMP, OPS_ODD, OPS_EVEN = 16, 14, 12
 # DRAM bytes (read + write) of one k_range launch, measured with ncu.
-K_RANGE_DRAM_BYTES = 5.366272e6 + 0.226048e6
+K_RANGE_DRAM_BYTES = 5.349376e6 + 0.220928e6
 # Frontier (k = 34): every block of 2^34 seeds streams the 5 mod-9 classes
 # of the 2.43 GB survivor table that it keeps; ncu on a 4-block launch read
 # 5.421552640e9 and wrote 9.596928e6 bytes, so traffic per launch = blocks x
@@ -58,8 +58,8 @@ K_RANGE_FRONTIER_DRAM_BYTES_PER_BLOCK = (5.421552640e9 + 9.596928e6) / 4
 # block, k = 24; 2^36 frontier, k = 34).  The ALU pipe is the one that
 # saturates first for this instruction mix (collatz_int_peak mix 1 reaches
 # its limit at 77 % of the issue slots).
-K_RANGE_ISSUE_NCU = {"block": 0.6703, "frontier": 0.7416}
-K_RANGE_ALU_PIPE_NCU = {"block": 0.5913, "frontier": 0.6560}
+K_RANGE_ISSUE_NCU = {"block": 0.6709, "frontier": 0.7416}
+K_RANGE_ALU_PIPE_NCU = {"block": 0.6029, "frontier": 0.6560}
 
 
 def dist_env():
@@ -380,8 +380,8 @@ def run_served(v, capacity: float, load: float = 0.7, duration: float = 1.0, see
                           and (exc == r.traj_excursion).all())
     t_plain = time.perf_counter() - t1
     sub_seeds = sum(a[1] for k, a in sub if k == "range")
-    return {"workload": f"Poisson arrivals for {duration:.1f} s at {load:.2f} x the plain kernel's "
-                        "seeds/s; 70% ranges (log-uniform 2^16..2^32 seeds, offsets uniform [2^40, 2^64)), "
+    return {"workload": f"Poisson arrivals for {duration:.1f} s at {load:.2f} x the batched "
+                        f"configuration's capacity ({capacity:.3g} seeds/s, measured in the same run); 70% ranges (log-uniform 2^16..2^32 seeds, offsets uniform [2^40, 2^64)), "
                         "30% trajectory queries (log-uniform 1..65536 seeds of 64..256 bits); numpy "
                         f"default_rng({seed})",
             "requests": n, "lambda_per_s": lam, "range_seeds": range_seeds, "traj_seeds": traj_seeds,
@@ -592,14 +592,18 @@ def main():
                                               f"{cdt:.1f} s (oracle run-length loop after cu:684-715, "
                                               f"{nthreads} threads)"}
         if world == 1 and not args.no_extras and args.workload == "block":
-            for key, fn in (("batched", lambda: run_batched(v)),
-                            ("served", lambda: run_served(v, value, load=args.served_load,
-                                                          duration=args.served_duration)),
-                            ("cases", run_cases)):
+            def extra(fn):
                 try:
-                    line[key] = fn()
+                    return fn()
                 except Exception as e:  # noqa: BLE001 -- the headline line is printed regardless
-                    line[key] = {"error": f"{type(e).__name__}: {e}"}
+                    return {"error": f"{type(e).__name__}: {e}"}
+            line["batched"] = extra(lambda: run_batched(v))
+            # served load: a fraction of the batched configuration's capacity (requests of the
+            # same offsets and sizes), else of the headline block's
+            cap = line["batched"].get("batched_seeds_per_s") or value
+            line["served"] = extra(lambda: run_served(v, cap, load=args.served_load,
+                                                      duration=args.served_duration))
+            line["cases"] = extra(run_cases)
         print(json.dumps(line), flush=True)
     plan.close()
     v.close()
