@@ -1212,10 +1212,10 @@ extern "C" int collatz_plan_results(collatz_plan* p, collatz_range_result* out) 
     CK(c, cudaMemcpy(st8, p->d_stats.p, sizeof st8, cudaMemcpyDeviceToHost));
     fprintf(stderr,
             "collatz range stats: run_pairs=%llu slow_e=%llu replays=%llu jumps=%llu pops=%llu expansions=%llu "
-            "passes=%llu offers=%llu warp_cycles: offers=%llu refill=%llu lanes=%llu (refill: wait=%llu "
-            "stage=%llu thresholds=%llu)\n",
-            st8[0], st8[1], st8[2], st8[3], st8[4], st8[5], st8[6], st8[7], st8[8], st8[9], st8[10], st8[11],
-            st8[12], st8[13]);
+            "passes=%llu offers=%llu windows=%llu pairs_64bit=%llu warp_cycles: offers=%llu refill=%llu "
+            "lanes=%llu (refill: wait=%llu stage=%llu thresholds=%llu)\n",
+            st8[0], st8[1], st8[2], st8[3], st8[4], st8[5], st8[6], st8[7], st8[14], st8[15], st8[8], st8[9],
+            st8[10], st8[11], st8[12], st8[13]);
   }
   for (uint32_t i = 0; i < p->n; i++) {
     rec_to_range_result(h[i], &out[i]);

@@ -125,8 +125,10 @@ struct RangeArgs {
 constexpr uint32_t RANGE_NARROW_MAX_BITS = 52;
 int range_variants();
 cudaError_t range_init();  // once per device, before the first launch
-// Diagnostics variant: counts run pairs, slow paths, replays, jumps, pops,
-// expansions, pop-block passes and offers into a.stats[0..7].
+// Diagnostics variant (the default shape with 3 blocks per SM): counts run
+// pairs, slow paths, replays, jumps, pops, expansions, pop-block passes and
+// offers into a.stats[0..7], clock64 cycles per phase into [8..13], 8-step
+// windows taken into [14] and run pairs on the 64-bit body into [15].
 cudaError_t launch_range_stats(const RangeArgs& a, uint32_t grid, cudaStream_t st);
 cudaError_t launch_range(const RangeArgs& a, int variant, uint32_t grid, cudaStream_t st);
 cudaError_t range_occupancy(int variant, int* blocks_per_sm);

@@ -233,7 +233,7 @@ __device__ __forceinline__ void stage_next(WT& W, uint4* dst, const RangeArgs& A
 // set up by the k-step jump and by an exact replay of the first k steps.
 struct ExpandStats {
   ull t_wait = 0, t_stage = 0, t_thr = 0, t_sub = 0;
-  u32 c_exp = 0, c_jump = 0, c_replay = 0;
+  u32 c_exp = 0, c_jump = 0, c_replay = 0, c_win = 0;
 };
 
 // Expands the staged item into the warp's seed queue (W.qa, W.qb from
@@ -394,6 +394,7 @@ __device__ __forceinline__ bool expand_one(WT& W, const RangeArgs& A, const uint
               V2 = y2;
               V3 = y3;
               s0 = k + 8u;
+              if (STATS) X.c_win++;
             }
           }
           if (STATS) X.c_jump++;
@@ -458,11 +459,43 @@ __device__ __forceinline__ bool expand_one(WT& W, const RangeArgs& A, const uint
   return true;
 }
 
+// Offers of several pending lanes (all lanes call this together): a value that
+// another pending lane of the same request beats -- larger, or equal with a
+// smaller seed -- cannot be the request's maximum, so its bit is dropped and
+// only the best of each request is offered.  Kept out of line: it runs in few
+// passes, and inlined it costs the lane loop registers.
+__device__ __noinline__ u32 drop_dominated(RangeWarp& W, u32 lane, u32 pend, u32 pm) {
+  const u32 m1 = __ballot_sync(FULL, pend & 1u), m2 = __ballot_sync(FULL, pend & 2u);
+  __syncwarp();
+  if (pend) {
+    const u32 rq = W.c[4][lane], s0 = W.c[1][lane], s1 = W.c[2][lane], s2 = W.c[3][lane];
+    for (u32 m = pm & ~(1u << lane); m; m &= m - 1) {
+      const u32 j = __ffs(m) - 1;
+      if (W.c[4][j] != rq) continue;
+      const u32 t0 = W.c[1][j], t1 = W.c[2][j], t2 = W.c[3][j];
+      const bool j_smaller = (t2 != s2) ? (t2 < s2) : ((t1 != s1) ? (t1 < s1) : (t0 < s0));
+      if ((pend & 1u) && ((m1 >> j) & 1u)) {
+        const u32 sj = W.c[0][j], si = W.c[0][lane];
+        if (sj > si || (sj == si && j_smaller)) pend &= ~1u;
+      }
+      if ((pend & 2u) && ((m2 >> j) & 1u)) {
+        int c = 0;  // E_j against this lane's E, from the top limb
+#pragma unroll
+        for (int i = 3; i >= 0; i--)
+          if (c == 0) c = (W.pe[i][j] > W.pe[i][lane]) ? 1 : ((W.pe[i][j] < W.pe[i][lane]) ? -1 : 0);
+        if (c > 0 || (c == 0 && j_smaller)) pend &= ~2u;
+      }
+    }
+  }
+  __syncwarp();
+  return pend;
+}
+
 template <int R, int MINB, bool STATS = false, bool NEG = false, bool WIN = false, bool N64 = false>
 __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) {
   // diagnostics (STATS variant only): run pairs, excursion slow paths, replays, jumps, pops,
   // expansions, passes, offers; clock64 cycles per phase (lane 0)
-  u32 c_iter = 0, c_slow = 0, c_pop = 0, c_blk = 0, c_offer = 0;
+  u32 c_iter = 0, c_slow = 0, c_pop = 0, c_blk = 0, c_offer = 0, c_narrow = 0;
   ull t_offer = 0, t_refill = 0, t_lanes = 0, t_mark = 0;
   ExpandStats X;
   extern __shared__ __align__(16) unsigned char range_smem[];
@@ -601,31 +634,39 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
     }
     // ---- warp-synchronous part: offers of finished seeds (rare), refill, exit ----
     u32 pm = __ballot_sync(FULL, pend != 0);
-    while (pm) {
-      const u32 leader = __ffs(pm) - 1;
-      const u32 lp = __shfl_sync(FULL, pend, leader), lreq = W.c[4][leader];
-      if (lane == leader) {
-        const u32 seed[4] = {W.c[1][lane], W.c[2][lane], W.c[3][lane], 0};
-        if (STATS) c_offer++;
-        if (pend & 1u) rec_offer_st(A.recs + lreq, W.c[0][lane], seed);
-        if (pend & 2u) {
-          const u32 e4[4] = {W.pe[0][lane], W.pe[1][lane], W.pe[2][lane], W.pe[3][lane]};
-          rec_offer_e<4>(A.recs + lreq, e4, seed);
-        }
-        pend = 0;
+    if (pm) {  // offers (rare)
+      if (pm & (pm - 1)) {
+        // several pending lanes (a warp's first seeds all finish under zero thresholds):
+        // offer only the best of each request
+        pend = drop_dominated(W, lane, pend, pm);
+        pm = __ballot_sync(FULL, pend != 0);
       }
-      __syncwarp();
-      if (lreq == w_req) {  // an offered value is a lower bound of the request's maximum
-        if (lp & 1u) w_thr_st = max(w_thr_st, W.c[0][leader]);
-        if (lp & 2u) {
-          const u32 e1 = W.pe[1][leader], e2 = W.pe[2][leader], e3 = W.pe[3][leader];
-          w_gate = max(w_gate, gate_window(e1, e2, e3));
-          const u32 t = e3 ? e3 : (e2 ? e2 : e1);
-          const u32 bl = t ? (e3 ? 96u : (e2 ? 64u : 32u)) + 32u - __clz(t) : 0u;
-          if (lane == 0) W.thr_bl = max(W.thr_bl, bl > 0 ? bl - 1 : 0u);
+      while (pm) {
+        const u32 leader = __ffs(pm) - 1;
+        const u32 lp = __shfl_sync(FULL, pend, leader), lreq = W.c[4][leader];
+        if (lane == leader) {
+          const u32 seed[4] = {W.c[1][lane], W.c[2][lane], W.c[3][lane], 0};
+          if (STATS) c_offer++;
+          if (pend & 1u) rec_offer_st(A.recs + lreq, W.c[0][lane], seed);
+          if (pend & 2u) {
+            const u32 e4[4] = {W.pe[0][lane], W.pe[1][lane], W.pe[2][lane], W.pe[3][lane]};
+            rec_offer_e<4>(A.recs + lreq, e4, seed);
+          }
+          pend = 0;
         }
+        __syncwarp();
+        if (lreq == w_req) {  // an offered value is a lower bound of the request's maximum
+          if (lp & 1u) w_thr_st = max(w_thr_st, W.c[0][leader]);
+          if (lp & 2u) {
+            const u32 e1 = W.pe[1][leader], e2 = W.pe[2][leader], e3 = W.pe[3][leader];
+            w_gate = max(w_gate, gate_window(e1, e2, e3));
+            const u32 t = e3 ? e3 : (e2 ? e2 : e1);
+            const u32 bl = t ? (e3 ? 96u : (e2 ? 64u : 32u)) + 32u - __clz(t) : 0u;
+            if (lane == 0) W.thr_bl = max(W.thr_bl, bl > 0 ? bl - 1 : 0u);
+          }
+        }
+        pm &= pm - 1;
       }
-      pm &= pm - 1;
     }
     if (STATS) {
       const ull now = clock64();
@@ -673,7 +714,10 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
         const u32 a = ctz32(v0 | (1u << 7));
         v = (v >> a) * pow3_le7(a);
         st += a;
-        if (STATS) c_iter++;
+        if (STATS) {
+          c_iter++;
+          c_narrow++;
+        }
         v0 = (u32)v;
         v1 = (u32)(v >> 32);
         if ((v >> 32) >= gate) EXC_CANDIDATE();  // v2 = v3 = 0
@@ -794,14 +838,14 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
     atomicAdd(&A.stats[13], X.t_thr);
   }
   if (STATS && A.stats) {
-    u32 c[8] = {c_iter, c_slow, X.c_replay, X.c_jump, c_pop, X.c_exp, c_blk, c_offer};
+    u32 c[10] = {c_iter, c_slow, X.c_replay, X.c_jump, c_pop, X.c_exp, c_blk, c_offer, X.c_win, c_narrow};
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
+    for (int i = 0; i < 10; i++) {
       u32 x = c[i];
       if (i == 5 || i == 6) x = (lane == 0) ? x : 0u;  // warp-uniform counters
 #pragma unroll
       for (u32 d = 16; d; d >>= 1) x += __shfl_xor_sync(FULL, x, d);
-      if (lane == 0) atomicAdd(&A.stats[i], (ull)x);
+      if (lane == 0) atomicAdd(&A.stats[i < 8 ? i : i + 6], (ull)x);  // windows, 64-bit pairs: [14], [15]
     }
   }
   if (lane == 0 && w_req != 0xFFFFFFFFu) {
@@ -903,7 +947,7 @@ int range_variants() { return 8; }
 constexpr size_t RANGE_SMEM = sizeof(RangeWarp) * RWARPS;
 
 cudaError_t launch_range_stats(const RangeArgs& a, u32 grid, cudaStream_t st) {
-  k_range<2, 3, true><<<grid, RWARPS * 32, RANGE_SMEM, st>>>(a);
+  k_range<2, 3, true, false, true, true><<<grid, RWARPS * 32, RANGE_SMEM, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -956,7 +1000,8 @@ cudaError_t range_init() {
   CZ_RANGE_VARIANTS(X)
 #undef X
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_range<2, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RANGE_SMEM);
+    e = cudaFuncSetAttribute(k_range<2, 3, true, false, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)RANGE_SMEM);
   return e;
 }
 
