@@ -44,6 +44,37 @@ struct CasesWarp {
   u32 thr[4];                       // excursion threshold (lower bound of the running max)
 };
 
+// Offers of several pending lanes of one request (all lanes call this
+// together; lane slots [0] sigma, [1..3] seed, [4..7] excursion): a value that
+// another pending lane beats -- larger, or equal with a smaller seed -- cannot
+// be the maximum, so its bit is dropped.  A warp's first seeds all finish
+// under zero thresholds.  Kept out of line: it runs in few passes.
+__device__ __noinline__ u32 cases_drop_dominated(u32 (*L)[8], u32 lane, u32 pend, u32 pm) {
+  const u32 m1 = __ballot_sync(FULL, pend & 1u), m2 = __ballot_sync(FULL, pend & 2u);
+  __syncwarp();
+  if (pend) {
+    const u32 s0 = L[lane][1], s1 = L[lane][2], s2 = L[lane][3];
+    for (u32 m = pm & ~(1u << lane); m; m &= m - 1) {
+      const u32 j = __ffs(m) - 1;
+      const u32 t0 = L[j][1], t1 = L[j][2], t2 = L[j][3];
+      const bool j_smaller = (t2 != s2) ? (t2 < s2) : ((t1 != s1) ? (t1 < s1) : (t0 < s0));
+      if ((pend & 1u) && ((m1 >> j) & 1u)) {
+        const u32 sj = L[j][0], si = L[lane][0];
+        if (sj > si || (sj == si && j_smaller)) pend &= ~1u;
+      }
+      if ((pend & 2u) && ((m2 >> j) & 1u)) {
+        int c = 0;  // E_j against this lane's E, from the top limb
+#pragma unroll
+        for (int i = 7; i >= 4; i--)
+          if (c == 0) c = (L[j][i] > L[lane][i]) ? 1 : ((L[j][i] < L[lane][i]) ? -1 : 0);
+        if (c > 0 || (c == 0 && j_smaller)) pend &= ~2u;
+      }
+    }
+  }
+  __syncwarp();
+  return pend;
+}
+
 // Exact excursion candidate x = v - 1 against the seed's maximum so far (or the
 // threshold): kept as the seed's maximum when it is at least as large.
 #define CASES_EXC_CANDIDATE()                                                                    \
@@ -92,6 +123,12 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
     // ---- offers of finished seeds, one lane at a time (bounded locks) ----
     {
       u32 pm = __ballot_sync(FULL, pend != 0);
+      if constexpr (!MULTI) {
+        if (pm & (pm - 1)) {  // several pending lanes of the one request: offer only the best
+          pend = cases_drop_dominated(W.lane, lane, pend, pm);
+          pm = __ballot_sync(FULL, pend != 0);
+        }
+      }
       while (pm) {
         const u32 leader = __ffs(pm) - 1;
         if (lane == leader) {
