@@ -414,7 +414,7 @@ def main():
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched and served measurements (run at N = 1 only)")
     ap.add_argument("--served-load", type=float, default=0.7)
-    ap.add_argument("--served-duration", type=float, default=1.0)
+    ap.add_argument("--served-duration", type=float, default=2.0)
     ap.add_argument("--variant", type=int, default=None)
     args = ap.parse_args()
     if args.impl == "reference":
