@@ -67,3 +67,11 @@ def test_step1_pairs_layout():
     for bi, base, number in leaves:
         assert base < (1 << mbi) and base % 2 == 1
         assert 0 <= bi < 16
+
+
+def test_int_peak_rejects_null_arguments():
+    """collatz_int_peak validates its arguments before touching a device."""
+    import collatz_b200 as cb
+    out = cb.IntPeakC()
+    assert cb.lib().collatz_int_peak(None, 1, ctypes.byref(out)) == cb.E_ARG
+    assert cb.lib().collatz_int_peak(None, 1, None) == cb.E_ARG
