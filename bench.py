@@ -367,11 +367,14 @@ def run_served(v, capacity: float, load: float = 0.7, duration: float = 1.0, see
     lat_t = np.array([r.latency_s for r, (k, _) in zip(resps, reqs) if k == "traj"]) * 1e3
     range_seeds = sum(a[1] for k, a in reqs if k == "range")
     traj_seeds = sum(len(a) for k, a in reqs if k == "traj")
-    # plain path: the first plain_sample requests one at a time
-    sub = reqs[:plain_sample]
+    # plain path: plain_sample requests spread evenly over the stream (the same mix of kinds
+    # and sizes), one at a time
+    stride = max(1, n // plain_sample)
+    pick = list(range(0, n, stride))[:plain_sample]
+    sub = [reqs[i] for i in pick]
     t1 = time.perf_counter()
     exact = True
-    for (kind, arg), r in zip(sub, resps):
+    for (kind, arg), r in zip(sub, [resps[i] for i in pick]):
         if kind == "range":
             exact &= _range_key(v.verify_range(*arg)) == _range_key(r.range)
         else:
@@ -395,7 +398,11 @@ def run_served(v, capacity: float, load: float = 0.7, duration: float = 1.0, see
             "slices": info["range_slices"], "traj_batches": info["traj_batches"],
             "device_busy_frac": info["device_busy_s"] / wall,
             "plain_seeds_per_s_same_stream": sub_seeds / t_plain,
-            "plain_sample": f"first {len(sub)} requests one at a time (verify_range / trajectory)",
+            "plain_sample": f"{len(sub)} requests, every {stride}th of the stream, one at a time "
+                            "(verify_range / trajectory)",
+            "host_s": {"admit": info["host_admit_s"], "build_slices": info["host_slice_s"],
+                       "build_batches": info["host_batch_s"], "complete": info["host_complete_s"],
+                       "idle": info["host_idle_s"], "wall": wall},
             "served_vs_plain": (range_seeds / wall) / (sub_seeds / t_plain),
             "bit_exact_vs_plain_sample": bool(exact)}
 
