@@ -305,7 +305,7 @@ extern "C" void collatz_destroy(collatz_ctx* c) {
                     &c->d_segs, &c->d_widen, &c->d_widen2, &c->d_wcount, &c->t_seeds, &c->t_st, &c->t_exc,
                     &c->t_status, &c->t_idx[0], &c->t_idx[1], &c->t_cnt, &c->s1_front[0], &c->s1_front[1],
                     &c->s1_off, &c->s1_cnt, &c->s1_scal, &c->s1_stk_num, &c->s1_stk_meta, &c->s1_hist, &c->d_recs,
-                    &c->d_rcursor};
+                    &c->d_rcursor, &c->d_first};
   for (DevBuf* b : bufs) b->release();
   c->h_rec.release();
   c->h_pairs.release();
@@ -1045,7 +1045,7 @@ struct collatz_plan {
   RangeTables* T = nullptr;
   std::vector<RangeSeg> segs;
   unsigned long long items = 0;
-  DevBuf d_segs, d_recs, d_cursor, d_widen, d_widen2, d_wcount, d_stats;
+  DevBuf d_segs, d_recs, d_cursor, d_widen, d_widen2, d_wcount, d_stats, d_first;
   HostBuf h_recs;
   bool stats = false, negative = false;
   cudaGraph_t graph = nullptr;
@@ -1057,7 +1057,7 @@ struct collatz_plan {
 // tables and lowers every request into segments.
 static int range_lower_batch(collatz_ctx* c, const collatz_range* r, uint32_t n, RangeTables** T, uint32_t* k_out,
                              bool* neg_out, std::vector<RangeSeg>& segs, unsigned long long& items,
-                             uint32_t* seed_bits) {
+                             uint32_t* seed_bits, std::vector<uint32_t>& first_seg) {
   const uint32_t k = r[0].k ? r[0].k : c->cfg.range_k;
   const bool neg = (r[0].flags & COLLATZ_RANGE_NEGATIVE) != 0;
   for (uint32_t i = 0; i < n; i++)  // one sieve (k, sign) per launch
@@ -1067,9 +1067,12 @@ static int range_lower_batch(collatz_ctx* c, const collatz_range* r, uint32_t n,
   int rc = get_range_tables(c, k, T, neg);
   if (rc) return rc;
   *seed_bits = 0;
+  first_seg.assign(n, ~0u);
   for (uint32_t i = 0; i < n; i++) {
+    const size_t before = segs.size();
     rc = lower_range(c, r[i], i, **T, segs, items);
     if (rc) return rc;
+    if (segs.size() > before) first_seg[i] = (uint32_t)before;  // the scouts' item
     *seed_bits = std::max(*seed_bits, range_seed_bits(r[i]));
   }
   if (segs.empty()) {  // keep the kernel's segment search well-defined
@@ -1095,6 +1098,7 @@ struct RangeBufs {
   WidenEntry* widen2;
   uint32_t* wcount;  // 2 counters
   unsigned long long* stats;
+  const uint32_t* first_seg;  // per request: its first segment (threshold scouts)
 };
 
 static RangeArgs range_args(collatz_ctx* c, const RangeTables& T, uint32_t k, bool neg, const RangeBufs& b,
@@ -1127,6 +1131,7 @@ static cudaError_t range_enqueue(collatz_ctx* c, const RangeArgs& a, const Range
   if (!e) e = cudaMemsetAsync(b.cursor, 0, sizeof(unsigned long long), s);
   if (!e) e = cudaMemsetAsync(b.wcount, 0, sizeof(uint32_t) * 2, s);
   if (!e && b.stats) e = cudaMemsetAsync(b.stats, 0, 16 * sizeof(unsigned long long), s);
+  if (!e && b.first_seg) e = launch_range_scout(a, b.first_seg, b.n, s);
   if (!e) e = (b.stats && !a.negative) ? launch_range_stats(a, grid, s) : launch_range(a, c->range_variant, grid, s);
   if (!e)
     e = launch_range_wide(b.widen, b.wcount, WIDEN_CAP, 6, b.recs, b.widen2, WIDEN_CAP, b.wcount + 1, c->iter_cap, s,
@@ -1145,11 +1150,14 @@ static bool range_stats_requested() {
 
 static int plan_build(collatz_ctx* c, const collatz_range* r, uint32_t n, collatz_plan* p) {
   uint32_t k = 0, seed_bits = 0;
-  int rc = range_lower_batch(c, r, n, &p->T, &k, &p->negative, p->segs, p->items, &seed_bits);
+  std::vector<uint32_t> first_seg;
+  int rc = range_lower_batch(c, r, n, &p->T, &k, &p->negative, p->segs, p->items, &seed_bits, first_seg);
   if (rc) return rc;
   p->n = n;
   CK(c, p->d_segs.ensure(sizeof(RangeSeg) * p->segs.size()));
   CK(c, cudaMemcpy(p->d_segs.p, p->segs.data(), sizeof(RangeSeg) * p->segs.size(), cudaMemcpyHostToDevice));
+  CK(c, p->d_first.ensure(sizeof(uint32_t) * n));
+  CK(c, cudaMemcpy(p->d_first.p, first_seg.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice));
   CK(c, p->d_recs.ensure(sizeof(ReqRec) * std::max(1u, n)));
   CK(c, p->h_recs.ensure(sizeof(ReqRec) * std::max(1u, n)));
   CK(c, p->d_cursor.ensure(sizeof(unsigned long long)));
@@ -1161,7 +1169,7 @@ static int plan_build(collatz_ctx* c, const collatz_range* r, uint32_t n, collat
   const RangeBufs b{p->d_segs.as<RangeSeg>(), (uint32_t)p->segs.size(), p->items, p->d_recs.as<ReqRec>(),
                     p->h_recs.p, n, p->d_cursor.as<unsigned long long>(), p->d_widen.as<WidenEntry>(),
                     p->d_widen2.as<WidenEntry>(), p->d_wcount.as<uint32_t>(),
-                    p->stats ? p->d_stats.as<unsigned long long>() : nullptr};
+                    p->stats ? p->d_stats.as<unsigned long long>() : nullptr, p->d_first.as<uint32_t>()};
   const RangeArgs a = range_args(c, *p->T, k, p->negative, b, seed_bits);
   cudaStream_t s = c->own_stream;
   CK(c, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -1236,6 +1244,7 @@ extern "C" void collatz_plan_destroy(collatz_plan* p) {
   p->d_widen2.release();
   p->d_wcount.release();
   p->d_stats.release();
+  p->d_first.release();
   p->h_recs.release();
   delete p;
 }
@@ -1262,11 +1271,13 @@ extern "C" int collatz_verify_batch(collatz_ctx* c, const collatz_range* r, uint
   RangeTables* T = nullptr;
   uint32_t k = 0, seed_bits = 0;
   bool neg = false;
-  int rc = range_lower_batch(c, r, n, &T, &k, &neg, segs, items, &seed_bits);
+  std::vector<uint32_t> first_seg;
+  int rc = range_lower_batch(c, r, n, &T, &k, &neg, segs, items, &seed_bits, first_seg);
   if (rc) return rc;
-  const size_t sb = sizeof(RangeSeg) * segs.size(), rb = sizeof(ReqRec) * n;
+  const size_t sb = sizeof(RangeSeg) * segs.size(), rb = sizeof(ReqRec) * n, fb = sizeof(uint32_t) * n;
   CK(c, c->d_segs.ensure(sb));
-  CK(c, c->h_segs.ensure(sb));
+  CK(c, c->d_first.ensure(fb));
+  CK(c, c->h_segs.ensure(sb + fb));  // the segments, then the scouts' first segments
   CK(c, c->d_recs.ensure(rb));
   CK(c, c->h_recs.ensure(rb));
   CK(c, c->d_rcursor.ensure(sizeof(unsigned long long)));
@@ -1274,11 +1285,13 @@ extern "C" int collatz_verify_batch(collatz_ctx* c, const collatz_range* r, uint
   CK(c, c->d_widen2.ensure(sizeof(WidenEntry) * WIDEN_CAP));
   CK(c, c->d_wcount.ensure(sizeof(uint32_t) * 2));
   std::memcpy(c->h_segs.p, segs.data(), sb);
+  std::memcpy(static_cast<char*>(c->h_segs.p) + sb, first_seg.data(), fb);
   const RangeBufs b{c->d_segs.as<RangeSeg>(), (uint32_t)segs.size(), items, c->d_recs.as<ReqRec>(), c->h_recs.p, n,
                     c->d_rcursor.as<unsigned long long>(), c->d_widen.as<WidenEntry>(),
-                    c->d_widen2.as<WidenEntry>(), c->d_wcount.as<uint32_t>(), nullptr};
+                    c->d_widen2.as<WidenEntry>(), c->d_wcount.as<uint32_t>(), nullptr, c->d_first.as<uint32_t>()};
   const RangeArgs a = range_args(c, *T, k, neg, b, seed_bits);
   CK(c, cudaMemcpyAsync(c->d_segs.p, c->h_segs.p, sb, cudaMemcpyHostToDevice, c->stream));
+  CK(c, cudaMemcpyAsync(c->d_first.p, static_cast<char*>(c->h_segs.p) + sb, fb, cudaMemcpyHostToDevice, c->stream));
   CK(c, cudaEventRecord(c->ev[2], c->stream));
   CK(c, range_enqueue(c, a, b, c->stream));
   CK(c, cudaEventRecord(c->ev[3], c->stream));

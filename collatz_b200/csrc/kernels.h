@@ -132,6 +132,10 @@ cudaError_t range_init();  // once per device, before the first launch
 cudaError_t launch_range_stats(const RangeArgs& a, uint32_t grid, cudaStream_t st);
 cudaError_t launch_range(const RangeArgs& a, int variant, uint32_t grid, cudaStream_t st);
 cudaError_t range_occupancy(int variant, int* blocks_per_sm);
+// Threshold scouts: first_seg[i] is the index of request i's first segment
+// (>= a.nsegs: none).  Raises each request's prefilter keys to the maxima of
+// the seeds of its first work item, before the range kernel runs.
+cudaError_t launch_range_scout(const RangeArgs& a, const uint32_t* first_seg, uint32_t nreq, cudaStream_t st);
 // Seeds of a widen list re-run from scratch with 6 (then 8) limbs; the
 // list length is read on the device (*count, at most cap), so the pass can
 // sit in a captured graph right behind the range kernel.

@@ -940,6 +940,98 @@ __global__ void __launch_bounds__(128) k_range_wide(const WidenEntry* __restrict
 }
 
 // ------------------------------------------------------------------
+// Threshold scouts, launched before k_range.  A request's prefilter keys
+// start at zero, and the item cursor hands a small request's items to many
+// warps at once, so without a head start most of its seeds would run under
+// zero thresholds: replaying their first k steps, taking the excursion slow
+// path at every odd run and offering at the end.  Lane j of warp i runs the
+// j-th seed of request i's first work item in full (4 limbs), and the warp
+// raises the request's keys to the largest stopping time and excursion among
+// them.  These are seeds the request checks, so the keys stay lower bounds of
+// its maxima, and k_range still offers them (values equal to a threshold pass
+// every prefilter test).
+// ------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_range_scout(const RangeArgs A, const u32* __restrict__ first_seg, u32 nreq) {
+  const u32 wi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = lane_id();
+  if (wi >= nreq) return;  // warp-uniform
+  const u32 si = first_seg[wi];
+  if (si >= A.nsegs) return;  // a request without seeds
+  const RangeSeg g = A.segs[si];
+  if (g.local0_lo | g.local0_hi) return;  // not the segment's first item
+  // this lane's seed n (3 limbs): entry lane of the first item, or integer d_lo + lane
+  bool have = false;
+  Limbs<4> N;
+  N.w[3] = 0;
+  if (g.kind == 0) {
+    const u32 idx = g.s_lo + lane;
+    if (idx < g.s_hi && lane < RANGE_ITEM) {
+      const RangeEntry e = A.table[idx];
+      const u32 k = A.k, kb = k & 31;
+      const u32 q0 = (u32)g.q_lo, q1 = (u32)(g.q_lo >> 32), q2 = g.q_hi;
+      const u32 t0 = q0 << kb, t1 = __funnelshift_l(q0, q1, kb), t2 = __funnelshift_l(q1, q2, kb);
+      N.w[0] = ((k >= 32) ? 0u : t0) | e.r_lo;
+      N.w[1] = ((k >= 32) ? t0 : t1) | (e.meta & 0xFFu);
+      N.w[2] = (k >= 32) ? t1 : t2;
+      have = true;
+      if (g.mod9) {
+        const u32 k9 = (u32)((1ull << (k % 6)) % 9ull);
+        u32 x = (mod9_96(q0, q1, q2) * k9) % 9u + ((e.meta >> 16) & 0xFFu);
+        x = (x >= 9u) ? x - 9u : x;
+        have = ((KEEP9 >> x) & 1u) != 0;
+      }
+    }
+  } else {
+    const ull n = g.q_lo + lane;
+    if (n < g.d_hi && n >= 2 && (!g.mod9 || ((KEEP9 >> (u32)(n % 9u)) & 1u))) {
+      N.w[0] = (u32)n;
+      N.w[1] = (u32)(n >> 32);
+      N.w[2] = 0;
+      have = true;
+    }
+  }
+  u32 sig = 0;
+  ull ekey = 0;
+  if (have) {
+    Limbs<4> v = N, E = N;
+    inc_l<4>(v);  // v = n + 1
+    ull st = 0;
+    for (u32 it = 0;; it++) {
+      if (v.w[3] >= (1u << 19) || it > A.iter_cap) break;  // could leave 128 bits: no scout
+      const u32 a = ctz32(v.w[0] | (1u << 8));
+      odd_run_l<4>(v, a, pow3_le8(a));
+      st += a;
+      Limbs<4> x = v;
+      dec_l<4>(x);
+      if (limbs_lt<4>(E, x)) E = x;
+      const u32 b = ctz32(x.w[0] | 0x80000000u);
+      Limbs<4> w = x;
+      shr_l<4>(w, b);
+      if (b != 0 && limbs_lt<4>(w, N)) {
+        u32 s = 1;
+        for (; s < b; s++) {
+          Limbs<4> y = x;
+          shr_l<4>(y, s);
+          if (limbs_lt<4>(y, N)) break;
+        }
+        sig = (u32)min(st + s, 0xFFFFFFFFull);
+        ekey = key_of<4>(E.w);
+        break;
+      }
+      st += b;
+      v = w;
+      inc_l<4>(v);
+    }
+  }
+  sig = __reduce_max_sync(FULL, sig);
+#pragma unroll
+  for (u32 d = 16; d; d >>= 1) ekey = max(ekey, (ull)__shfl_xor_sync(FULL, ekey, d));
+  if (lane == 0) {
+    if (sig) atomicMax(&A.recs[g.req].st_key, (ull)sig);
+    if (ekey) atomicMax(&A.recs[g.req].e_key, ekey);
+  }
+}
+
+// ------------------------------------------------------------------
 // Launchers.
 // ------------------------------------------------------------------
 int range_variants() { return 8; }
@@ -1003,6 +1095,12 @@ cudaError_t range_init() {
     e = cudaFuncSetAttribute(k_range<2, 3, true, false, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)RANGE_SMEM);
   return e;
+}
+
+cudaError_t launch_range_scout(const RangeArgs& a, const u32* first_seg, u32 nreq, cudaStream_t st) {
+  if (!nreq || a.negative) return cudaSuccess;  // the negative variant keeps zero thresholds
+  k_range_scout<<<(nreq + 3) / 4, 128, 0, st>>>(a, first_seg, nreq);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_range_wide(const WidenEntry* list, const u32* count, u32 cap, int limbs, ReqRec* recs,

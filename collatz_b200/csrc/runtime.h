@@ -86,7 +86,7 @@ struct collatz_ctx {
   cz::DevBuf d_rec, d_counter, d_overflow, d_ovcount, d_pairs[2], d_segs, d_widen, d_widen2, d_wcount;
   cz::HostBuf h_rec, h_pairs;
   // one-shot range batches (collatz_verify_batch / collatz_verify_range)
-  cz::DevBuf d_recs, d_rcursor;
+  cz::DevBuf d_recs, d_rcursor, d_first;  // d_first: per request, its first segment (threshold scouts)
   cz::HostBuf h_segs, h_recs;
   std::vector<cz::RangeSeg> range_segs;
   cz::DevBuf t_seeds, t_st, t_exc, t_status, t_idx[2], t_cnt;

@@ -327,11 +327,15 @@ int launch_slice(collatz_server* s, int si) {
   std::vector<RangeSeg> segs;
   unsigned long long slice_items = 0, budget = s->cfg.slice_items;
   uint32_t seed_bits = 0;
+  std::vector<uint32_t> scouts;  // the first segment of each request that starts in this slice
   for (size_t i = 0; i < want.size(); i++) {
     const unsigned long long share = std::max<unsigned long long>(1, budget / (want.size() - i));
     const unsigned long long q = std::min(want[i].first, share);
     if (q) seed_bits = std::max(seed_bits, range_seed_bits(want[i].second->q.range));
+    const bool starts = want[i].second->cursor == 0;
+    const size_t before = segs.size();
     take_items(want[i].second, q, segs, slice_items);
+    if (starts && segs.size() > before) scouts.push_back((uint32_t)before);
     budget -= std::min(budget, q);
     if (want[i].second->cursor == want[i].second->items) S.finishing.push_back(want[i].second);
   }
@@ -339,13 +343,14 @@ int launch_slice(collatz_server* s, int si) {
   RangeTables* T = nullptr;
   int rc = get_range_tables(c, k, &T, neg);
   if (rc) return rc;
-  const size_t sb = sizeof(RangeSeg) * segs.size();
+  const size_t sb = sizeof(RangeSeg) * segs.size(), fb = sizeof(uint32_t) * scouts.size();
   const size_t rb = sizeof(ReqRec) * s->cfg.max_active;
-  cudaError_t e = S.d_segs.ensure(sb);
-  if (!e) e = S.h_segs.ensure(sb);
+  cudaError_t e = S.d_segs.ensure(sb + fb);  // the segments, then the scouts' segment indices
+  if (!e) e = S.h_segs.ensure(sb + fb);
   if (!e) e = S.h_recs.ensure(rb);
   if (e) return set_cuda_error(c, e, "server slice buffers");
   std::memcpy(S.h_segs.p, segs.data(), sb);
+  if (fb) std::memcpy(static_cast<char*>(S.h_segs.p) + sb, scouts.data(), fb);
   RangeArgs a;
   a.table = T->dev.table;
   a.k = k;
@@ -362,10 +367,14 @@ int launch_slice(collatz_server* s, int si) {
   a.negative = neg ? 1u : 0u;
   a.seed_bits = seed_bits;
   cudaStream_t st = s->sa;
-  e = cudaMemcpyAsync(S.d_segs.p, S.h_segs.p, sb, cudaMemcpyHostToDevice, st);
+  e = cudaMemcpyAsync(S.d_segs.p, S.h_segs.p, sb + fb, cudaMemcpyHostToDevice, st);
   if (!e) e = cudaMemsetAsync(S.d_cursor.p, 0, sizeof(unsigned long long), st);
   if (!e) e = cudaMemsetAsync(S.d_wcount.p, 0, 2 * sizeof(uint32_t), st);
   if (!e) e = cudaEventRecord(S.t0, st);
+  // threshold scouts for the requests that start here (their records were zeroed at admission)
+  if (!e && fb)
+    e = launch_range_scout(a, reinterpret_cast<const uint32_t*>(static_cast<const char*>(S.d_segs.p) + sb),
+                           (uint32_t)scouts.size(), st);
   if (!e) e = launch_range(a, c->range_variant, s->grid, st);
   if (!e)
     e = launch_range_wide(S.d_widen[0].as<WidenEntry>(), S.d_wcount.as<uint32_t>(), WIDEN_CAP, 6, a.recs,
@@ -770,7 +779,8 @@ extern "C" int collatz_server_start(const collatz_config* cfg, const collatz_ser
   // Host and device staging is allocated here, once: growing a pinned or
   // device buffer later (cudaFreeHost / cudaFree synchronise the device,
   // large cudaMallocHost calls take milliseconds) would stall both workers.
-  const size_t seg_bytes = sizeof(RangeSeg) * SEGS_PER_REQ * s->cfg.max_active;
+  // per request: its segments and one threshold-scout index
+  const size_t seg_bytes = (sizeof(RangeSeg) * SEGS_PER_REQ + sizeof(uint32_t)) * s->cfg.max_active;
   for (Slice& S : s->slices) {
     if ((e = S.d_segs.ensure(seg_bytes))) return fail(e, "slice");
     if ((e = S.h_segs.ensure(seg_bytes))) return fail(e, "slice");
