@@ -39,23 +39,27 @@ struct CasesWarp {
   unsigned short q[CQ];             // (slot << 10) | a
   u32 ring[CR][MULTI ? 17 : 12];    // base0..2, number0..3, 3^f limbs 0..3, flags (bit 0 cpu, line << 1);
                                     // MULTI: [12] st threshold, [13..16] excursion threshold of the line
-  u32 lane[32][MULTI ? 13 : 8];     // per lane: [0] st, [1..3] seed, [4..7] seed-local max E;
-                                    // MULTI: [8] st threshold, [9..12] excursion threshold of its line
+  u32 lane[32][MULTI ? 14 : 8];     // per lane: [0] st, [1..3] seed, [4..7] seed-local max E;
+                                    // MULTI: [8] st threshold, [9..12] excursion threshold of its line,
+                                    // [13] the line of a pending offer
   u32 thr[4];                       // excursion threshold (lower bound of the running max)
 };
 
-// Offers of several pending lanes of one request (all lanes call this
-// together; lane slots [0] sigma, [1..3] seed, [4..7] excursion): a value that
-// another pending lane beats -- larger, or equal with a smaller seed -- cannot
-// be the maximum, so its bit is dropped.  A warp's first seeds all finish
-// under zero thresholds.  Kept out of line: it runs in few passes.
-__device__ __noinline__ u32 cases_drop_dominated(u32 (*L)[8], u32 lane, u32 pend, u32 pm) {
+// Offers of several pending lanes (all lanes call this together; lane slots
+// [0] sigma, [1..3] seed, [4..7] excursion, and in line batches [13] the
+// line): a value that another pending lane of the same line beats -- larger,
+// or equal with a smaller seed -- cannot be the line's maximum, so its bit is
+// dropped.  A warp's first seeds of a line all finish under zero thresholds.
+// Kept out of line: it runs in few passes.
+template <int WD, bool MULTI>
+__device__ __noinline__ u32 cases_drop_dominated(u32 (*L)[WD], u32 lane, u32 pend, u32 pm) {
   const u32 m1 = __ballot_sync(FULL, pend & 1u), m2 = __ballot_sync(FULL, pend & 2u);
   __syncwarp();
   if (pend) {
     const u32 s0 = L[lane][1], s1 = L[lane][2], s2 = L[lane][3];
     for (u32 m = pm & ~(1u << lane); m; m &= m - 1) {
       const u32 j = __ffs(m) - 1;
+      if (MULTI && L[j][MULTI ? 13 : 0] != L[lane][MULTI ? 13 : 0]) continue;
       const u32 t0 = L[j][1], t1 = L[j][2], t2 = L[j][3];
       const bool j_smaller = (t2 != s2) ? (t2 < s2) : ((t1 != s1) ? (t1 < s1) : (t0 < s0));
       if ((pend & 1u) && ((m1 >> j) & 1u)) {
@@ -123,11 +127,9 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
     // ---- offers of finished seeds, one lane at a time (bounded locks) ----
     {
       u32 pm = __ballot_sync(FULL, pend != 0);
-      if constexpr (!MULTI) {
-        if (pm & (pm - 1)) {  // several pending lanes of the one request: offer only the best
-          pend = cases_drop_dominated(W.lane, lane, pend, pm);
-          pm = __ballot_sync(FULL, pend != 0);
-        }
+      if (pm & (pm - 1)) {  // several pending lanes: offer only the best of each line
+        pend = cases_drop_dominated<MULTI ? 14 : 8, MULTI>(W.lane, lane, pend, pm);
+        pm = __ballot_sync(FULL, pend != 0);
       }
       while (pm) {
         const u32 leader = __ffs(pm) - 1;
@@ -420,6 +422,7 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
               W.lane[lane][1] = n0;
               W.lane[lane][2] = n1;
               W.lane[lane][3] = n2;
+              if (MULTI) W.lane[lane][MULTI ? 13 : 0] = hline;
             }
           }
           active = false;
