@@ -12,7 +12,9 @@
 // test, even run <= 31] x 2, XOR the low limb, stop when v < n -- so the
 // XOR hash, the seed count and the overflow list are identical; the order
 // of work does not matter because every output is an XOR, a sum or a max.
-// Stopping time and maximum excursion are tracked on the side.
+// Stopping time and maximum excursion are tracked on the side.  While every
+// lane running a step holds a value below 2^59, the step runs on one 64-bit
+// value instead of four limbs (variant 4, for N <= 52).
 //
 // Line batches (MULTI): the pairs of many cases_* lines in one launch.  Base
 // limb 3 of a pair holds bigindex | line << 8 and every line has its own

@@ -12,9 +12,13 @@
 // every seed up with a warp scan into its shared-memory queue, and idle
 // lanes pull seeds from the queue with one ballot per step.  A seed starts
 // after one k-step jump, T^k(n) + 1 = q 3^f + c (no descent is possible in
-// those k steps), then runs odd/even runs in 4 x 32-bit limbs with the exact
-// stopping time and excursion.  A value that could leave 2^128 sends the
-// seed to the widen list, re-run from scratch with 6 and then 8 limbs.
+// those k steps), and, when bit lengths prove it exact, 8 more steps from a
+// 256-entry shared-memory table.  It then runs odd/even runs in 4 x 32-bit
+// limbs -- or on one 64-bit value while the warp's values are below 2^59 --
+// with the exact stopping time and excursion.  A value that could leave
+// 2^128 sends the seed to the widen list, re-run from scratch with 6 and then
+// 8 limbs.  Before the kernel, threshold scouts run the first seeds of each
+// request in full to give its prefilter keys a head start.
 #include <cuda_runtime.h>
 
 #include "common.cuh"
