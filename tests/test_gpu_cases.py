@@ -190,3 +190,30 @@ def test_iteration_cap_reports_instead_of_running_on():
         assert v.trajectory([27, 97])[0][0] == 3  # trajectory queries: status 3, iteration cap
     # a fresh context computes the reference's answer
     assert f"{cb.Verifier(26).run_case(3, 2, 2, 9, 1, 0).hash:X}" == "86E5527C"
+
+
+@pytest.mark.parametrize("n", [52, 53])
+def test_narrow_body_matches_four_limbs_at_high_n(verifier, n):
+    """N = 52 is the largest N that runs the 64-bit body: its seeds lie below
+    2^52 and their values pass 2^59 often, so lanes switch bodies step by step.
+    At N = 53 variant 4 falls back to the four-limb kernel.  Variant 4 and the
+    four-limb variant 3 must give identical hashes, counts, overflow lists and
+    maxima on lines of the N-bit tree."""
+    import collatz_b200 as cb
+    lines = cb.split_cases(n, (3, 2, 2, 9, 1, 0), 26)
+    picks = [cb.case_tuple(lines[i]) for i in (0, 1, 1000, len(lines) // 2, len(lines) - 1)]
+    v = verifier(n)
+    try:
+        for t in picks:
+            v.set_variant(0, 4)
+            a = v.run_case(*t)
+            v.set_variant(0, 3)
+            b = v.run_case(*t)
+            assert (a.hash, a.seeds_checked, a.launches, a.n_overflow) == \
+                (b.hash, b.seeds_checked, b.launches, b.n_overflow), t
+            assert sorted(a.overflow) == sorted(b.overflow), t
+            assert (a.max_stopping_time, a.max_stopping_time_seed) == (b.max_stopping_time, b.max_stopping_time_seed)
+            assert (a.max_excursion, a.max_excursion_seed) == (b.max_excursion, b.max_excursion_seed)
+            assert a.seeds_checked > 0
+    finally:
+        v.set_variant(0, 4)  # the default
