@@ -137,7 +137,7 @@ struct collatz_server {
   collatz_server_info_t info{};
   double host_t[2][T_N] = {};  // [range, query thread][bucket]
 
-  std::atomic<uint32_t> active{0};  // admitted requests not yet complete
+  std::atomic<uint32_t> active[2] = {{0}, {0}};  // admitted, not yet complete: [0] ranges, [1] queries
 
   // admission budget (guarded by mb)
   std::mutex mb;
@@ -207,10 +207,12 @@ bool take_budget(collatz_server* s, uint64_t need) {
   return true;
 }
 
-bool take_active(collatz_server* s) {
-  uint32_t a = s->active.load();
+// Each kind has its own max_active admissions, so a backlog of range
+// requests never holds back trajectory queries (or the other way round).
+bool take_active(collatz_server* s, int kind) {
+  uint32_t a = s->active[kind].load();
   while (a < s->cfg.max_active)
-    if (s->active.compare_exchange_weak(a, a + 1)) return true;
+    if (s->active[kind].compare_exchange_weak(a, a + 1)) return true;
   return false;
 }
 
@@ -250,9 +252,9 @@ void admit_ranges(collatz_server* s) {
   for (;;) {
     Req* r = front(s, s->pend_range, 0);
     if (!r || s->free_slots.empty()) return;
-    if (!take_active(s)) return;
+    if (!take_active(s, 0)) return;
     if (!take_budget(s, 0)) {
-      s->active--;
+      s->active[0]--;
       return;
     }
     pop_admitted(s, s->pend_range, r);
@@ -262,7 +264,7 @@ void admit_ranges(collatz_server* s) {
     int rc = get_range_tables(c, r->k, &T, r->neg);
     if (!rc) rc = lower_range(c, r->q.range, 0, *T, r->segs, r->items);
     if (rc || r->items == 0) {  // an error, or no seed in the range
-      s->active--;
+      s->active[0]--;
       publish(s, r, rc);
       continue;
     }
@@ -270,7 +272,7 @@ void admit_ranges(collatz_server* s) {
     cudaError_t e = cudaMemsetAsync(s->d_recs.as<ReqRec>() + r->slot, 0, sizeof(ReqRec), s->sa);
     if (e != cudaSuccess) {
       cudaGetLastError();
-      s->active--;
+      s->active[0]--;
       publish(s, r, COLLATZ_E_CUDA);
       continue;
     }
@@ -404,7 +406,7 @@ void complete_slice(collatz_server* s, int si) {
     seeds += r->res.seeds_checked;
     s->free_slots.push_back(r->slot);
     s->ranges.erase(std::find(s->ranges.begin(), s->ranges.end(), r));
-    s->active--;
+    s->active[0]--;
     publish(s, r, r->res.status);
   }
   S.busy = false;
@@ -422,9 +424,9 @@ void admit_queries(collatz_server* s) {
     Req* r = front(s, s->pend_query, TRAJ_BYTES_PER_SEED);
     if (!r) return;
     const uint64_t need = TRAJ_BYTES_PER_SEED * r->q.nseeds + 256;
-    if (!take_active(s)) return;
+    if (!take_active(s, 1)) return;
     if (!take_budget(s, need)) {
-      s->active--;
+      s->active[1]--;
       return;
     }
     pop_admitted(s, s->pend_query, r);
@@ -538,7 +540,7 @@ void complete_batch(collatz_server* s, int bi) {
     std::memcpy(r->q.stopping_time, B.h_st.as<uint64_t>() + o, 8 * m);
     std::memcpy(r->q.excursion, B.h_exc.as<uint32_t>() + 16 * o, 64 * m);
     std::memcpy(r->q.status, B.h_status.as<uint32_t>() + o, 4 * m);
-    s->active--;
+    s->active[1]--;
     publish(s, r, COLLATZ_OK);
   }
   B.reqs.clear();
@@ -573,7 +575,7 @@ void fail_worker(collatz_server* s, bool range_side, int rc) {
     s->stopping = true;
   }
   for (Req* r : all) {
-    s->active--;
+    s->active[range_side ? 0 : 1]--;
     publish(s, r, rc);
   }
   for (Req* r : pend) publish(s, r, rc);
@@ -886,7 +888,7 @@ extern "C" int collatz_server_info(collatz_server* s, collatz_server_info_t* inf
   std::lock_guard<std::mutex> g(s->mu);
   *info = s->info;
   info->pending = (uint32_t)(s->pend_range.size() + s->pend_query.size());
-  info->active = s->active.load();
+  info->active = s->active[0].load() + s->active[1].load();
   info->host_admit_s = s->host_t[0][T_ADMIT] + s->host_t[1][T_ADMIT];
   info->host_slice_s = s->host_t[0][T_BUILD];
   info->host_batch_s = s->host_t[1][T_BUILD];

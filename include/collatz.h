@@ -298,7 +298,8 @@ typedef struct collatz_server collatz_server;
 enum { COLLATZ_REQ_RANGE = 0, COLLATZ_REQ_TRAJECTORY = 1 };
 
 typedef struct {
-  uint32_t max_active;        /* requests admitted at once; default 256, at most 4096 */
+  uint32_t max_active;        /* range requests admitted at once, and as many trajectory queries;
+                               * default 256, at most 4096 */
   uint32_t slice_items;       /* work items (64 survivor entries) per range slice; default 1 << 19 */
   uint64_t hbm_reserve;       /* device bytes that admission leaves free; default 1 GiB */
   uint32_t traj_batch_seeds;  /* seeds per trajectory batch (and per query); default 1 << 20, at
