@@ -102,6 +102,14 @@ __device__ __noinline__ u32 cases_drop_dominated(u32 (*L)[WD], u32 lane, u32 pen
 template <int ITERS, int REFILL_MIN, bool MULTI, bool N64 = false>
 __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
   __shared__ CasesWarp<MULTI> S[CWARPS];
+  // 3^a for the 64-bit body: one shared load on the load/store pipe instead of
+  // the ALU byte lookups (the ALU pipe is the busy one)
+  __shared__ u32 s_p3[9];
+  if (threadIdx.x < 9) {
+    u32 p = 1;
+    for (u32 i = 0; i < threadIdx.x; i++) p *= 3u;
+    s_p3[threadIdx.x] = p;
+  }
   const u32 lane = lane_id();
   CasesWarp<MULTI>& W = S[threadIdx.x >> 5];
   if (lane < 4) W.thr[lane] = 0;
@@ -341,7 +349,7 @@ __global__ void __launch_bounds__(CWARPS * 32) k_cases(const CasesArgs A) {
           if (N64 && narrow) {
             u64 v = ((u64)v1 << 32) | v0;
             const u32 a = ctz32(v0 | (1u << 8));
-            v = (v >> a) * pow3_le8(a);
+            v = (v >> a) * s_p3[a];
             st += a;
             v0 = (u32)v;
             v1 = (u32)(v >> 32);

@@ -716,7 +716,7 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
       if (N64 && !NEG && narrow) {
         u64 v = ((u64)v1 << 32) | v0;
         const u32 a = ctz32(v0 | (1u << 7));
-        v = (v >> a) * pow3_le7(a);
+        v = (v >> a) * s_pow3[a];  // shared table: the load/store pipe, not the busy ALU pipe
         st += a;
         if (STATS) {
           c_iter++;
