@@ -385,7 +385,7 @@ __device__ __forceinline__ bool expand_one(WT& W, const RangeArgs& A, const uint
             const u32 glen = (e8 >> 20) & 31u, hlen = (e8 >> 25) & 31u;
             if ((xb + glen >= nbl + 10u) & (xb + hlen < w_thr_bl + 8u) & (xb <= 100u)) {
               u32 y0 = x0, y1 = x1, y2 = x2, y3 = x3;
-              odd_run4(y0, y1, y2, y3, 8u, pow3_le8((e8 >> 16) & 15u));  // (x >> 8) 3^f_8
+              odd_run4(y0, y1, y2, y3, 8u, (u32)s_p3[(e8 >> 16) & 15u]);  // (x >> 8) 3^f_8
               // + T^8(r) + 1 (back to v space)
               asm("add.cc.u32 %0, %0, %4;\n\t"
                   "addc.cc.u32 %1, %1, 0;\n\t"
