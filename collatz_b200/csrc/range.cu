@@ -736,9 +736,12 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
       } else {
         {
           // odd run capped at 7 steps (a longer run continues in the next pass, after an empty
-          // even run); 3^a from byte lookups in registers keeps shared memory off this path
+          // even run)
           const u32 a = ctz32(v0 | (1u << 7));
-          odd_run4(v0, v1, v2, v3, a, pow3_le7(a));
+          // 3^a: the shared table where this body is the hot one (measured: the
+          // frontier's four-limb kernel gains 1 %), register lookups beside the
+          // 64-bit body (the table there cost the block 0.5 %)
+          odd_run4(v0, v1, v2, v3, a, N64 ? pow3_le7(a) : s_pow3[a]);
           st += a;
           if (STATS) c_iter++;
         }
