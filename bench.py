@@ -48,18 +48,18 @@ UNIT = "seeds/s"
 # shifts, increment with carry, descent test).
 OPS_JUMP, OPS_ODD, OPS_EVEN = 16, 14, 12
 # DRAM bytes (read + write) of one k_range launch, measured with ncu.
-K_RANGE_DRAM_BYTES = 4.901888e6 + 0.204800e6
+K_RANGE_DRAM_BYTES = 4.886784e6 + 0.195584e6
 # Frontier (k = 34): every block of 2^34 seeds streams the 5 mod-9 classes
 # of the 2.43 GB survivor table that it keeps; ncu on a 4-block launch read
-# 5.422884864e9 and wrote 9.251328e6 bytes, so traffic per launch = blocks x
+# 5.424081664e9 and wrote 8.218368e6 bytes, so traffic per launch = blocks x
 # this figure.
-K_RANGE_FRONTIER_DRAM_BYTES_PER_BLOCK = (5.422884864e9 + 9.251328e6) / 4
+K_RANGE_FRONTIER_DRAM_BYTES_PER_BLOCK = (5.424081664e9 + 8.218368e6) / 4
 # Issue-slot and ALU-pipe utilisation of k_range measured with ncu (2^33
 # block, k = 24; 2^36 frontier, k = 34).  The ALU pipe is the one that
 # saturates first for this instruction mix (collatz_int_peak mix 1 reaches
 # its limit at 77 % of the issue slots).
-K_RANGE_ISSUE_NCU = {"block": 0.7568, "frontier": 0.7636}
-K_RANGE_ALU_PIPE_NCU = {"block": 0.6812, "frontier": 0.6727}
+K_RANGE_ISSUE_NCU = {"block": 0.7565, "frontier": 0.7686}
+K_RANGE_ALU_PIPE_NCU = {"block": 0.6515, "frontier": 0.6483}
 
 
 def dist_env():
