@@ -583,12 +583,13 @@ def main():
                                         "profiles/k_range_frontier_2p36.md, profiles/int_peak_mixes.md)"},
             # request (32 B) + its work list: an aligned range of many blocks lowers to 55
             # 64-byte segments (5 kept mod-9 classes of the first and last block, 9 x 5 for the
-            # blocks between)
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 32 + 64 * 55,
+            # blocks between), and the request's 4-byte first-segment index (threshold scouts)
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 32 + 64 * 55 + 4,
                     "d2h_bytes_per_step": 136,
                     "call": "collatz_verify_range (lower + upload work list + launches + result copy)"},
             "clocks": clocks,
-            "gpu_launches": 3 * args.steps,
+            # per step: k_range_scout, k_range and the two widening passes
+            "gpu_launches": 4 * args.steps,
             "wall_s_timed": wall,
         }
         if not args.no_cpu_baseline:
