@@ -47,19 +47,34 @@ UNIT = "seeds/s"
 # ctz, table, overflow test) and, per even run, 2L + 4 (decrement, ctz, L
 # shifts, increment with carry, descent test).
 OPS_JUMP, OPS_ODD, OPS_EVEN = 16, 14, 12
-# DRAM bytes (read + write) of one k_range launch, measured with ncu.
-K_RANGE_DRAM_BYTES = 4.886784e6 + 0.195584e6
-# Frontier (k = 34): every block of 2^34 seeds streams the 5 mod-9 classes
-# of the 2.43 GB survivor table that it keeps; ncu on a 4-block launch read
-# 5.424081664e9 and wrote 8.218368e6 bytes, so traffic per launch = blocks x
-# this figure.
-K_RANGE_FRONTIER_DRAM_BYTES_PER_BLOCK = (5.424081664e9 + 8.218368e6) / 4
-# Issue-slot and ALU-pipe utilisation of k_range measured with ncu (2^33
-# block, k = 24; 2^36 frontier, k = 34).  The ALU pipe is the one that
-# saturates first for this instruction mix (collatz_int_peak mix 1 reaches
-# its limit at 77 % of the issue slots).
-K_RANGE_ISSUE_NCU = {"block": 0.7565, "frontier": 0.7686}
-K_RANGE_ALU_PIPE_NCU = {"block": 0.6515, "frontier": 0.6483}
+# Counters of one k_range launch taken with ncu, valid only for the kernel
+# sources they were captured from: `src` is kernel_source_hash() at capture
+# time, and a line reports them only while the sources still hash to it.
+#   block:    2^33 launch at 2^40, k = 24 (dram bytes per launch do not grow
+#             with the block: the 4.6 MB survivor table is read from DRAM once
+#             and from L2 after that);
+#   frontier: 2^36 launch at 2^60, k = 34 (dram bytes per 2^34 block: each
+#             block streams the 5 mod-9 classes it keeps of the 2.43 GB table).
+NCU_CAPTURES = {
+    "block": {"src": "fbc65cb3163b5004", "dram_bytes": 4.886784e6 + 0.195584e6, "per": "launch",
+              "issue_slots_busy": 0.7565, "alu_pipe_busy": 0.6515},
+    "frontier": {"src": "fbc65cb3163b5004", "dram_bytes": (5.424081664e9 + 8.218368e6) / 4, "per": "2^34 block",
+                 "issue_slots_busy": 0.7686, "alu_pipe_busy": 0.6483},
+}
+KERNEL_SOURCES = ("range.cu", "common.cuh", "kernels.h", "tables.h", "tables.cu")
+# CPU sample of the block workload, the same for the reference arm's steps and
+# the cpu_baseline leg: 2^32 seeds at 2^40 + i 2^32 with the k = 24 sieve.
+CPU_SAMPLE_LOG2 = 32
+
+
+def kernel_source_hash() -> str:
+    """sha256 (first 16 hex digits) of the range kernel's sources."""
+    import hashlib
+    h = hashlib.sha256()
+    for name in KERNEL_SOURCES:
+        with open(os.path.join(ROOT, "collatz_b200", "csrc", name), "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()[:16]
 
 
 def dist_env():
@@ -121,39 +136,39 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_sample(offset: int, target_s: float, k: int, nthreads: int, max_log2: int = 34):
-    """Times the oracle's run-length loop (the reference's search3 shape) on a
-    bounded sample of the workload; returns (seeds/s, sample size, seconds)."""
+def cpu_reference_steps(base: int, size: int, k: int, nthreads: int, steps: int, warmup: int) -> list[float]:
+    """Times the oracle's run-length loop (the reference's search3 shape,
+    collatz_cudav7.cu:684-715) on `steps` samples [base + i size, base + (i+1)
+    size) after `warmup` untimed ones, on nthreads host threads; returns the
+    seconds per step.  The reference arm and the cpu_baseline leg both call
+    this with the same sample, so their rates agree."""
     from oracle import oracle as O
-    size = 1 << 22
-    t0 = time.perf_counter()
-    O.range_verify(offset, size, k, True, 1, nthreads)
-    dt = max(time.perf_counter() - t0, 1e-3)
-    while dt < target_s / 4 and size < (1 << max_log2):
-        size <<= 2
+    for i in range(warmup):
+        O.range_verify(base + i * size, size, k, True, 1, nthreads)
+    times = []
+    for i in range(steps):
         t0 = time.perf_counter()
-        O.range_verify(offset, size, k, True, 1, nthreads)
-        dt = max(time.perf_counter() - t0, 1e-3)
-    return size / dt, size, dt
+        O.range_verify(base + i * size, size, k, True, 1, nthreads)
+        times.append(time.perf_counter() - t0)
+    return times
+
+
+def cpu_sample_desc(wl: dict, size: int, steps: int, nthreads: int) -> str:
+    return (f"{steps} x {size} seeds at 2^{wl['offset_log2']} + i*{size}, k={wl['k']} sieve + mod-9 "
+            f"(oracle/collatz_oracle.c run-length loop after cu:684-715, {nthreads} threads; the 2^{wl['k']} "
+            "sieve table is built once per process, outside the timed steps)")
 
 
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
-    from oracle import oracle as O
     wl = WORKLOADS[args.workload]
     base, ksv = wl["offset"], wl["k"]
     nthreads = os.cpu_count() or 1
-    # one step = a bounded sample of the workload (the full block takes CPU-hours)
-    rate, size, _ = cpu_sample(base, 2.0, ksv, nthreads, max_log2=32)
-    for _ in range(args.warmup):
-        O.range_verify(base, size, ksv, True, 1, nthreads)
-    times = []
-    for i in range(args.steps):
-        t0 = time.perf_counter()
-        O.range_verify(base + i * size, size, ksv, True, 1, nthreads)
-        times.append(time.perf_counter() - t0)
+    # one step = a bounded sample of the workload (the full block takes CPU-minutes)
+    size = 1 << CPU_SAMPLE_LOG2
+    times = cpu_reference_steps(base, size, ksv, nthreads, args.steps, args.warmup)
     tot = sum(times)
     value = size * args.steps / tot
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
@@ -161,13 +176,11 @@ def run_reference(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u128",
             "data": "synthetic (deterministic seed range)",
             "config": {"workload": f"range [2^{wl['offset_log2']} + i*S, 2^{wl['offset_log2']} + (i+1)*S), "
-                                   f"S = {size} (bounded sample of the 2^{args.size_log2 or wl['size_log2']} "
+                                   f"S = 2^{CPU_SAMPLE_LOG2} (bounded sample of the 2^{args.size_log2 or wl['size_log2']} "
                                    f"{wl['name']}), k={ksv} sieve + mod-9",
                        "k": ksv, "sample_size": size},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
-                             "sample": f"{args.steps} x {size} seeds at 2^{wl['offset_log2']} "
-                                       "(oracle/collatz_oracle.c run-length loop after cu:684-715, "
-                                       f"{nthreads} threads)"},
+                             "sample": cpu_sample_desc(wl, size, args.steps, nthreads)},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -178,21 +191,30 @@ def _range_key(r):
             r.max_stopping_time, r.max_stopping_time_seed, r.errors)
 
 
-def run_batched(v, n_req: int = 4096, seed: int = 4096, lo_log2: int = 20, hi_log2: int = 34) -> dict:
-    """Batched configuration: n_req range requests, sizes log-uniform in
-    [2^lo, 2^hi] seeds, offsets uniform in [2^40, 2^64) aligned to the 2^24
-    sieve modulus (seeded), all in one persistent launch (a plan: lowered work
-    list + captured graph), against the plain path that verifies the same
-    requests one at a time (collatz_verify_range).  Bit-exact per request."""
+def batched_requests(n_req: int = 4096, seed: int = 4096, lo_log2: int = 20, hi_log2: int = 34):
+    """The batched configuration's requests: n_req (offset, size, k, mod9)
+    tuples, sizes log-uniform in [2^lo, 2^hi] seeds, offsets uniform in
+    [2^40, 2^64) rounded down to a multiple of the 2^24 sieve modulus, drawn
+    from numpy default_rng(seed)."""
     import numpy as np
-    import torch
     rng = np.random.default_rng(seed)
     sizes = np.exp(rng.uniform(lo_log2 * np.log(2), hi_log2 * np.log(2), n_req)).astype(np.uint64)
     reqs = []
     for s in sizes:
         off = int(rng.integers(1 << 40, 1 << 64, dtype=np.uint64))
         reqs.append((off - off % (1 << K_SIEVE), int(s), K_SIEVE, True))
-    total = sum(int(s) for s in sizes)
+    return reqs
+
+
+def run_batched(v, n_req: int = 4096, seed: int = 4096, lo_log2: int = 20, hi_log2: int = 34) -> dict:
+    """Batched configuration: n_req range requests, sizes log-uniform in
+    [2^lo, 2^hi] seeds, offsets uniform in [2^40, 2^64) aligned to the 2^24
+    sieve modulus (seeded), all in one persistent launch (a plan: lowered work
+    list + captured graph), against the plain path that verifies the same
+    requests one at a time (collatz_verify_range).  Bit-exact per request."""
+    import torch
+    reqs = batched_requests(n_req, seed, lo_log2, hi_log2)
+    total = sum(q[1] for q in reqs)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     plan = v.plan(reqs)
@@ -289,7 +311,11 @@ def run_cases() -> dict:
     c = T.run_case(3, 2, 2, 9, 1, 0)
     cdt = time.perf_counter() - t0
     n45 = [o for o in out if o["N"] == 45]
-    return {"workload": "collatz_run_case (Step 1 and Steps 2-3 on the GPU) on the reference's golden tuples",
+    try:
+        refgpu = run_reference_gpu_program()
+    except Exception as e:  # noqa: BLE001
+        refgpu = {"error": f"{type(e).__name__}: {e}"}
+    return {"reference_gpu_program": refgpu,"workload": "collatz_run_case (Step 1 and Steps 2-3 on the GPU) on the reference's golden tuples",
             "runs": out,
             "n45_seeds_per_s": sum(o["seeds"] for o in n45) / max(1e-9, sum(o["s"] for o in n45)),
             "all_match_reference": all(o["hash_ok"] and o["launches_ok"] and o["seeds_ok"] for o in out),
@@ -298,6 +324,46 @@ def run_cases() -> dict:
                              "sample": f"N=36 root case (3 2 2 9 1 0), {c.seeds} seeds in {cdt:.1f} s "
                                        "(oracle/collatz_oracle.c orc_run_case, the reference's kernel "
                                        "semantics cu:185-411 on one thread)"}}
+
+
+def run_reference_gpu_program(reps: int = 2) -> dict:
+    """The reference program itself -- collatz_cudav7.cu compiled unchanged
+    for sm_100a (MAXBITS = 45, the source's own value; built from the
+    reference's sources by oracle/build_ref_gpu.sh) -- against this
+    repository's drop-in CLI, on the same box and from the same process tree:
+    cases_tiny line 1 at N = 45, each a whole process (context creation,
+    tables, Step 1, Steps 2-3), wall time, best of `reps`.  An input whose
+    Step 1 has no leaves (start-up only) separates start-up from the run."""
+    ref = os.path.join(ROOT, "oracle", "_ref", "ref_gpu_N45")
+    cli = os.path.join(ROOT, "collatz_b200", "collatz_b200")
+    if not (os.path.exists(ref) and os.path.exists(cli)):
+        return {"unavailable": "oracle/_ref/ref_gpu_N45 or the CLI is not built (the reference sources were "
+                               "absent at build time)"}
+    line1, empty = "27 10 8 183 0 0\n", "0 5 0 1 0 0\n"
+
+    def run(cmd, text):
+        best, summ = None, None
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            p = subprocess.run(cmd, input=text, capture_output=True, text=True, timeout=300)
+            dt = time.perf_counter() - t0
+            if p.returncode:
+                raise RuntimeError(f"{os.path.basename(cmd[0])} rc={p.returncode}: {p.stderr[-200:]}")
+            summ = next((ln for ln in p.stderr.splitlines() if ln.startswith("Number of kernel launches")), None)
+            best = dt if best is None else min(best, dt)
+        return best, summ
+
+    r_line, r_sum = run([ref], line1)
+    c_line, c_sum = run([cli, "45"], line1)
+    r_empty, _ = run([ref], empty)
+    c_empty, _ = run([cli, "45"], empty)
+    return {"input": "27 10 8 183 0 0 (cases_tiny line 1, N = 45; the reference's own default run)",
+            "reference_program": "oracle/_ref/ref_gpu_N45 (collatz_cudav7.cu, nvcc -O3 sm_100a, unchanged)",
+            "reference_summary": r_sum, "cli_summary": c_sum, "same_summary_line": r_sum == c_sum,
+            "reference_s": r_line, "cli_s": c_line, "reference_startup_s": r_empty, "cli_startup_s": c_empty,
+            "reference_run_s": r_line - r_empty, "cli_run_s": c_line - c_empty,
+            "note": "wall time of whole processes; *_run_s = line 1 minus the start-up-only input "
+                    "(0 5 0 1 0 0, no Step-1 leaves); the reference's start-up includes its CPU table precompute"}
 
 
 def run_served(v, capacity: float, load: float = 0.7, duration: float = 1.0, seed: int = 5,
@@ -407,6 +473,192 @@ def run_served(v, capacity: float, load: float = 0.7, duration: float = 1.0, see
             "bit_exact_vs_plain_sample": bool(exact)}
 
 
+def roofline(workload: str, base: int, k: int, survivors: int, mean_ms: float, size: int, sm_count: int,
+             sm_mhz: float, ipk: dict) -> dict:
+    """Integer roofline of one k_range launch: algorithmic 32-bit operations
+    (per surviving seed: the jump plus the odd and even runs the oracle's
+    jump+runs model counts on a 2^24-seed sample of the same workload) per
+    second of device time, against the measured integer peak at the sampled
+    SM clock.  ncu counters are attached only while the kernel sources still
+    hash to those they were captured from."""
+    from oracle import oracle as O
+    samp = O.range_verify(base, 1 << 24, k, True, 2, min(8, os.cpu_count() or 1))
+    odd_per = samp.odd_runs / samp.seeds
+    even_per = samp.even_runs / samp.seeds
+    ops_per_seed = OPS_JUMP + OPS_ODD * odd_per + OPS_EVEN * even_per
+    achieved = survivors * ops_per_seed / (mean_ms / 1e3) / 1e12
+    peak = ipk[1]["ops_per_clk_sm"] * sm_count * sm_mhz * 1e6 / 1e12
+    issue_peak = sm_count * 128 * sm_mhz * 1e6 / 1e12
+    cap = NCU_CAPTURES[workload]
+    src = kernel_source_hash()
+    valid = cap["src"] == src
+    traffic = None
+    if valid:
+        traffic = cap["dram_bytes"] * (1 if cap["per"] == "launch" else max(1, size >> k))
+    d = {"bound": "int", "achieved": achieved, "peak": peak, "unit": "Tops/s (32-bit)", "frac": achieved / peak,
+         "traffic": traffic,
+         "traffic_basis": (f"ncu dram__bytes_read.sum + dram__bytes_write.sum per {cap['per']}, captured from "
+                           f"kernel sources {cap['src']}" + (f" x {max(1, size >> k)} blocks" if cap["per"] != "launch"
+                                                             else "")) if valid else
+         f"null: the kernel sources ({src}) changed since the last ncu capture ({cap['src']})",
+         "model": f"{ops_per_seed:.1f} algorithmic 32-bit ops per surviving seed ({OPS_JUMP} + {OPS_ODD} x "
+                  f"{odd_per:.2f} odd runs + {OPS_EVEN} x {even_per:.2f} even runs) x {survivors} seeds per launch",
+         "peak_basis": f"measured integer peak (collatz_int_peak mix 1: funnel shift, 3-input add, multiply-add "
+                       f"chains on every SM): {ipk[1]['ops_per_clk_sm']:.1f} ops per SM clock x {sm_count} SMs x "
+                       f"{sm_mhz:.0f} MHz (sampled median SM clock); MEASURED_PEAKS.json has no integer peak",
+         "int_peak_measured": {
+             "mix1_kernel_mix": {"tops": ipk[1]["ops_per_s"] / 1e12, "ops_per_clk_sm": ipk[1]["ops_per_clk_sm"],
+                                 "sm_mhz": ipk[1]["sm_mhz"]},
+             "mix0_alu_only": {"tops": ipk[0]["ops_per_s"] / 1e12, "ops_per_clk_sm": ipk[0]["ops_per_clk_sm"],
+                               "sm_mhz": ipk[0]["sm_mhz"]}},
+         "issue_peak": issue_peak, "frac_of_issue_peak": achieved / issue_peak}
+    if valid:
+        # every issued instruction (work distribution included), where achieved/peak counts only
+        # the algorithmic operations
+        d["ncu"] = {"issue_slots_busy": cap["issue_slots_busy"], "alu_pipe_busy": cap["alu_pipe_busy"],
+                    "kernel_sources": cap["src"],
+                    "metrics": "sm__inst_issued.avg.pct_of_peak_sustained_active, "
+                               "sm__pipe_alu_cycles_active.avg.pct_of_peak_sustained_active"}
+    return d
+
+
+def run_frontier(local: int, stream, flush, sm_count: int, ipk: dict, steps: int = 5, warmup: int = 3) -> dict:
+    """Frontier configuration: [2^60, 2^60 + 2^40) with the 2^34-bit sieve and
+    its class-major survivor table resident in HBM (built on the GPU first),
+    one plan launch per step, L2 flushed between steps, CUDA events on the
+    library's stream; clocks sampled during the timed steps."""
+    import torch
+    import collatz_b200 as cb
+    wl = WORKLOADS["frontier"]
+    size = 1 << wl["size_log2"]
+    fv = cb.Verifier(26, range_k=wl["k"], device=local)
+    try:
+        fv.set_stream(stream.cuda_stream)
+        t0 = time.perf_counter()
+        plan = fv.plan([(wl["offset"], size, wl["k"], True)])
+        t_tab = time.perf_counter() - t0
+
+        def step():
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            plan.launch()
+            e1.record(stream)
+            return e0, e1
+
+        for _ in range(warmup):
+            step()
+        torch.cuda.synchronize()
+        clk = ClockSampler(local)
+        clk.start()
+        time.sleep(0.3)
+        evs = [step() for _ in range(steps)]
+        torch.cuda.synchronize()
+        clocks = clk.stop()
+        ms = [a.elapsed_time(b) for a, b in evs]
+        res = plan.results()[0]
+        plan.close()
+        mean_ms = sum(ms) / len(ms)
+        roof = roofline("frontier", wl["offset"], wl["k"], res.seeds_checked, mean_ms, size, sm_count,
+                        clocks.get("sm_mhz") or 1965.0, ipk)
+        return {"workload": f"range [2^60, 2^60 + 2^40), k={wl['k']} sieve (2^34-bit bit array + class-major "
+                            "survivor table resident in HBM) + mod-9, 128-bit limbs widening to 192/256, plain kernel",
+                "steps": steps, "warmup": warmup, "ms_per_step": mean_ms, "seeds_per_s": size / (mean_ms / 1e3),
+                "survivors_per_step": res.seeds_checked, "table_build_s": t_tab,
+                "results": {"seeds_checked": res.seeds_checked, "failures": res.failures, "widened": res.widened,
+                            "max_stopping_time": res.max_stopping_time,
+                            "max_stopping_time_seed": str(res.max_stopping_time_seed),
+                            "max_excursion": str(res.max_excursion),
+                            "max_excursion_seed": str(res.max_excursion_seed), "errors": res.errors},
+                "roofline": roof, "clocks": clocks,
+                "l2": "flushed between steps (256 MiB write, outside the timed events)"}
+    finally:
+        fv.close()
+
+
+def run_config1(local: int, nthreads: int) -> dict:
+    """Plain verification: every n in [0, 2^32) with the 2^16 residue sieve
+    and the mod-9 sieve.  CPU: the oracle's run-length loop in 64-bit
+    arithmetic with overflow detection (a seed that would leave 64 bits is
+    re-run in 128 bits) on all host threads; GPU: collatz_verify_range on the
+    same range.  Both must give the same outputs."""
+    import collatz_b200 as cb
+    from oracle import oracle as O
+    n = 1 << 32
+    v1 = cb.Verifier(26, range_k=16, device=local)
+    try:
+        v1.verify_range(0, n, 16)  # tables, buffers
+        walls, devs = [], []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            g = v1.verify_range(0, n, 16)
+            walls.append(time.perf_counter() - t0)
+            devs.append(g.device_ms)
+    finally:
+        v1.close()
+    t0 = time.perf_counter()
+    c = O.range_verify(0, n, 16, True, 3, nthreads)
+    cdt = time.perf_counter() - t0
+    exact = (g.seeds_checked, g.failures, g.max_stopping_time, g.max_stopping_time_seed, g.max_excursion,
+             g.max_excursion_seed) == (c.seeds, c.failures, c.max_st, c.max_st_seed, c.max_exc, c.max_exc_seed)
+    return {"workload": "every n in [0, 2^32) (n >= 2), k=16 residue sieve (n >= 2^16) + mod-9 sieve",
+            "results": {"seeds_checked": g.seeds_checked, "failures": g.failures,
+                        "max_stopping_time": g.max_stopping_time,
+                        "max_stopping_time_seed": str(g.max_stopping_time_seed),
+                        "max_excursion": str(g.max_excursion), "max_excursion_seed": str(g.max_excursion_seed)},
+            "cpu": {"value": n / cdt, "unit": UNIT, "s": cdt, "cores": nthreads, "kind": "port",
+                    "arith": "u64, __builtin_mul_overflow on every odd run; seeds leaving 64 bits re-run in u128",
+                    "seeds_leaving_64_bits": c.wide64,
+                    "code": "oracle/collatz_oracle.c method 3 (run-length loop after cu:684-715)"},
+            "gpu": {"value": n / statistics.median(walls), "unit": UNIT, "wall_s": statistics.median(walls),
+                    "device_ms": statistics.median(devs), "call": "collatz_verify_range"},
+            "bit_exact_gpu_vs_cpu": bool(exact)}
+
+
+def _sig(x, d=4):
+    return float(f"{x:.{d}g}") if isinstance(x, (int, float)) and not isinstance(x, bool) else x
+
+
+def summary(line: dict) -> dict:
+    """The figures of every leg in a few hundred bytes, printed last on the line."""
+    def get(d, *ks):
+        for k in ks:
+            if not isinstance(d, dict):
+                return None
+            d = d.get(k)
+        return _sig(d)
+    s = {"block_seeds_per_s": get(line, "value"), "block_frac": get(line, "roofline", "frac"),
+         "block_e2e": get(line, "e2e", "value"), "cpu_baseline": get(line, "cpu_baseline", "value"),
+         "frontier_seeds_per_s": get(line, "frontier", "seeds_per_s"),
+         "frontier_frac": get(line, "frontier", "roofline", "frac"),
+         "frontier_widened": get(line, "frontier", "results", "widened"),
+         "config1_cpu_seeds_per_s": get(line, "config1", "cpu", "value"),
+         "config1_gpu_seeds_per_s": get(line, "config1", "gpu", "value"),
+         "config1_bit_exact": get(line, "config1", "bit_exact_gpu_vs_cpu"),
+         "batched_seeds_per_s": get(line, "batched", "batched_seeds_per_s"),
+         "batched_vs_plain": get(line, "batched", "speedup_vs_plain_wall"),
+         "batched_bit_exact": get(line, "batched", "bit_exact_vs_plain"),
+         "served_seeds_per_s": get(line, "served", "seeds_per_s"),
+         "served_vs_plain": get(line, "served", "served_vs_plain"),
+         "served_p50_ms": get(line, "served", "p50_ms"), "served_p99_ms": get(line, "served", "p99_ms"),
+         "served_range_p99_ms": get(line, "served", "range_p99_ms"),
+         "served_traj_p99_ms": get(line, "served", "traj_p99_ms"),
+         "served_bit_exact": get(line, "served", "bit_exact_vs_plain_sample"),
+         "cases_n45_seeds_per_s": get(line, "cases", "n45_seeds_per_s"),
+         "cases_match_reference": get(line, "cases", "all_match_reference"),
+         "cases_ref_gpu_program_s": get(line, "cases", "reference_gpu_program", "reference_s"),
+         "cases_cli_s": get(line, "cases", "reference_gpu_program", "cli_s"),
+         "cases_ref_gpu_program_run_s": get(line, "cases", "reference_gpu_program", "reference_run_s"),
+         "cases_cli_run_s": get(line, "cases", "reference_gpu_program", "cli_run_s")}
+    errs = [k for k in ("frontier", "config1", "batched", "served", "cases")
+            if isinstance(line.get(k), dict) and "error" in line[k]]
+    if errs:
+        s["errors_in"] = errs
+    return {k: x for k, x in s.items() if x is not None}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -508,26 +760,16 @@ def main():
     e2e_value = world * size / e2e_s
 
     if rank == 0:
-        from oracle import oracle as O
-        # algorithmic work per step: survivors x ops, runs per survivor from the
-        # oracle's jump+runs model on a fixed sample of this workload
-        samp = O.range_verify(base, 1 << 24, ksv, True, 2, min(8, os.cpu_count() or 1))
-        odd_per = samp.odd_runs / samp.seeds
-        even_per = samp.even_runs / samp.seeds
-        ops_per_seed = OPS_JUMP + OPS_ODD * odd_per + OPS_EVEN * even_per
-        ops_step = res.seeds_checked * ops_per_seed
-        mean_ms = sum(ms) / len(ms)
-        achieved = ops_step / (mean_ms / 1e3) / 1e12
         sm_mhz = clocks.get("sm_mhz") or 1965.0
-        issue_peak = sm_count * 128 * sm_mhz * 1e6 / 1e12
         # measured integer peak (collatz_int_peak, after the timed region): the
         # kernel mix's operations per SM clock, scaled to the clock sampled under load
         ipk = {m: v.int_peak(m) for m in (1, 0)}
-        peak = ipk[1]["ops_per_clk_sm"] * sm_count * sm_mhz * 1e6 / 1e12
+        roof = roofline(args.workload, base, ksv, res.seeds_checked, sum(ms) / len(ms), size, sm_count, sm_mhz,
+                        ipk)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * dev_s / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "scaling": "weak", "vs_baseline": None, "dtype": "u128 (4x u32 limbs)",
             "data": "synthetic (deterministic seed range)",
             "config": {"workload": f"range [2^{wl['offset_log2']} + r*2^{args.size_log2}, "
                                    f"2^{wl['offset_log2']} + (r+1)*2^{args.size_log2}) per rank r, k={ksv} "
@@ -544,43 +786,7 @@ def main():
                         "max_stopping_time_seed": str(res.max_stopping_time_seed),
                         "max_excursion": str(res.max_excursion),
                         "max_excursion_seed": str(res.max_excursion_seed), "errors": res.errors},
-            "roofline": {"bound": "int", "achieved": achieved, "peak": peak, "unit": "Tops/s (32-bit)",
-                         "frac": achieved / peak,
-                         "traffic": K_RANGE_DRAM_BYTES if args.workload == "block" else
-                         K_RANGE_FRONTIER_DRAM_BYTES_PER_BLOCK * max(1, size >> ksv),
-                         "traffic_basis": "dram__bytes_read.sum + dram__bytes_write.sum of one k_range "
-                                          "launch (ncu, 2^33 block); the k = 24 survivor table is read "
-                                          "from DRAM once per launch and from L2 after that, so the "
-                                          "figure does not grow with the block size"
-                                          if args.workload == "block" else
-                                          "ncu dram__bytes_read.sum + dram__bytes_write.sum of a 4-block "
-                                          "(2^36) launch, scaled by blocks: each 2^34 block streams the 5 "
-                                          "mod-9 classes it keeps (1.35 GB of the 2.43 GB survivor table)",
-                         "model": f"{ops_per_seed:.1f} algorithmic 32-bit ops per surviving seed "
-                                  f"({OPS_JUMP} + {OPS_ODD} x {odd_per:.2f} odd runs + {OPS_EVEN} x "
-                                  f"{even_per:.2f} even runs) x {res.seeds_checked} seeds per launch",
-                         "peak_basis": f"measured integer peak (collatz_int_peak mix 1: funnel shift, 3-input "
-                                       f"add, multiply-add chains on every SM): {ipk[1]['ops_per_clk_sm']:.1f} "
-                                       f"ops per SM clock x {sm_count} SMs x {sm_mhz:.0f} MHz (sampled median "
-                                       "SM clock); MEASURED_PEAKS.json has no integer peak",
-                         "int_peak_measured": {
-                             "mix1_kernel_mix": {"tops": ipk[1]["ops_per_s"] / 1e12,
-                                                 "ops_per_clk_sm": ipk[1]["ops_per_clk_sm"],
-                                                 "sm_mhz": ipk[1]["sm_mhz"]},
-                             "mix0_alu_only": {"tops": ipk[0]["ops_per_s"] / 1e12,
-                                               "ops_per_clk_sm": ipk[0]["ops_per_clk_sm"],
-                                               "sm_mhz": ipk[0]["sm_mhz"]}},
-                         "issue_peak": issue_peak,
-                         "frac_of_issue_peak": achieved / issue_peak,
-                         # issue-slot utilisation of the same kernel, measured with ncu on a smaller
-                         # launch of this workload: achieved/peak counts only the algorithmic ops, this
-                         # counts every issued instruction (work distribution included)
-                         "issue_slots_busy_ncu": K_RANGE_ISSUE_NCU[args.workload],
-                         "alu_pipe_busy_ncu": K_RANGE_ALU_PIPE_NCU[args.workload],
-                         "issue_basis": "sm__inst_issued.avg.pct_of_peak_sustained_active and "
-                                        "sm__pipe_alu_cycles_active.avg.pct_of_peak_sustained_active of one "
-                                        "k_range launch (profiles/k_range_2p38_block.md, "
-                                        "profiles/k_range_frontier_2p36.md, profiles/int_peak_mixes.md)"},
+            "roofline": roof,
             # request (32 B) + its work list: an aligned range of many blocks lowers to 55
             # 64-byte segments (5 kept mod-9 classes of the first and last block, 9 x 5 for the
             # blocks between), and the request's 4-byte first-segment index (threshold scouts)
@@ -592,19 +798,20 @@ def main():
             "gpu_launches": 4 * args.steps,
             "wall_s_timed": wall,
         }
+        nthreads = os.cpu_count() or 1
         if not args.no_cpu_baseline:
-            nthreads = os.cpu_count() or 1
-            rate, csize, cdt = cpu_sample(base, 15.0, ksv, nthreads)
-            line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": nthreads, "kind": "port",
-                                    "sample": f"[2^{wl['offset_log2']}, 2^{wl['offset_log2']} + {csize}) in "
-                                              f"{cdt:.1f} s (oracle run-length loop after cu:684-715, "
-                                              f"{nthreads} threads)"}
+            csize, csteps = 1 << CPU_SAMPLE_LOG2, 3
+            ctimes = cpu_reference_steps(base, csize, ksv, nthreads, csteps, 1)
+            line["cpu_baseline"] = {"value": csize * csteps / sum(ctimes), "unit": UNIT, "cores": nthreads,
+                                    "kind": "port", "sample": cpu_sample_desc(wl, csize, csteps, nthreads)}
         if world == 1 and not args.no_extras and args.workload == "block":
             def extra(fn):
                 try:
                     return fn()
                 except Exception as e:  # noqa: BLE001 -- the headline line is printed regardless
                     return {"error": f"{type(e).__name__}: {e}"}
+            line["frontier"] = extra(lambda: run_frontier(local, stream, flush, sm_count, ipk))
+            line["config1"] = extra(lambda: run_config1(local, nthreads))
             line["batched"] = extra(lambda: run_batched(v))
             # served load: a fraction of the batched configuration's capacity (requests of the
             # same offsets and sizes), else of the headline block's
@@ -612,6 +819,7 @@ def main():
             line["served"] = extra(lambda: run_served(v, cap, load=args.served_load,
                                                       duration=args.served_duration))
             line["cases"] = extra(run_cases)
+        line["summary"] = summary(line)
         print(json.dumps(line), flush=True)
     plan.close()
     v.close()

@@ -277,7 +277,8 @@ extern "C" int collatz_create(const collatz_config* cfg, collatz_ctx** out) {
     c->range_variant = (int)cfg->variant;
   }
   int rc = COLLATZ_OK;
-  cudaError_t e = cudaSetDevice(c->device);
+  DeviceScope dev_scope(c->device);
+  cudaError_t e = dev_scope.err;
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);
   for (int i = 0; i < 4 && e == cudaSuccess; i++) e = cudaEventCreate(&c->ev[i]);
@@ -296,7 +297,7 @@ extern "C" int collatz_create(const collatz_config* cfg, collatz_ctx** out) {
 
 extern "C" void collatz_destroy(collatz_ctx* c) {
   if (!c) return;
-  cudaSetDevice(c->device);
+  DeviceScope dev_scope(c->device);
   if (c->own_stream) cudaStreamSynchronize(c->own_stream);
   if (c->stream && c->stream != c->own_stream) cudaStreamSynchronize(c->stream);
   free_case_tables(&c->ct);
@@ -415,7 +416,7 @@ static int case_finish(collatz_ctx* c, collatz_case_result* out) {
     for (uint64_t i = 0; i < n; i++) limbs4(seeds[i], out->overflow_seeds + 4 * i);
   }
   if (r.errors) {
-    c->err = "device error bits 0x" + std::to_string(r.errors);
+    c->err = "device error bits " + hex_u32(r.errors);
     return COLLATZ_E_DEVICE;
   }
   return COLLATZ_OK;
@@ -424,14 +425,15 @@ static int case_finish(collatz_ctx* c, collatz_case_result* out) {
 extern "C" int collatz_verify_pairs(collatz_ctx* c, uint32_t bigindex, const uint32_t* pairs, uint32_t npairs,
                                     collatz_case_result* out) {
   if (!c || !out || (npairs && !pairs)) return COLLATZ_E_ARG;
-  if (c->ct.tpo + bigindex >= POW3_COUNT) return COLLATZ_E_ARG;
+  if (bigindex >= POW3_COUNT || (uint64_t)c->ct.tpo + bigindex >= POW3_COUNT) return COLLATZ_E_ARG;
   std::lock_guard<std::recursive_mutex> g(c->mu);
   uint32_t* ovbuf = out->overflow_seeds;
   const uint64_t ovcap = out->overflow_cap;
   std::memset(out, 0, sizeof *out);
   out->overflow_seeds = ovbuf;
   out->overflow_cap = ovcap;
-  CK(c, cudaSetDevice(c->device));
+  DeviceScope dev_scope(c->device);
+  CK(c, dev_scope.err);
   int rc = case_prepare(c);
   if (rc) return rc;
   if (npairs) {
@@ -850,7 +852,8 @@ extern "C" int collatz_run_case(collatz_ctx* c, const collatz_case* cs, collatz_
   std::memset(out, 0, sizeof *out);
   out->overflow_seeds = ovbuf;
   out->overflow_cap = ovcap;
-  CK(c, cudaSetDevice(c->device));
+  DeviceScope dev_scope(c->device);
+  CK(c, dev_scope.err);
   int rc = case_prepare(c);
   if (rc) return rc;
   return (c->cfg.flags & COLLATZ_CFG_HOST_STEP1) ? run_case_host(c, cs, out) : run_case_device(c, cs, out);
@@ -974,7 +977,8 @@ extern "C" int collatz_run_case_batch(collatz_ctx* c, const collatz_case* cases,
     if (cases[i].sigfig > c->ct.mbi || cases[i].threepower >= 128) return COLLATZ_E_ARG;
   std::lock_guard<std::recursive_mutex> g(c->mu);
   std::memset(out, 0, sizeof(collatz_case_result) * n);
-  CK(c, cudaSetDevice(c->device));
+  DeviceScope dev_scope(c->device);
+  CK(c, dev_scope.err);
   uint64_t used = 0;
   int status = COLLATZ_OK;
   std::vector<uint32_t> shallow;
@@ -1019,7 +1023,8 @@ extern "C" int collatz_step1_pairs_device(collatz_ctx* c, const collatz_case* cs
   if (!c || !cs || !count || (cap && !pairs)) return COLLATZ_E_ARG;
   if (cs->sigfig > c->ct.mbi || cs->threepower >= 128) return COLLATZ_E_ARG;
   std::lock_guard<std::recursive_mutex> g(c->mu);
-  CK(c, cudaSetDevice(c->device));
+  DeviceScope dev_scope(c->device);
+  CK(c, dev_scope.err);
   S1Run R;
   int rc = s1_count(c, cs, R);
   if (rc) return rc;
@@ -1184,7 +1189,8 @@ static int plan_build(collatz_ctx* c, const collatz_range* r, uint32_t n, collat
 extern "C" int collatz_plan_create(collatz_ctx* c, const collatz_range* r, uint32_t n, collatz_plan** out) {
   if (!c || !r || !n || !out) return COLLATZ_E_ARG;
   std::lock_guard<std::recursive_mutex> g(c->mu);
-  CK(c, cudaSetDevice(c->device));
+  DeviceScope dev_scope(c->device);
+  CK(c, dev_scope.err);
   collatz_plan* p = new collatz_plan();
   p->c = c;
   int rc = plan_build(c, r, n, p);
@@ -1200,6 +1206,8 @@ extern "C" int collatz_plan_launch(collatz_plan* p) {
   if (!p || !p->exec) return COLLATZ_E_ARG;
   collatz_ctx* c = p->c;
   std::lock_guard<std::recursive_mutex> g(c->mu);
+  DeviceScope dev_scope(c->device);
+  CK(c, dev_scope.err);
   CK(c, cudaEventRecord(c->ev[2], c->stream));
   CK(c, cudaGraphLaunch(p->exec, c->stream));
   CK(c, cudaEventRecord(c->ev[3], c->stream));
@@ -1210,6 +1218,8 @@ extern "C" int collatz_plan_results(collatz_plan* p, collatz_range_result* out) 
   if (!p || !out) return COLLATZ_E_ARG;
   collatz_ctx* c = p->c;
   std::lock_guard<std::recursive_mutex> g(c->mu);
+  DeviceScope dev_scope(c->device);
+  CK(c, dev_scope.err);
   CK(c, cudaStreamSynchronize(c->stream));
   float ms = 0;
   cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);
@@ -1235,6 +1245,7 @@ extern "C" int collatz_plan_results(collatz_plan* p, collatz_range_result* out) 
 
 extern "C" void collatz_plan_destroy(collatz_plan* p) {
   if (!p) return;
+  DeviceScope dev_scope(p->c->device);
   if (p->exec) cudaGraphExecDestroy(p->exec);
   if (p->graph) cudaGraphDestroy(p->graph);
   p->d_segs.release();
@@ -1264,7 +1275,8 @@ extern "C" int collatz_verify_batch(collatz_ctx* c, const collatz_range* r, uint
     return rc;
   }
   std::lock_guard<std::recursive_mutex> g(c->mu);
-  CK(c, cudaSetDevice(c->device));
+  DeviceScope dev_scope(c->device);
+  CK(c, dev_scope.err);
   std::vector<RangeSeg>& segs = c->range_segs;
   segs.clear();
   unsigned long long items = 0;
@@ -1321,7 +1333,8 @@ extern "C" int collatz_trajectory(collatz_ctx* c, const uint32_t* seeds, uint32_
   if (!c || (n && (!seeds || !st || !exc || !status))) return COLLATZ_E_ARG;
   if (n == 0) return COLLATZ_OK;
   std::lock_guard<std::recursive_mutex> g(c->mu);
-  CK(c, cudaSetDevice(c->device));
+  DeviceScope dev_scope(c->device);
+  CK(c, dev_scope.err);
   static const int classes[5] = {4, 6, 8, 12, 16};
   std::vector<std::vector<uint32_t>> lists(5);
   for (uint32_t i = 0; i < n; i++) {
@@ -1385,7 +1398,8 @@ extern "C" int collatz_trajectory(collatz_ctx* c, const uint32_t* seeds, uint32_
 extern "C" int collatz_case_tables(collatz_ctx* c, uint32_t* bv, uint32_t* mod9) {
   if (!c || !bv || !mod9) return COLLATZ_E_ARG;
   std::lock_guard<std::recursive_mutex> g(c->mu);
-  CK(c, cudaSetDevice(c->device));
+  DeviceScope dev_scope(c->device);
+  CK(c, dev_scope.err);
   CK(c, cudaMemcpy(bv, c->ct.bv, sizeof(uint32_t) * 16 * BV_WORDS_HOST, cudaMemcpyDeviceToHost));
   CK(c, cudaMemcpy(mod9, c->ct.mod9, sizeof(uint32_t) * 9 * 32, cudaMemcpyDeviceToHost));
   return COLLATZ_OK;
@@ -1394,7 +1408,8 @@ extern "C" int collatz_case_tables(collatz_ctx* c, uint32_t* bv, uint32_t* mod9)
 extern "C" int collatz_range_sieve(collatz_ctx* c, uint32_t k, uint8_t* bits, uint64_t* count) {
   if (!c || k < 8 || k > 34) return COLLATZ_E_ARG;
   std::lock_guard<std::recursive_mutex> g(c->mu);
-  CK(c, cudaSetDevice(c->device));
+  DeviceScope dev_scope(c->device);
+  CK(c, dev_scope.err);
   RangeTables* T = nullptr;
   int rc = get_range_tables(c, k, &T);
   if (rc) return rc;

@@ -75,7 +75,8 @@ extern "C" int collatz_int_peak(collatz_ctx* ctx, int mix, collatz_int_peak_t* o
   if (!ctx || !out || (mix != 0 && mix != 1)) return COLLATZ_E_ARG;
   std::lock_guard<std::recursive_mutex> g(ctx->mu);
   std::memset(out, 0, sizeof *out);
-  cudaError_t e = cudaSetDevice(ctx->device);
+  DeviceScope dev_scope(ctx->device);
+  cudaError_t e = dev_scope.err;
   const uint32_t grid = (uint32_t)ctx->sm_count * PEAK_BLOCKS_PER_SM;
   const uint32_t threads = grid * PEAK_BLOCK;
   // 2^17 iterations: 24 operations per iteration and thread, about 30 ms per launch

@@ -19,8 +19,15 @@
 //    call; a larger overflow_cap is rejected with COLLATZ_E_LIMIT;
 //  * every call shares the array: the call clears it first, and calls that
 //    overlap on the GPU (several host threads or streams at once) race;
-//  * the first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress); make that first call before any stream capture.
+//  * every call looks up the array's device address (cudaGetSymbolAddress)
+//    with the context's device current, so the address stays right after the
+//    host application resets or recreates the primary context; the first call
+//    on a device also loads the module, so make it before any stream capture;
+//  * when the caller's overflow_cap is smaller than the number of overflow
+//    seeds, the smallest overflow_cap seeds are returned, as by
+//    collatz_verify_pairs (the device list is read in fixed-size pieces
+//    through a stack buffer and kept in a bounded heap in the caller's
+//    buffer, so no host memory is allocated either).
 #include <algorithm>
 #include <cstring>
 #include <mutex>
@@ -42,22 +49,24 @@ static_assert(sizeof(ReqRec) <= NOALLOC_COUNTER_OFF, "scratch layout");
 // device array; kernels get its device address from cudaGetSymbolAddress.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 
-// Device address of g_noalloc_scratch per device, looked up once per device
-// with that device current.
-static std::mutex g_noalloc_mu;
-static void* g_noalloc_addr[256];
-
-static cudaError_t noalloc_scratch(int device, unsigned char** out) {
-  if (device < 0 || device >= 256) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> g(g_noalloc_mu);
-  if (!g_noalloc_addr[device]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return e;
-    g_noalloc_addr[device] = p;
-  }
-  *out = static_cast<unsigned char*>(g_noalloc_addr[device]);
+// Device address of g_noalloc_scratch on the current device.
+static cudaError_t noalloc_scratch(unsigned char** out) {
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return e;
+  *out = static_cast<unsigned char*>(p);
   return cudaSuccess;
+}
+
+// An overflow seed as the kernel reports it: limbs 0..2 of a 96-bit value
+// (limb 3 unused), ordered by value.
+struct Seed4 {
+  uint32_t w[4];
+};
+static bool seed_less(const Seed4& x, const Seed4& y) {
+  for (int i = 2; i >= 0; i--)
+    if (x.w[i] != y.w[i]) return x.w[i] < y.w[i];
+  return false;
 }
 
 }  // namespace cz
@@ -73,21 +82,23 @@ using namespace cz;
 extern "C" int collatz_verify_pairs_noalloc(collatz_ctx* c, uint32_t bigindex, const uint32_t* d_pairs,
                                             uint32_t npairs, collatz_case_result* out) {
   if (!c || !out || (npairs && !d_pairs)) return COLLATZ_E_ARG;
-  if (c->ct.tpo + bigindex >= POW3_COUNT) return COLLATZ_E_ARG;
-  if (out->overflow_cap > NOALLOC_OVERFLOW_MAX || (out->overflow_cap && !out->overflow_seeds)) {
+  if (bigindex >= POW3_COUNT || (uint64_t)c->ct.tpo + bigindex >= POW3_COUNT) return COLLATZ_E_ARG;
+  if (out->overflow_cap && !out->overflow_seeds) return COLLATZ_E_ARG;
+  std::lock_guard<std::recursive_mutex> g(c->mu);
+  if (out->overflow_cap > NOALLOC_OVERFLOW_MAX) {
     c->err = "collatz_verify_pairs_noalloc: overflow_cap " + std::to_string(out->overflow_cap) +
              " exceeds the allocation-free maximum of " + std::to_string(NOALLOC_OVERFLOW_MAX) + " seeds";
     return COLLATZ_E_LIMIT;
   }
-  std::lock_guard<std::recursive_mutex> g(c->mu);
   uint32_t* ovbuf = out->overflow_seeds;
   const uint64_t ovcap = out->overflow_cap;
   std::memset(out, 0, sizeof *out);
   out->overflow_seeds = ovbuf;
   out->overflow_cap = ovcap;
-  NA_CK(c, cudaSetDevice(c->device));
+  DeviceScope dev_scope(c->device);
+  NA_CK(c, dev_scope.err);
   unsigned char* base = nullptr;
-  NA_CK(c, noalloc_scratch(c->device, &base));
+  NA_CK(c, noalloc_scratch(&base));
   ReqRec* d_rec = reinterpret_cast<ReqRec*>(base + NOALLOC_REC_OFF);
   unsigned long long* d_ovcount = reinterpret_cast<unsigned long long*>(base + NOALLOC_OVCOUNT_OFF);
   // the previous call's contents stay in the array: clear the record and the counters
@@ -144,22 +155,34 @@ extern "C" int collatz_verify_pairs_noalloc(collatz_ctx* c, uint32_t bigindex, c
     out->max_stopping_time = r.st;
     std::memcpy(out->max_stopping_time_seed, r.st_seed, sizeof out->max_stopping_time_seed);
   }
-  const uint64_t have = std::min<uint64_t>(std::min<uint64_t>(nov, NOALLOC_OVERFLOW_MAX), ovcap);
-  if (have) {
-    // copy straight into the caller's buffer, then sort in place (no allocation)
-    NA_CK(c, cudaMemcpy(out->overflow_seeds, base + NOALLOC_OVERFLOW_OFF, 16 * have, cudaMemcpyDeviceToHost));
-    struct Seed4 {
-      uint32_t w[4];
-    };
-    Seed4* s = reinterpret_cast<Seed4*>(out->overflow_seeds);
-    std::sort(s, s + have, [](const Seed4& x, const Seed4& y) {
-      for (int i = 3; i >= 0; i--)
-        if (x.w[i] != y.w[i]) return x.w[i] < y.w[i];
-      return false;
-    });
+  const uint64_t have = std::min<uint64_t>(nov, NOALLOC_OVERFLOW_MAX);
+  const uint64_t keep = std::min<uint64_t>(have, ovcap);
+  if (keep) {
+    // the smallest `keep` of the `have` device entries: read them in pieces through a
+    // stack buffer into a max-heap of at most `keep` seeds held in the caller's buffer,
+    // then sort the heap (no allocation)
+    Seed4* heap = reinterpret_cast<Seed4*>(out->overflow_seeds);
+    uint64_t n = 0;
+    Seed4 piece[128];
+    for (uint64_t i = 0; i < have; i += 128) {
+      const uint64_t m = std::min<uint64_t>(128, have - i);
+      NA_CK(c, cudaMemcpy(piece, base + NOALLOC_OVERFLOW_OFF + 16 * i, 16 * m, cudaMemcpyDeviceToHost));
+      for (uint64_t j = 0; j < m; j++) {
+        piece[j].w[3] = 0;
+        if (n < keep) {
+          heap[n++] = piece[j];
+          std::push_heap(heap, heap + n, seed_less);
+        } else if (seed_less(piece[j], heap[0])) {
+          std::pop_heap(heap, heap + n, seed_less);
+          heap[n - 1] = piece[j];
+          std::push_heap(heap, heap + n, seed_less);
+        }
+      }
+    }
+    std::sort_heap(heap, heap + n, seed_less);
   }
   if (r.errors) {
-    c->err = "device error bits 0x" + std::to_string(r.errors);
+    c->err = "device error bits " + hex_u32(r.errors);
     return COLLATZ_E_DEVICE;
   }
   return COLLATZ_OK;

@@ -63,6 +63,38 @@ struct HostBuf {
   }
 };
 
+// Makes a device current for the lifetime of the object and then restores
+// the device that was current for the calling thread, so that a library call
+// does not change the caller's current device.
+struct DeviceScope {
+  int prev = -1;
+  cudaError_t err = cudaSuccess;
+  explicit DeviceScope(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) err = cudaSetDevice(dev);
+  }
+  ~DeviceScope() {
+    int now = -1;
+    if (prev >= 0 && cudaGetDevice(&now) == cudaSuccess && now != prev) cudaSetDevice(prev);
+  }
+  DeviceScope(const DeviceScope&) = delete;
+  DeviceScope& operator=(const DeviceScope&) = delete;
+};
+
+// "0x" followed by the value in upper-case hexadecimal.
+inline std::string hex_u32(uint32_t x) {
+  static const char* d = "0123456789ABCDEF";
+  std::string s = "0x";
+  bool lead = true;
+  for (int i = 28; i >= 0; i -= 4) {
+    const uint32_t n = (x >> i) & 15u;
+    if (lead && n == 0 && i) continue;
+    lead = false;
+    s += d[n];
+  }
+  return s;
+}
+
 constexpr uint32_t WIDEN_CAP = 1u << 16;
 constexpr uint32_t OVERFLOW_CAP = 1u << 16;
 constexpr uint32_t CASE_BATCH = 1u << 20;  // pairs per device batch in run_case

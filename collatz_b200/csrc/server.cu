@@ -756,7 +756,8 @@ extern "C" int collatz_server_start(const collatz_config* cfg, const collatz_ser
     destroy(s);
     return COLLATZ_E_CUDA;
   };
-  cudaError_t e = cudaSetDevice(c->device);
+  DeviceScope dev_scope(c->device);
+  cudaError_t e = dev_scope.err;
   if (e) return fail(e, "cudaSetDevice");
   int lo = 0, hi = 0;
   cudaDeviceGetStreamPriorityRange(&lo, &hi);

@@ -194,6 +194,8 @@ void tune_on_create(collatz_ctx* c) {
 extern "C" int collatz_autotune(collatz_ctx* c, uint32_t flags, collatz_tune_result* out) {
   if (!c) return COLLATZ_E_ARG;
   std::lock_guard<std::recursive_mutex> g(c->mu);
+  DeviceScope dev_scope(c->device);
+  if (dev_scope.err != cudaSuccess) return set_cuda_error(c, dev_scope.err, "collatz_autotune");
   collatz_tune_result res;
   std::memset(&res, 0, sizeof res);
   for (int i = 0; i < 8; i++) res.range_ms[i] = res.cases_ms[i] = -1.0f;

@@ -1,6 +1,7 @@
 #!/usr/bin/env bash
 # Builds the reference program for the CPU, from its own source where it lies
-# (default /root/reference/collatz_cudav7.cu), through the fake CUDA runtime
+# ($REF_DIR/collatz_cudav7.cu; REF_DIR defaults to the directory "reference"
+# beside this repository), through the fake CUDA runtime
 # header in oracle/ref_shim/.  Outputs go only to oracle/_ref/ (git-ignored).
 #
 # The source is compiled as written except for three mechanical edits that
@@ -13,7 +14,7 @@
 # Products per N: ref_N<N> (the reference program: stdin 6-tuple, stdout
 # overflow seeds, stderr summary) and ref_tool_N<N> (oracle/ref_shim/ref_tool.cpp).
 set -euo pipefail
-REF_DIR=${REF_DIR:-/root/reference}
+REF_DIR=${REF_DIR:-$(cd "$(dirname "$0")/../.." && pwd)/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
 NS=${NS:-"26 30 36 40 42 45"}

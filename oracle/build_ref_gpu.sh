@@ -1,6 +1,7 @@
 #!/usr/bin/env bash
 # Builds the reference program for the B200 (sm_100a) from its own source
-# where it lies (default /root/reference/collatz_cudav7.cu), to time the
+# where it lies ($REF_DIR/collatz_cudav7.cu; REF_DIR defaults to the directory
+# "reference" beside this repository), to time the
 # reference's own CUDA kernel on the same GPU as the product in cases mode.
 # Outputs go only to oracle/_ref/ (git-ignored).  The source is compiled as
 # written; the one edit sets MAXBITS (cu:43, a compile-time constant) to each
@@ -8,7 +9,7 @@
 # Products: oracle/_ref/ref_gpu_N<N> (stdin 6-tuple, stdout overflow seeds,
 # stderr summary, exactly as the reference program).
 set -euo pipefail
-REF_DIR=${REF_DIR:-/root/reference}
+REF_DIR=${REF_DIR:-$(cd "$(dirname "$0")/../.." && pwd)/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
 NS=${NS:-"45"}

@@ -407,6 +407,27 @@ uint64_t orc_range_sieve(uint32_t k, uint8_t *bits) {
   return count;
 }
 
+/* Sieve tables kept for the life of the process, one per k <= 26, built on
+ * first use under a lock (repeated range calls then pay for the table once). */
+static pthread_mutex_t g_sieve_mu = PTHREAD_MUTEX_INITIALIZER;
+static uint8_t *g_sieve[27];
+static const uint8_t *cached_sieve(uint32_t k) {
+  if (k == 0 || k > 26) return NULL;
+  pthread_mutex_lock(&g_sieve_mu);
+  if (!g_sieve[k]) {
+    uint8_t *b = (uint8_t *)malloc((size_t)((1ull << k) + 7) / 8);
+    if (b) orc_range_sieve(k, b);
+    g_sieve[k] = b;
+  }
+  const uint8_t *out = g_sieve[k];
+  pthread_mutex_unlock(&g_sieve_mu);
+  return out;
+}
+/* The first j <= k0 parity steps of r depend only on r mod 2^k0, so a residue
+ * removed by the 2^k0 sieve is removed by every 2^k sieve with k >= k0: the
+ * direct test of a large k first looks r mod 2^20 up in the cached table. */
+#define DIRECT_PREFILTER_K 20u
+
 uint64_t orc_range_sieve_validate(uint32_t k) {
   uint64_t bad = 0;
   for (uint64_t r = 0; r < (1ull << k); r++) {
@@ -501,7 +522,7 @@ static int big_seed(const big *n, uint64_t *st_out, big *E_out, uint64_t *steps)
 }
 
 typedef struct {
-  uint64_t seeds, failures, steps, odd_runs, even_runs;
+  uint64_t seeds, failures, steps, odd_runs, even_runs, wide64;
   big E;
   u128 E_seed;
   uint64_t st;
@@ -535,6 +556,7 @@ static void acc_merge(range_acc *a, const range_acc *b) {
   a->steps += b->steps;
   a->odd_runs += b->odd_runs;
   a->even_runs += b->even_runs;
+  a->wide64 += b->wide64;
   if (!b->have) return;
   if (!a->have) {
     a->have = 1;
@@ -641,6 +663,52 @@ wide : {
   }
   acc_seed(a, n, st2, &Eb);
 }
+}
+
+/* method 3: method 1 in uint64_t with overflow detection.  The odd run's
+ * multiply 3^a (v >> a) is checked with __builtin_mul_overflow; the even
+ * run only shrinks the value.  A seed whose value would leave 64 bits is
+ * re-run with the 128-bit method 1 (counted in wide64), so the results
+ * equal method 1's. */
+static void seed_runs64(range_acc *a, u128 n128) {
+  if (n128 >> 63) {
+    a->wide64++;
+    seed_runs(a, n128);
+    return;
+  }
+  const uint64_t n = (uint64_t)n128;
+  uint64_t v = n + 1, E = n, st = 0;
+  uint64_t odd = 0, even = 0;
+  for (;;) {
+    unsigned oa = ctz32((uint32_t)v | (1u << 8));
+    uint64_t w;
+    if (__builtin_mul_overflow(v >> oa, (uint64_t)P3[oa], &w)) {
+      a->wide64++;
+      seed_runs(a, n128);
+      return;
+    }
+    v = w;
+    st += oa;
+    odd++;
+    if (v - 1 > E) E = v - 1;
+    const uint64_t m = v - 1;
+    unsigned b = ctz32((uint32_t)m | 0x80000000u);
+    even++;
+    if ((m >> b) < n) {
+      unsigned i = 1;
+      while ((m >> i) >= n) i++;
+      st += i;
+      break;
+    }
+    st += b;
+    v = (m >> b) + 1;
+  }
+  big Eb;
+  big_from_u128(&Eb, E);
+  a->steps += st;
+  a->odd_runs += odd;
+  a->even_runs += even;
+  acc_seed(a, n128, st, &Eb);
 }
 
 /* method 2: the device kernel's structure for sieved seeds n >= 2^k: the
@@ -809,6 +877,7 @@ typedef struct {
   uint32_t k;
   int use_mod9, method, neg;
   const uint8_t *bits;
+  const uint8_t *pre; /* direct test: the 2^DIRECT_PREFILTER_K sieve, or NULL */
   range_acc acc;
 } range_job;
 
@@ -827,7 +896,13 @@ static void *range_worker(void *p) {
     }
     if (j->k && n >= K) {
       uint64_t r = (uint64_t)n & mask;
-      if (j->bits ? !((j->bits[r >> 3] >> (r & 7)) & 1) : !residue_survives_v(r, j->k, j->neg)) continue;
+      if (j->bits) {
+        if (!((j->bits[r >> 3] >> (r & 7)) & 1)) continue;
+      } else {
+        const uint64_t rp = r & ((1ull << DIRECT_PREFILTER_K) - 1);
+        if (j->pre && !((j->pre[rp >> 3] >> (rp & 7)) & 1)) continue;
+        if (!residue_survives_v(r, j->k, j->neg)) continue;
+      }
     }
     j->acc.seeds++;
     if (j->neg) {
@@ -839,6 +914,8 @@ static void *range_worker(void *p) {
         seed_runs_neg(&j->acc, n);
     } else if (j->method == 0) {
       seed_steps(&j->acc, n);
+    } else if (j->method == 3) {
+      seed_runs64(&j->acc, n);
     } else if (j->method == 2 && j->k && n >= K) {
       seed_jump_runs(&j->acc, n, j->k);
     } else {
@@ -865,11 +942,12 @@ int orc_range_ex(uint64_t offset_lo, uint64_t offset_hi, uint64_t size,
   const int neg = (flags & ORC_RANGE_NEGATIVE) != 0;
   const int direct_sieve = neg || (flags & ORC_RANGE_DIRECT_SIEVE);
   memset(out, 0, sizeof *out);
-  uint8_t *bits = NULL;
+  const uint8_t *bits = NULL, *pre = NULL;
   if (k && !direct_sieve) {
-    bits = (uint8_t *)malloc((size_t)((1ull << k) + 7) / 8);
+    bits = cached_sieve(k);
     if (!bits) return -2;
-    orc_range_sieve(k, bits);
+  } else if (k > DIRECT_PREFILTER_K && !neg) {
+    pre = cached_sieve(DIRECT_PREFILTER_K);
   }
   range_job *jobs = (range_job *)calloc((size_t)nthreads, sizeof *jobs);
   pthread_t *th = (pthread_t *)calloc((size_t)nthreads, sizeof *th);
@@ -885,6 +963,7 @@ int orc_range_ex(uint64_t offset_lo, uint64_t offset_hi, uint64_t size,
     jobs[i].method = method;
     jobs[i].neg = neg;
     jobs[i].bits = bits;
+    jobs[i].pre = pre;
   }
   for (int i = 1; i < nthreads; i++) pthread_create(&th[i], NULL, range_worker, &jobs[i]);
   range_worker(&jobs[0]);
@@ -897,6 +976,7 @@ int orc_range_ex(uint64_t offset_lo, uint64_t offset_hi, uint64_t size,
   out->steps = tot.steps;
   out->odd_runs = tot.odd_runs;
   out->even_runs = tot.even_runs;
+  out->wide64 = tot.wide64;
   if (tot.have) {
     big_to_u32(&tot.E, out->max_exc);
     for (int i = 0; i < 4; i++) {
@@ -907,7 +987,6 @@ int orc_range_ex(uint64_t offset_lo, uint64_t offset_hi, uint64_t size,
   }
   free(jobs);
   free(th);
-  free(bits);
   return 0;
 }
 

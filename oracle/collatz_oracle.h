@@ -76,6 +76,7 @@ typedef struct {
   uint32_t max_st_seed[4];
   uint64_t steps;        /* T-steps executed from the seed */
   uint64_t odd_runs, even_runs;
+  uint64_t wide64;       /* method 3: seeds whose value left 64 bits (re-run in 128) */
 } orc_range_result;
 
 /* ---------------- cases mode (reference restatement) ---------------- */
@@ -133,7 +134,11 @@ uint64_t orc_range_sieve_validate(uint32_t k);
  * in {0,1,3,6,7} (when use_mod9), and, when n >= 2^k, r = n mod 2^k a
  * sieve survivor (k = 0: no residue sieve).  method 0 = single T-steps,
  * 1 = run-length loop after search3 (cu:684-715), 2 = the GPU kernel's
- * structure (one k-step jump, then method 1; counts runs after the jump).
+ * structure (one k-step jump, then method 1; counts runs after the jump),
+ * 3 = method 1 in 64-bit unsigned arithmetic with overflow detection
+ * (__builtin_mul_overflow on each odd run's multiply; a seed whose value
+ * would leave 64 bits is re-run with method 1 and counted in wide64) -- the
+ * plain CPU verification of n < 2^32 with 64-bit values.
  * All methods give identical results.  nthreads >= 1. */
 int orc_range(uint64_t offset_lo, uint64_t offset_hi, uint64_t size,
               uint32_t k, int use_mod9, int method, int nthreads,

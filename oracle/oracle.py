@@ -60,7 +60,8 @@ class _RangeResult(C.Structure):
     _fields_ = [("seeds", C.c_uint64), ("failures", C.c_uint64),
                 ("max_exc", C.c_uint32 * 16), ("max_exc_seed", C.c_uint32 * 4),
                 ("max_st", C.c_uint64), ("max_st_seed", C.c_uint32 * 4),
-                ("steps", C.c_uint64), ("odd_runs", C.c_uint64), ("even_runs", C.c_uint64)]
+                ("steps", C.c_uint64), ("odd_runs", C.c_uint64), ("even_runs", C.c_uint64),
+                ("wide64", C.c_uint64)]
 
 
 def _u128(x: _U128) -> int:
@@ -281,6 +282,7 @@ class RangeResult:
     steps: int
     odd_runs: int
     even_runs: int
+    wide64: int = 0
 
 
 def range_verify(offset: int, size: int, k: int, use_mod9: bool = True, method: int = 1,
@@ -299,7 +301,7 @@ def range_verify(offset: int, size: int, k: int, use_mod9: bool = True, method: 
     if rc:
         raise ValueError(f"orc_range rc={rc}")
     return RangeResult(r.seeds, r.failures, _limbs(r.max_exc), _limbs(r.max_exc_seed),
-                       r.max_st, _limbs(r.max_st_seed), r.steps, r.odd_runs, r.even_runs)
+                       r.max_st, _limbs(r.max_st_seed), r.steps, r.odd_runs, r.even_runs, r.wide64)
 
 
 def range_sieve(k: int) -> tuple[int, bytes]:

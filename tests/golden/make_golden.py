@@ -1,7 +1,7 @@
 """Generates the golden fixtures in tests/golden/ from the reference itself.
 
-Runs in the development container only (it needs the reference sources under
-/root/reference): oracle/build_ref.sh compiles collatz_cudav7.cu for the CPU
+Runs where the reference sources are present ($REF_DIR, else the directory
+"reference" beside this repository): oracle/build_ref.sh compiles collatz_cudav7.cu for the CPU
 through oracle/ref_shim/, then this script records
 
   cases_runs.json   whole reference runs (stdin 6-tuple -> hash, launches,
@@ -30,7 +30,8 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 from oracle import oracle as O  # noqa: E402
 
-REF = os.environ.get("REF_DIR", "/root/reference")
+# the reference project: $REF_DIR, else the directory "reference" beside this repository
+REF = os.environ.get("REF_DIR", os.path.join(os.path.dirname(ROOT), "reference"))
 OUT = os.path.join(ROOT, "oracle", "_ref")
 
 

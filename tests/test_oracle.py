@@ -148,6 +148,21 @@ def test_range_methods_agree(case):
     assert keys[0] == keys[1] == keys[2]
 
 
+@pytest.mark.parametrize("case", [(0, 1 << 22, 16), ((1 << 32) - (1 << 20), 1 << 20, 16),
+                                  ((1 << 62) + 1, 1 << 16, 16), ((1 << 64) - (1 << 17), 1 << 18, 16)])
+def test_range_u64_method_equals_u128(case):
+    """The 64-bit loop with overflow detection (the plain verification of
+    n < 2^32 in 64-bit arithmetic) gives the 128-bit loop's results; near
+    2^62..2^64 some seeds leave 64 bits and are re-run in 128 bits."""
+    from oracle import oracle as O
+    off, size, k = case
+    a = O.range_verify(off, size, k, True, method=1, nthreads=4)
+    b = O.range_verify(off, size, k, True, method=3, nthreads=4)
+    assert (a.seeds, a.failures, a.max_st, a.max_st_seed, a.max_exc, a.max_exc_seed) == \
+        (b.seeds, b.failures, b.max_st, b.max_st_seed, b.max_exc, b.max_exc_seed)
+    assert (b.wide64 > 0) == (off >= 1 << 62)
+
+
 @pytest.mark.parametrize("case", [(1 << 40, 1 << 18, 16), ((1 << 60) + 12345, 1 << 17, 20), (3, 1 << 16, 12),
                                   ((1 << 50) - 4096, 1 << 16, 24)])
 def test_range_direct_sieve_equals_table(case):

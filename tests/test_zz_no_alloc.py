@@ -70,3 +70,40 @@ def test_noalloc_rejects_oversized_report():
     assert rc == cb.E_LIMIT
     assert "4064" in cb.lib().collatz_last_error(v.handle).decode()
     v.close()
+
+
+def test_noalloc_small_cap_returns_the_smallest_seeds():
+    """With an overflow_cap of 1 or 2 and more overflow seeds than that, both
+    entry points return the smallest seeds, twice in a row."""
+    import torch
+    cb, f = _lib()
+    v = cb.Verifier(45)
+    fx = load_golden("pairs_N45.json")
+    batches = [b for b in fx["batches"] if 2 < len(b["overflow"]) <= NOALLOC_OVERFLOW_MAX]
+    assert batches
+    for b in batches[:2]:
+        pairs = [(int(x), int(y)) for x, y in b["pairs"]]
+        packed = cb.pack_pairs(pairs)
+        dev = torch.tensor(list(packed), dtype=torch.int64).to(torch.int32).cuda()
+        torch.cuda.synchronize()
+        for cap in (1, 2):
+            ref = v.launchkernel(b["bigindex"], pairs, overflow_cap=cap)
+            assert ref.n_overflow == len(b["overflow"]) > cap
+            for _ in range(2):
+                rc, got = _noalloc(cb, f, v, b["bigindex"], dev.data_ptr(), len(pairs), cap)
+                assert rc == 0
+                assert got.overflow == ref.overflow and len(got.overflow) == cap
+                assert _key(got) == _key(ref)
+    v.close()
+
+
+def test_noalloc_rejects_null_report_buffer():
+    import torch
+    cb, f = _lib()
+    v = cb.Verifier(26)
+    dev = torch.zeros(8, dtype=torch.int32, device="cuda")
+    out = cb.CaseResultC()
+    out.overflow_cap = 4
+    rc = f(v.handle, 0, C.c_void_p(dev.data_ptr()), 1, C.byref(out))
+    assert rc == cb.E_ARG
+    v.close()
