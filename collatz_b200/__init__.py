@@ -72,11 +72,17 @@ class RangeResultC(C.Structure):
 
 REQ_RANGE, REQ_TRAJECTORY = 0, 1
 TUNE_RANGE, TUNE_CASES, TUNE_NO_CACHE = 0x1, 0x2, 0x4
+# collatz_set_variant modes: cases kernel, four-limb range kernel, 64-bit range
+# kernel, and the limb width (largest seed bit length run by the 64-bit kernel)
+MODE_CASES, MODE_RANGE, MODE_RANGE64, MODE_RANGE64_BITS = 0, 1, 2, 3
+RANGE64_BITS_DEFAULT = 48
 
 
 class TuneResultC(C.Structure):
     _fields_ = [("range_variant", C.c_int32), ("cases_variant", C.c_int32),
-                ("range_ms", C.c_float * 8), ("cases_ms", C.c_float * 8)]
+                ("range_ms", C.c_float * 8), ("cases_ms", C.c_float * 8),
+                ("range64_variant", C.c_int32), ("range64_bits", C.c_uint32),
+                ("range64_ms", C.c_float * 8), ("width_ms", C.c_float * 4)]
 
 
 class IntPeakC(C.Structure):
@@ -387,7 +393,9 @@ class Verifier:
         r = TuneResultC()
         self._check(lib().collatz_autotune(self._h, flags, C.byref(r)), "autotune")
         return {"range_variant": r.range_variant, "cases_variant": r.cases_variant,
-                "range_ms": [x for x in r.range_ms if x >= 0], "cases_ms": [x for x in r.cases_ms if x >= 0]}
+                "range_ms": [x for x in r.range_ms if x >= 0], "cases_ms": [x for x in r.cases_ms if x >= 0],
+                "range64_variant": r.range64_variant, "range64_bits": r.range64_bits,
+                "range64_ms": [x for x in r.range64_ms if x >= 0], "width_ms": list(r.width_ms)}
 
     def int_peak(self, mix: int = 1) -> dict:
         """Measured 32-bit integer peak of this device (collatz_int_peak): mix 0 is

@@ -283,6 +283,7 @@ extern "C" int collatz_create(const collatz_config* cfg, collatz_ctx** out) {
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);
   for (int i = 0; i < 4 && e == cudaSuccess; i++) e = cudaEventCreate(&c->ev[i]);
   if (e == cudaSuccess) e = range_init();
+  if (e == cudaSuccess) e = range64_init();
   if (e == cudaSuccess) e = build_case_tables(&c->ct, cfg->maxbits, c->own_stream);
   if (e != cudaSuccess) {
     rc = set_cuda_error(c, e, "collatz_create");
@@ -334,12 +335,25 @@ extern "C" int collatz_device_info(const collatz_ctx* c, int* sm_count, int* sm_
   return COLLATZ_OK;
 }
 
-extern "C" int collatz_variant_count(int mode) { return mode == 0 ? cases_variants() : range_variants(); }
+extern "C" int collatz_variant_count(int mode) {
+  switch (mode) {
+    case COLLATZ_MODE_CASES: return cases_variants();
+    case COLLATZ_MODE_RANGE: return range_variants();
+    case COLLATZ_MODE_RANGE64: return range64_variants();
+    case COLLATZ_MODE_RANGE64_BITS: return (int)range64_max_seed_bits() + 1;
+    default: return 0;
+  }
+}
 
 extern "C" int collatz_set_variant(collatz_ctx* c, int mode, int v) {
   if (!c || v < 0 || v >= collatz_variant_count(mode)) return COLLATZ_E_ARG;
   std::lock_guard<std::recursive_mutex> g(c->mu);
-  if (mode == 0) c->cases_variant = v; else c->range_variant = v;
+  switch (mode) {
+    case COLLATZ_MODE_CASES: c->cases_variant = v; break;
+    case COLLATZ_MODE_RANGE: c->range_variant = v; break;
+    case COLLATZ_MODE_RANGE64: c->range64_variant = v; break;
+    default: c->range64_bits = (uint32_t)v; break;
+  }
   return COLLATZ_OK;
 }
 
@@ -1126,18 +1140,29 @@ static RangeArgs range_args(collatz_ctx* c, const RangeTables& T, uint32_t k, bo
   return a;
 }
 
+cudaError_t cz::range_kernel_launch(collatz_ctx* c, const RangeArgs& a, bool stats, cudaStream_t s) {
+  int bps = 0;
+  if (!a.negative && a.seed_bits && a.seed_bits <= std::min(c->range64_bits, range64_max_seed_bits())) {
+    if (range64_occupancy(c->range64_variant, &bps) != cudaSuccess || bps <= 0) bps = 1;
+    const uint32_t grid = (uint32_t)(bps * c->sm_count);
+    return stats ? launch_range64_stats(a, c->range64_variant, grid, s)
+                 : launch_range64(a, c->range64_variant, grid, s);
+  }
+  const uint32_t grid = (uint32_t)grid_for(c, 1, c->range_variant);
+  return (stats && !a.negative) ? launch_range_stats(a, grid, s) : launch_range(a, c->range_variant, grid, s);
+}
+
 // One range launch on stream s: record and counter reset, k_range, the
 // 192- and 256-bit widening passes, the record copy-back.  Captured into a
 // graph by plans; issued directly by collatz_verify_batch.
 static cudaError_t range_enqueue(collatz_ctx* c, const RangeArgs& a, const RangeBufs& b, cudaStream_t s) {
   const size_t rb = sizeof(ReqRec) * std::max(1u, b.n);
-  const uint32_t grid = (uint32_t)grid_for(c, 1, c->range_variant);
   cudaError_t e = cudaMemsetAsync(b.recs, 0, rb, s);
   if (!e) e = cudaMemsetAsync(b.cursor, 0, sizeof(unsigned long long), s);
   if (!e) e = cudaMemsetAsync(b.wcount, 0, sizeof(uint32_t) * 2, s);
   if (!e && b.stats) e = cudaMemsetAsync(b.stats, 0, 16 * sizeof(unsigned long long), s);
   if (!e && b.first_seg) e = launch_range_scout(a, b.first_seg, b.n, s);
-  if (!e) e = (b.stats && !a.negative) ? launch_range_stats(a, grid, s) : launch_range(a, c->range_variant, grid, s);
+  if (!e) e = range_kernel_launch(c, a, b.stats != nullptr, s);
   if (!e)
     e = launch_range_wide(b.widen, b.wcount, WIDEN_CAP, 6, b.recs, b.widen2, WIDEN_CAP, b.wcount + 1, c->iter_cap, s,
                           a.negative != 0);

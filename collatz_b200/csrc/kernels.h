@@ -132,6 +132,21 @@ cudaError_t range_init();  // once per device, before the first launch
 cudaError_t launch_range_stats(const RangeArgs& a, uint32_t grid, cudaStream_t st);
 cudaError_t launch_range(const RangeArgs& a, int variant, uint32_t grid, cudaStream_t st);
 cudaError_t range_occupancy(int variant, int* blocks_per_sm);
+// The 64-bit range kernel (range64.cu): the same seeds and results as
+// launch_range for launches of the positive variant whose seeds all lie
+// below 2^range64_max_seed_bits(); one 64-bit value per seed, four limbs per
+// lane only while a lane's value is at or above 2^59.  Variants differ in
+// run pairs per pass, resident blocks per SM and the in-loop table steps J
+// (0: none; 8, 10, 11).
+int range64_variants();
+uint32_t range64_max_seed_bits();
+cudaError_t range64_init();  // once per device, before the first launch
+cudaError_t launch_range64(const RangeArgs& a, int variant, uint32_t grid, cudaStream_t st);
+// Diagnostics form: run pairs, slow paths, replays, jumps, pops, expansions,
+// passes, offers into a.stats[0..7], table steps [13], windows [14], 64-bit
+// pairs [15]; clock64 cycles of offers, refill and lanes into [8..10].
+cudaError_t launch_range64_stats(const RangeArgs& a, int variant, uint32_t grid, cudaStream_t st);
+cudaError_t range64_occupancy(int variant, int* blocks_per_sm);
 // Threshold scouts: first_seg[i] is the index of request i's first segment
 // (>= a.nsegs: none).  Raises each request's prefilter keys to the maxima of
 // the seeds of its first work item, before the range kernel runs.

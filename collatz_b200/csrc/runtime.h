@@ -113,6 +113,10 @@ struct collatz_ctx {
   cz::CaseTables ct;
   std::map<uint32_t, cz::RangeTables> rt;
   int cases_variant = 4, range_variant = 4;
+  // 64-bit range kernel: its variant, and the limb-width cutoff -- launches whose seeds
+  // all have at most range64_bits bits run it, the others run the four-limb kernel
+  int range64_variant = 0;
+  uint32_t range64_bits = 48;
   uint32_t iter_cap = 1u << 16;
   // scratch for the synchronous calls
   cz::DevBuf d_rec, d_counter, d_overflow, d_ovcount, d_pairs[2], d_segs, d_widen, d_widen2, d_wcount;
@@ -146,6 +150,11 @@ inline uint32_t range_seed_bits(const collatz_range& r) {
   return b;
 }
 int get_range_tables(collatz_ctx* c, uint32_t k, RangeTables** out, bool negative = false);
+// Launches the range kernel for a on stream s: the 64-bit kernel when every
+// seed of the launch has at most c->range64_bits bits (positive variant),
+// else the four-limb kernel; grid = resident blocks per SM x SMs.  stats:
+// the diagnostics form of the chosen kernel.
+cudaError_t range_kernel_launch(collatz_ctx* c, const RangeArgs& a, bool stats, cudaStream_t s);
 int lower_range(collatz_ctx* c, const collatz_range& r, uint32_t req, const RangeTables& T,
                 std::vector<RangeSeg>& segs, unsigned long long& items);
 void rec_to_range_result(const ReqRec& r, collatz_range_result* out);

@@ -377,7 +377,7 @@ int launch_slice(collatz_server* s, int si) {
   if (!e && fb)
     e = launch_range_scout(a, reinterpret_cast<const uint32_t*>(static_cast<const char*>(S.d_segs.p) + sb),
                            (uint32_t)scouts.size(), st);
-  if (!e) e = launch_range(a, c->range_variant, s->grid, st);
+  if (!e) e = range_kernel_launch(c, a, false, st);
   if (!e)
     e = launch_range_wide(S.d_widen[0].as<WidenEntry>(), S.d_wcount.as<uint32_t>(), WIDEN_CAP, 6, a.recs,
                           S.d_widen[1].as<WidenEntry>(), WIDEN_CAP, S.d_wcount.as<uint32_t>() + 1, c->iter_cap, st,

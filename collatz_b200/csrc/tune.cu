@@ -39,7 +39,7 @@ std::string device_key(const collatz_ctx* c) {
     if (ch == ' ' || ch == '\t') ch = '_';
   std::ostringstream k;
   k << name << ":sm" << p.multiProcessorCount << ":cc" << p.major << "." << p.minor << ":abi"
-    << COLLATZ_ABI_VERSION << ":v" << range_variants() << "." << cases_variants();
+    << COLLATZ_ABI_VERSION << ":v" << range_variants() << "." << cases_variants() << "." << range64_variants();
   return k.str();
 }
 
@@ -177,6 +177,11 @@ void tune_on_create(collatz_ctx* c) {
   if (cache_lookup(path, "range", key, c->cfg.range_k, range_variants(), &v)) {
     c->range_variant = v;
     have_r = true;
+    if (cache_lookup(path, "range64", key, c->cfg.range_k, range64_variants(), &v)) c->range64_variant = v;
+    else have_r = false;
+    if (cache_lookup(path, "range64bits", key, c->cfg.range_k, (int)range64_max_seed_bits() + 1, &v))
+      c->range64_bits = (uint32_t)v;
+    else have_r = false;
   }
   if (cache_lookup(path, "cases", key, c->cfg.maxbits, cases_variants(), &v)) {
     c->cases_variant = v;
@@ -198,9 +203,12 @@ extern "C" int collatz_autotune(collatz_ctx* c, uint32_t flags, collatz_tune_res
   if (dev_scope.err != cudaSuccess) return set_cuda_error(c, dev_scope.err, "collatz_autotune");
   collatz_tune_result res;
   std::memset(&res, 0, sizeof res);
-  for (int i = 0; i < 8; i++) res.range_ms[i] = res.cases_ms[i] = -1.0f;
+  for (int i = 0; i < 8; i++) res.range_ms[i] = res.cases_ms[i] = res.range64_ms[i] = -1.0f;
+  for (int i = 0; i < 4; i++) res.width_ms[i] = -1.0f;
   res.range_variant = c->range_variant;
   res.cases_variant = c->cases_variant;
+  res.range64_variant = c->range64_variant;
+  res.range64_bits = c->range64_bits;
   const std::string key = device_key(c), path = (flags & COLLATZ_TUNE_NO_CACHE) ? "" : cache_path();
   int rc = COLLATZ_OK;
   if (flags & COLLATZ_TUNE_RANGE) {
@@ -209,18 +217,49 @@ extern "C" int collatz_autotune(collatz_ctx* c, uint32_t flags, collatz_tune_res
     r.offset[0] = 1ull << 40;
     r.size = 1ull << 34;
     r.k = c->cfg.range_k;
-    const int keep = c->range_variant, nv = std::min(range_variants(), 8);
+    const int keep = c->range_variant, keep64 = c->range64_variant;
+    const uint32_t keep_bits = c->range64_bits;
+    const int nv = std::min(range_variants(), 8), nv64 = std::min(range64_variants(), 8);
+    c->range64_bits = 0;  // the four-limb kernel's variants
     for (int v = 0; v < nv && !rc; v++) {
       c->range_variant = v;
       rc = time_range(c, r, &res.range_ms[v]);
     }
+    const int best = rc ? keep : (int)(std::min_element(res.range_ms, res.range_ms + nv) - res.range_ms);
+    c->range_variant = best;
+    c->range64_bits = range64_max_seed_bits();  // the 64-bit kernel's variants
+    for (int v = 0; v < nv64 && !rc; v++) {
+      c->range64_variant = v;
+      rc = time_range(c, r, &res.range64_ms[v]);
+    }
+    const int best64 =
+        rc ? keep64 : (int)(std::min_element(res.range64_ms, res.range64_ms + nv64) - res.range64_ms);
+    c->range64_variant = best64;
+    // limb width: both kernels on seeds of 44 and of 48 bits
+    uint32_t bits = 0;
+    const uint32_t at_bits[2] = {44, range64_max_seed_bits()};
+    for (int i = 0; i < 2 && !rc; i++) {
+      collatz_range w = r;
+      w.size = 1ull << 32;
+      w.offset[0] = (1ull << at_bits[i]) - w.size;  // seeds of exactly at_bits[i] bits
+      c->range64_bits = 0;
+      rc = time_range(c, w, &res.width_ms[2 * i]);
+      c->range64_bits = range64_max_seed_bits();
+      if (!rc) rc = time_range(c, w, &res.width_ms[2 * i + 1]);
+      if (!rc && res.width_ms[2 * i + 1] < res.width_ms[2 * i]) bits = at_bits[i];
+    }
     if (!rc) {
-      const int best = (int)(std::min_element(res.range_ms, res.range_ms + nv) - res.range_ms);
-      c->range_variant = best;
+      c->range64_bits = bits;
       res.range_variant = best;
+      res.range64_variant = best64;
+      res.range64_bits = bits;
       cache_store(path, "range", key, c->cfg.range_k, best, res.range_ms, nv);
+      cache_store(path, "range64", key, c->cfg.range_k, best64, res.range64_ms, nv64);
+      cache_store(path, "range64bits", key, c->cfg.range_k, (int)bits, res.width_ms, 4);
     } else {
       c->range_variant = keep;
+      c->range64_variant = keep64;
+      c->range64_bits = keep_bits;
     }
   }
   if (!rc && (flags & COLLATZ_TUNE_CASES)) {

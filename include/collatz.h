@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define COLLATZ_ABI_VERSION 1
+#define COLLATZ_ABI_VERSION 2
 
 enum collatz_status_code {
   COLLATZ_OK = 0,
@@ -358,23 +358,46 @@ int collatz_server_info(collatz_server *s, collatz_server_info_t *info);
  * COLLATZ_E_STATE, joins the scheduler and frees the server. */
 int collatz_server_stop(collatz_server *s);
 
-/* Kernel variants (block shapes) for the autotuner. */
-int collatz_variant_count(int mode); /* mode 0 cases, 1 range */
+/* Kernel choices for the autotuner (no counterpart in the reference).
+ *   COLLATZ_MODE_CASES, COLLATZ_MODE_RANGE: variant (block shape, body) of
+ *     the cases kernel and of the four-limb range kernel;
+ *   COLLATZ_MODE_RANGE64: variant of the 64-bit range kernel (run pairs per
+ *     pass, blocks per SM, in-loop table steps J of 0, 8, 10 or 11);
+ *   COLLATZ_MODE_RANGE64_BITS: the limb width -- launches whose seeds all have
+ *     at most this many bits (0..52) run the 64-bit kernel, the others the
+ *     four-limb kernel (0: always four limbs).
+ * collatz_variant_count gives the number of choices (0..count-1). */
+#define COLLATZ_MODE_CASES 0
+#define COLLATZ_MODE_RANGE 1
+#define COLLATZ_MODE_RANGE64 2
+#define COLLATZ_MODE_RANGE64_BITS 3
+int collatz_variant_count(int mode);
 int collatz_set_variant(collatz_ctx *ctx, int mode, int variant);
 
 /* Autotuner (no counterpart in the reference).  Times every variant of the
- * selected modes on a fixed sample on this device -- range: 2^34 seeds at
- * 2^40 with the context's k; cases: about 2^20 Step-1 pairs of the root case
- * "3 2 2 9 1 0" for the context's N -- keeps the fastest for the context and
- * records it in a text cache (COLLATZ_TUNE_CACHE, else
+ * selected modes on a fixed sample on this device and keeps the fastest:
+ *   range: the four-limb kernel's variants and the 64-bit kernel's variants
+ *     (window length j of the jump table, windows and run pairs per seed at
+ *     expansion, in-loop table steps) on 2^34 seeds at 2^40 with the
+ *     context's k, then the limb width: the two best variants timed on the
+ *     2^32 largest seeds of 44 bits and of 48 bits; range64_bits is the
+ *     largest of 48, 44 at which the 64-bit kernel is faster, else 0 (four
+ *     limbs throughout);
+ *   cases: about 2^20 Step-1 pairs of the root case "3 2 2 9 1 0" for the
+ *     context's N.
+ * The choices go into a text cache (COLLATZ_TUNE_CACHE, else
  * $XDG_CACHE_HOME/collatz_b200/tune.txt or ~/.cache/collatz_b200/tune.txt),
  * keyed by device, variant set and k or N.  A context created with
  * COLLATZ_VARIANT_AUTO applies cached choices; with COLLATZ_AUTOTUNE=1 in the
- * environment it also tunes what the cache lacks.  Variants never change
- * results, only speed. */
+ * environment it also tunes what the cache lacks.  Variants and the limb
+ * width never change results, only speed. */
 typedef struct {
   int32_t range_variant, cases_variant; /* chosen (or kept when not tuned) */
   float range_ms[8], cases_ms[8];       /* device ms per variant on the sample; -1 = not timed */
+  int32_t range64_variant;              /* 64-bit range kernel: chosen variant */
+  uint32_t range64_bits;                /* chosen limb width (COLLATZ_MODE_RANGE64_BITS) */
+  float range64_ms[8];                  /* device ms per 64-bit variant on the sample; -1 = not timed */
+  float width_ms[4];                    /* 44-bit seeds: four limbs, 64 bits; 48-bit seeds: four limbs, 64 bits */
 } collatz_tune_result;
 #define COLLATZ_TUNE_RANGE 0x1u
 #define COLLATZ_TUNE_CASES 0x2u

@@ -64,6 +64,7 @@ def test_range_variants_match_oracle(verifier, variant):
     assert cb.lib().collatz_variant_count(1) == 8
     v = verifier(26)
     v.set_variant(1, variant)
+    v.set_variant(cb.MODE_RANGE64_BITS, 0)  # every launch on the four-limb kernel
     try:
         for off, size, k, mod9 in VARIANT_CASES:
             g = v.verify_range(off, size, k, mod9)
@@ -75,7 +76,68 @@ def test_range_variants_match_oracle(verifier, variant):
             o = O.range_verify(*q, method=1, nthreads=NT)
             _cmp(m, o)
     finally:
-        v.set_variant(1, 4)  # the default
+        v.set_variant(1, 4)  # the defaults
+        v.set_variant(cb.MODE_RANGE64_BITS, cb.RANGE64_BITS_DEFAULT)
+
+
+VARIANT64_CASES = [CASES[i] for i in (0, 1, 3, 4, 5, 6)] + [
+    ((1 << 46) + 999, 1 << 21, 24, True),       # values cross 2^59 lane by lane
+    ((1 << 48) - (3 << 24), 1 << 21, 24, True),  # at the kernel's seed limit
+    ((1 << 44) + 5, 1 << 21, 34, True),         # k = 34 (q < 2^14)
+    (3, 1 << 18, 16, False),                    # below 2^k, no mod-9 sieve: every n, even ones too
+]
+
+
+@pytest.mark.parametrize("variant", range(8))
+def test_range64_variants_match_oracle(verifier, variant):
+    """Every variant of the 64-bit range kernel (run pairs per pass, blocks per
+    SM, in-loop table steps J, expansion windows of 8, 10 or 11 steps and run
+    pairs at expansion) gives the oracle's results, for single ranges and a
+    batch, with the limb width at its maximum (48 bits)."""
+    import collatz_b200 as cb
+    from oracle import oracle as O
+    assert cb.lib().collatz_variant_count(cb.MODE_RANGE64) == 8
+    v = verifier(26)
+    v.set_variant(cb.MODE_RANGE64, variant)
+    v.set_variant(cb.MODE_RANGE64_BITS, 48)
+    try:
+        for off, size, k, mod9 in VARIANT64_CASES:
+            g = v.verify_range(off, size, k, mod9)
+            o = O.range_verify(off, size, k, mod9, method=1, nthreads=NT)
+            _cmp(g, o)
+        reqs = [((1 << 40) + i * (1 << 24) + 9 * i, (1 << 18) + 1000 * i, 24, True) for i in range(6)]
+        reqs.append((17, 40000, 24, True))
+        for q, m in zip(reqs, v.verify_batch(reqs)):
+            o = O.range_verify(*q, method=1, nthreads=NT)
+            _cmp(m, o)
+    finally:
+        v.set_variant(cb.MODE_RANGE64, 0)
+        v.set_variant(cb.MODE_RANGE64_BITS, cb.RANGE64_BITS_DEFAULT)
+
+
+@pytest.mark.parametrize("off,size,k", [((1 << 40) + 777, 1 << 34, 24), ((1 << 46) + 12345, 1 << 32, 24),
+                                        ((1 << 47) + (7 << 24), 1 << 31, 24), ((1 << 44) + (3 << 34), 1 << 34, 34)])
+def test_range64_equals_four_limbs(verifier, off, size, k):
+    """On large ranges the 64-bit kernel (every variant) and the four-limb
+    kernel give the same seeds, maxima with their seeds, failures and widened
+    seeds."""
+    import collatz_b200 as cb
+    v = verifier(26, range_k=k)
+    try:
+        v.set_variant(cb.MODE_RANGE64_BITS, 0)
+        p = v.verify_range(off, size, k)
+        v.set_variant(cb.MODE_RANGE64_BITS, 48)
+        for var in range(cb.lib().collatz_variant_count(cb.MODE_RANGE64)):
+            v.set_variant(cb.MODE_RANGE64, var)
+            w = v.verify_range(off, size, k)
+            assert (w.seeds_checked, w.failures, w.widened, w.errors) == \
+                (p.seeds_checked, p.failures, p.widened, p.errors), var
+            assert (w.max_stopping_time, w.max_stopping_time_seed) == \
+                (p.max_stopping_time, p.max_stopping_time_seed), var
+            assert (w.max_excursion, w.max_excursion_seed) == (p.max_excursion, p.max_excursion_seed), var
+    finally:
+        v.set_variant(cb.MODE_RANGE64, 0)
+        v.set_variant(cb.MODE_RANGE64_BITS, cb.RANGE64_BITS_DEFAULT)
 
 
 def test_batch_of_tiny_requests(verifier):
@@ -195,13 +257,16 @@ def test_window_variant_equals_plain(verifier, off, size, k):
     unchanged on large ranges, where most seeds take it: seeds, maxima with
     their seeds, failures and widened seeds equal the plain variant's."""
     v = verifier(26, range_k=k)
+    import collatz_b200 as cb
+    v.set_variant(cb.MODE_RANGE64_BITS, 0)  # the four-limb kernel
     try:
         v.set_variant(1, 4)
         w = v.verify_range(off, size, k)
         v.set_variant(1, 2)
         p = v.verify_range(off, size, k)
     finally:
-        v.set_variant(1, 4)  # the default
+        v.set_variant(1, 4)  # the defaults
+        v.set_variant(cb.MODE_RANGE64_BITS, cb.RANGE64_BITS_DEFAULT)
     assert (w.seeds_checked, w.failures, w.widened, w.errors) == (p.seeds_checked, p.failures, p.widened, p.errors)
     assert (w.max_stopping_time, w.max_stopping_time_seed) == (p.max_stopping_time, p.max_stopping_time_seed)
     assert (w.max_excursion, w.max_excursion_seed) == (p.max_excursion, p.max_excursion_seed)
@@ -215,13 +280,16 @@ def test_narrow_variant_equals_plain(verifier, off, size, k):
     2^56-2^58 warps switch between the bodies, at 2^63 the seeds start above
     its limit."""
     v = verifier(26, range_k=k)
+    import collatz_b200 as cb
+    v.set_variant(cb.MODE_RANGE64_BITS, 0)  # the four-limb kernel
     try:
         v.set_variant(1, 6)
         w = v.verify_range(off, size, k)
         v.set_variant(1, 2)
         p = v.verify_range(off, size, k)
     finally:
-        v.set_variant(1, 4)  # the default
+        v.set_variant(1, 4)  # the defaults
+        v.set_variant(cb.MODE_RANGE64_BITS, cb.RANGE64_BITS_DEFAULT)
     assert (w.seeds_checked, w.failures, w.widened, w.errors) == (p.seeds_checked, p.failures, p.widened, p.errors)
     assert (w.max_stopping_time, w.max_stopping_time_seed) == (p.max_stopping_time, p.max_stopping_time_seed)
     assert (w.max_excursion, w.max_excursion_seed) == (p.max_excursion, p.max_excursion_seed)

@@ -15,11 +15,18 @@ def test_every_variant_same_results(verifier):
     import collatz_b200 as cb
     v = verifier(36)
     ref_range = None
+    v.set_variant(cb.MODE_RANGE64_BITS, 0)  # the four-limb kernel's variants first
     for var in range(cb.lib().collatz_variant_count(1)):
         v.set_variant(1, var)
         r = _key(v.verify_range((1 << 44) + 12345, 3 << 21, 24))
         assert ref_range is None or r == ref_range, var
         ref_range = r
+    v.set_variant(cb.MODE_RANGE64_BITS, 48)  # then the 64-bit kernel's
+    for var in range(cb.lib().collatz_variant_count(cb.MODE_RANGE64)):
+        v.set_variant(cb.MODE_RANGE64, var)
+        assert _key(v.verify_range((1 << 44) + 12345, 3 << 21, 24)) == ref_range, var
+    v.set_variant(cb.MODE_RANGE64, 0)
+    v.set_variant(cb.MODE_RANGE64_BITS, cb.RANGE64_BITS_DEFAULT)
     ref_case = None
     for var in range(cb.lib().collatz_variant_count(0)):
         v.set_variant(0, var)
@@ -42,6 +49,9 @@ def test_autotune_records_and_reuses(tmp_path, monkeypatch):
     assert len(t["range_ms"]) == nr and len(t["cases_ms"]) == nc
     assert t["range_ms"][t["range_variant"]] == min(t["range_ms"])
     assert t["cases_ms"][t["cases_variant"]] == min(t["cases_ms"])
+    n64 = cb.lib().collatz_variant_count(cb.MODE_RANGE64)
+    assert len(t["range64_ms"]) == n64 and t["range64_ms"][t["range64_variant"]] == min(t["range64_ms"])
+    assert t["range64_bits"] in (0, 44, 48) and all(x > 0 for x in t["width_ms"])
     lines = cache.read_text().splitlines()
     assert any(ln.startswith("range ") and f" 20 {t['range_variant']} " in ln for ln in lines)
     assert any(ln.startswith("cases ") and f" 36 {t['cases_variant']} " in ln for ln in lines)
@@ -49,3 +59,4 @@ def test_autotune_records_and_reuses(tmp_path, monkeypatch):
     with cb.Verifier(36, range_k=20) as v2:
         t2 = v2.autotune(range_mode=False, cases_mode=False)
         assert (t2["range_variant"], t2["cases_variant"]) == (t["range_variant"], t["cases_variant"])
+        assert (t2["range64_variant"], t2["range64_bits"]) == (t["range64_variant"], t["range64_bits"])
