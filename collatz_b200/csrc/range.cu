@@ -66,7 +66,42 @@ struct ExpandStats {
 // request and thresholds from their item's slot when they are popped, so a
 // slot is reused only after the last seed of its previous item has left the
 // queue; the queue is then not empty).  Warp-uniform.
-template <bool STATS, bool NEG, bool WIN, class WT>
+// Up to M run pairs of a seed at expansion on four limbs, with every lane
+// busy.  A pair is kept only in the common case: the value stays below 2^114
+// before the odd run (so it stays below 2^119 after it), the value after the
+// odd run is below the excursion gate window, and the seed either does not
+// descend or descends with a stopping time below thr_st.  Otherwise the pair
+// is left to the run loop.  Returns false when the seed finished here.
+template <int M>
+__device__ __forceinline__ bool first_pairs4(u32& V0, u32& V1, u32& V2, u32& V3, u32& s0, u32 n0, u32 n1, u32 n2,
+                                             u64 gate_w, u32 thr_st) {
+#pragma unroll
+  for (int m = 0; m < M; m++) {
+    if (V3 >= (1u << 18)) break;
+    u32 y0 = V0, y1 = V1, y2 = V2, y3 = V3;
+    const u32 a = ctz32(y0 | 0x80u);
+    odd_run4(y0, y1, y2, y3, a, pow3_le7(a));
+    if (!lt96c(y1, y2, y3, (u32)gate_w, (u32)(gate_w >> 32), 0u)) break;  // candidate: the loop takes it
+    y0 -= 1;  // y0 == 0 gives b == 0 below, and the borrow cancels against the +1
+    const u32 b = ctz32(y0 | 0x80000000u);
+    const u32 w0 = __funnelshift_r(y0, y1, b), w1 = __funnelshift_r(y1, y2, b);
+    const u32 w2 = __funnelshift_r(y2, y3, b), w3 = y3 >> b;
+    const u32 st2 = s0 + a + b;
+    if ((w3 == 0) & (b != 0) & lt96c(w0, w1, w2, n0, n1, n2)) {
+      if (st2 >= thr_st) break;  // sigma may reach the maximum: the loop takes it
+      return false;
+    }
+    V0 = w0 + 1;
+    V1 = w1;
+    V2 = w2;
+    V3 = w3;
+    add_carry3(V1, V2, V3, (V0 == 0) & (b != 0));
+    s0 = st2;
+  }
+  return true;
+}
+
+template <bool STATS, bool NEG, bool WIN, int M, class WT>
 __device__ __forceinline__ bool expand_one(WT& W, const RangeArgs& A, const uint4* __restrict__ T, u32 lane, u32 k,
                                            u32 k9, const unsigned long long* s_p3, const u32* s_win, u32 head,
                                            u32& tail, bool& exhausted, u32& w_thr_st, u32& w_req, u64& w_gate,
@@ -135,7 +170,7 @@ __device__ __forceinline__ bool expand_one(WT& W, const RangeArgs& A, const uint
   const u32 w_thr_bl = W.thr_bl;
   const u64 gate_w = w_gate;
   const u32 slot = W.ring_seq & (RR - 1);
-  u32 mask = 0, total;
+  u32 mask = 0, total, seeds;
   u32 pos;
   if (it.kind == 0) {
     const u32 q0 = (u32)it.q_lo, q1 = (u32)(it.q_lo >> 32), q2 = it.q_hi;
@@ -161,13 +196,17 @@ __device__ __forceinline__ bool expand_one(WT& W, const RangeArgs& A, const uint
       for (u32 j = 0; j < RANGE_ITEM / 32; j++)
         if (it.sbase + j * 32 + lane < it.send) mask |= 1u << j;
     }
-    pos = tail + warp_excl_scan(__popc(mask), &total);
+    // each entry in turn: its seed's start state, then one ballot places the lanes' seeds
+    seeds = __reduce_add_sync(FULL, __popc(mask));
+    total = 0;
 #pragma unroll
     for (u32 j = 0; j < RANGE_ITEM / 32; j++) {
+      bool keep = false;
+      u32 V0 = 0, V1 = 0, V2 = 0, V3 = 0, s0 = 0, m0 = 0, m1 = 0;
       if ((mask >> j) & 1u) {
         const u32 f = (e[j].y >> 8) & 0xFFu, emax = e[j].y >> 24;
-        const u32 m0 = qk0 | e[j].x, m1 = qk1 | (e[j].y & 0xFFu);
-        u32 V0, V1, V2, V3, s0;
+        m0 = qk0 | e[j].x;
+        m1 = qk1 | (e[j].y & 0xFFu);
         // T^0..T^k(n) < 2^emax (n + 1 + k) <= 2^(bitlen(n) + 1 + emax): skip them when that is
         // below the excursion threshold, else replay the first k steps exactly
         if (jump_ok_base && nbl + 1 + emax < w_thr_bl) {
@@ -231,13 +270,20 @@ __device__ __forceinline__ bool expand_one(WT& W, const RangeArgs& A, const uint
           s0 = 0;
           if (STATS) X.c_replay++;
         }
+        keep = true;
+        if (M > 0 && !NEG) keep = first_pairs4<M>(V0, V1, V2, V3, s0, m0, m1, qk2, gate_w, w_thr_st);
+      }
+      const u32 bk = __ballot_sync(FULL, keep);
+      if (keep) {
         // excursion candidate T^s(n) = v - 1 <= v: bits 32..95 of v against the threshold
         // T': the candidate is u + 1, whose window exceeds u's by at most 1
-        const u32 cand = ((V3 != 0) | ((((u64)V2 << 32) | V1) >= (NEG ? gate_w - (gate_w != 0) : gate_w))) ? 1u : 0u;
-        W.qa[pos & (RQ - 1)] = make_uint4(V0, V1, V2, V3);
-        W.qb[pos & (RQ - 1)] = make_uint4(m0, m1, qk2, s0 | meta_item | (cand << 13));
-        pos++;
+        const u32 cand =
+            ((V3 != 0) | ((((u64)V2 << 32) | V1) >= (NEG ? gate_w - (gate_w != 0) : gate_w))) ? 1u : 0u;
+        const u32 at = (tail + total + __popc(bk & lanemask_lt())) & (RQ - 1);
+        W.qa[at] = make_uint4(V0, V1, V2, V3);
+        W.qb[at] = make_uint4(m0, m1, qk2, s0 | meta_item | (cand << 13));
       }
+      total += __popc(bk);
     }
   } else {
     // integers below 2^k: [d, d + 64) of [q_lo, d_hi), no residue sieve
@@ -250,6 +296,7 @@ __device__ __forceinline__ bool expand_one(WT& W, const RangeArgs& A, const uint
       if (n < it.d_hi && n >= 2 && (!it.mod9 || keep9)) mask |= 1u << j;
     }
     pos = tail + warp_excl_scan(__popc(mask), &total);
+    seeds = total;
 #pragma unroll
     for (u32 j = 0; j < 2; j++) {
       if ((mask >> j) & 1u) {
@@ -268,7 +315,7 @@ __device__ __forceinline__ bool expand_one(WT& W, const RangeArgs& A, const uint
     W.ring[slot] = make_uint4(rq, w_thr_st, (u32)w_gate, (u32)(w_gate >> 32));
     W.ring_end[slot] = tail + total;
     W.ring_seq++;
-    W.acc_seeds += total;
+    W.acc_seeds += seeds;
     W.acc_items++;
   }
   if (STATS) X.c_exp++;
@@ -309,7 +356,7 @@ __device__ __noinline__ u32 drop_dominated(RangeWarp& W, u32 lane, u32 pend, u32
   return pend;
 }
 
-template <int R, int MINB, bool STATS = false, bool NEG = false, bool WIN = false, bool N64 = false>
+template <int R, int MINB, bool STATS = false, bool NEG = false, bool WIN = false, bool N64 = false, int M = 0>
 __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) {
   // diagnostics (STATS variant only): run pairs, excursion slow paths, replays, jumps, pops,
   // expansions, passes, offers; clock64 cycles per phase (lane 0)
@@ -493,7 +540,7 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
     }
     // ---- refill: keep 32 R seeds queued (each lane pops at most R per pass) ----
     while (tail - head < 32u * R && !exhausted) {
-      if (!expand_one<STATS, NEG, WIN>(W, A, T, lane, k, k9, s_p3, s_win, head, tail, exhausted, w_thr_st, w_req,
+      if (!expand_one<STATS, NEG, WIN, M>(W, A, T, lane, k, k9, s_p3, s_win, head, tail, exhausted, w_thr_st, w_req,
                                        w_gate, X))
         break;
     }
@@ -860,26 +907,26 @@ int range_variants() { return 8; }
 constexpr size_t RANGE_SMEM = sizeof(RangeWarp) * RWARPS;
 
 cudaError_t launch_range_stats(const RangeArgs& a, u32 grid, cudaStream_t st) {
-  k_range<2, 3, true, false, true, true><<<grid, RWARPS * 32, RANGE_SMEM, st>>>(a);
+  k_range<2, 3, true, false, true, false, 3><<<grid, RWARPS * 32, RANGE_SMEM, st>>>(a);
   return cudaGetLastError();
 }
 
 // (run pairs per pass, minimum resident blocks per SM, 8-step window after the k-step jump,
-// 64-bit body while the warp's values are below 2^59)
+// 64-bit body while the warp's values are below 2^59, run pairs per seed taken at expansion)
+// Measured on B200, 2^36 seeds at 2^60 + 3 2^34 with k = 34: 8.20 ms (variant 0), 8.49 (1),
+// 10.15 (2), 8.82 (3), 9.63 (4: the window alone), 8.9-9.2 (5, 6), 8.30 (7).
 #define CZ_RANGE_VARIANTS(X)                                                                   \
-  X(0, 1, 3, 0, 0) X(1, 2, 3, 0, 0) X(2, 2, 4, 0, 0) X(3, 1, 4, 0, 0) X(4, 2, 4, 1, 0) X(5, 2, 3, 1, 0) \
-  X(6, 2, 4, 1, 1) X(7, 2, 3, 1, 1)
+  X(0, 2, 4, 1, 0, 3) X(1, 2, 4, 1, 0, 4) X(2, 2, 4, 0, 0, 0) X(3, 2, 4, 1, 0, 5) X(4, 2, 4, 1, 0, 0) \
+  X(5, 2, 3, 1, 0, 3) X(6, 2, 4, 1, 1, 3) X(7, 1, 4, 1, 0, 3)
 
 cudaError_t launch_range(const RangeArgs& a, int variant, u32 grid, cudaStream_t st) {
-  if (!a.negative && a.seed_bits && a.seed_bits <= RANGE_NARROW_MAX_BITS && (variant == 4 || variant == 5))
-    variant += 2;  // the same shape with the 64-bit body
   switch (variant) {
-#define X(id, rm, mb, win, n64)                                                          \
-  case id:                                                                               \
-    if (a.negative)                                                                      \
-      k_range<rm, mb, false, true><<<grid, RWARPS * 32, RANGE_SMEM, st>>>(a);            \
-    else                                                                                 \
-      k_range<rm, mb, false, false, win, n64><<<grid, RWARPS * 32, RANGE_SMEM, st>>>(a); \
+#define X(id, rm, mb, win, n64, m)                                                              \
+  case id:                                                                                      \
+    if (a.negative)                                                                             \
+      k_range<rm, mb, false, true><<<grid, RWARPS * 32, RANGE_SMEM, st>>>(a);                   \
+    else                                                                                        \
+      k_range<rm, mb, false, false, win, n64, m><<<grid, RWARPS * 32, RANGE_SMEM, st>>>(a);    \
     break;
     CZ_RANGE_VARIANTS(X)
 #undef X
@@ -890,10 +937,10 @@ cudaError_t launch_range(const RangeArgs& a, int variant, u32 grid, cudaStream_t
 
 cudaError_t range_occupancy(int variant, int* bps) {
   switch (variant) {
-#define X(id, rm, mb, win, n64) \
-  case id:                      \
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_range<rm, mb, false, false, win, n64>, RWARPS * 32, \
-                                                         RANGE_SMEM);
+#define X(id, rm, mb, win, n64, m)                                                                                 \
+  case id:                                                                                                         \
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_range<rm, mb, false, false, win, n64, m>,         \
+                                                         RWARPS * 32, RANGE_SMEM);
     CZ_RANGE_VARIANTS(X)
 #undef X
     default: return cudaErrorInvalidValue;
@@ -903,9 +950,9 @@ cudaError_t range_occupancy(int variant, int* bps) {
 // Opts every range kernel into RANGE_SMEM (> 48 KB) of dynamic shared memory.
 cudaError_t range_init() {
   cudaError_t e = cudaSuccess;
-#define X(id, rm, mb, win, n64)                                                                                 \
+#define X(id, rm, mb, win, n64, m)                                                                              \
   if (e == cudaSuccess)                                                                                         \
-    e = cudaFuncSetAttribute(k_range<rm, mb, false, false, win, n64>,                                          \
+    e = cudaFuncSetAttribute(k_range<rm, mb, false, false, win, n64, m>,                                       \
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RANGE_SMEM);                    \
   if (e == cudaSuccess)                                                                                        \
     e = cudaFuncSetAttribute(k_range<rm, mb, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,         \
@@ -913,7 +960,7 @@ cudaError_t range_init() {
   CZ_RANGE_VARIANTS(X)
 #undef X
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_range<2, 3, true, false, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_range<2, 3, true, false, true, false, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)RANGE_SMEM);
   return e;
 }

@@ -108,17 +108,6 @@ __device__ __noinline__ u32 drop_dominated64(Warp64& W, u32 lane, u32 pend, u32 
   return pend;
 }
 
-// Queue position of this lane's first entry among the warp's entries, each
-// lane holding at most two (bits 0 and 1 of m), in lane order; *total gets
-// the warp's count.  Two ballots instead of a shuffle scan.
-__device__ __forceinline__ u32 queue_rank2(u32 m, u32 lane, u32* total) {
-  static_assert(RANGE_ITEM / 32 == 2, "two entries per lane");
-  const u32 b0 = __ballot_sync(FULL, m & 1u), b1 = __ballot_sync(FULL, m & 2u);
-  const u32 lt = (1u << lane) - 1u;
-  *total = __popc(b0) + __popc(b1);
-  return __popc(b0 & lt) + __popc(b1 & lt);
-}
-
 struct Stats64 {
   u32 pairs = 0, fast = 0, slow_e = 0, replay = 0, jump = 0, pop = 0, exp = 0, pass = 0, offer = 0, win = 0,
       tab = 0, xpairs = 0, xfin = 0;
@@ -232,7 +221,7 @@ __device__ __forceinline__ bool expand64(Warp64& W, const RangeArgs& A, const ui
   const u32 w_thr_bl = W.thr_bl;
   const u64 G = gate64_of(w_gate);
   const u32 slot = W.ring_seq & (RR - 1);
-  u32 mask = 0, total, pos, seeds;
+  u32 mask = 0, total, seeds;
   if (it.kind == 0) {
     const u64 q = it.q_lo;  // < 2^(52 - k)
     const u64 qk = q << k;
@@ -252,10 +241,10 @@ __device__ __forceinline__ bool expand64(Warp64& W, const RangeArgs& A, const ui
       for (u32 j = 0; j < RANGE_ITEM / 32; j++)
         if (it.sbase + j * 32 + lane < it.send) mask |= 1u << j;
     }
-    // each seed's start state: the k-step jump, up to C windows of JW steps, up to M run pairs
-    u64 vs[RANGE_ITEM / 32], ns[RANGE_ITEM / 32];
-    u32 ss[RANGE_ITEM / 32];
-    u32 qmask = 0;
+    // each entry in turn: its seed's start state (the k-step jump, up to C windows of JW
+    // steps, up to M run pairs), then one ballot places the lanes' seeds in the queue
+    seeds = __reduce_add_sync(FULL, __popc(mask));
+    total = 0;
 #pragma unroll
     for (u32 j = 0; j < RANGE_ITEM / 32; j++) {
       const u32 f = (e[j].y >> 8) & 0xFFu, emax = e[j].y >> 24;
@@ -275,49 +264,39 @@ __device__ __forceinline__ bool expand64(Warp64& W, const RangeArgs& A, const ui
           chain_windows<JW, C, STATS>(v, st, nbl, w_thr_bl, s_win, s_pow3, X);
         }
       }
-      if (STATS && st == 0) X.replay++;
+      if (STATS && ((mask >> j) & 1u) && st == 0) X.replay++;
       const bool keep = ((mask >> j) & 1u) && first_pairs<M, STATS>(v, st, n, G, w_thr_st, s_pow3, X);
-      vs[j] = v;
-      ns[j] = n;
-      ss[j] = st;
-      qmask |= keep ? 1u << j : 0u;
-    }
-    seeds = __reduce_add_sync(FULL, __popc(mask));
-    pos = tail + queue_rank2(qmask, lane, &total);
-#pragma unroll
-    for (u32 j = 0; j < RANGE_ITEM / 32; j++) {
-      if ((qmask >> j) & 1u) {
-        const u32 cand = vs[j] >= G ? 1u : 0u;
-        W.q[pos & (Q64 - 1)] = make_uint4((u32)vs[j], (u32)(vs[j] >> 32), (u32)ns[j],
-                                          (u32)(ns[j] >> 32) | (slot << 16) | (cand << 21) | (ss[j] << 22));
-        pos++;
+      const u32 bk = __ballot_sync(FULL, keep);
+      if (keep) {
+        const u32 cand = v >= G ? 1u : 0u;
+        W.q[(tail + total + __popc(bk & lanemask_lt())) & (Q64 - 1)] =
+            make_uint4((u32)v, (u32)(v >> 32), (u32)n, (u32)(n >> 32) | (slot << 16) | (cand << 21) | (st << 22));
       }
+      total += __popc(bk);
     }
   } else {
     // integers below 2^k: [d, d + 64) of [q_lo, d_hi), no residue sieve
     const ull d = it.q_lo + 2ull * lane;
-    u64 vs[2];
-    u32 ss[2], qmask = 0;
 #pragma unroll
     for (u32 j = 0; j < 2; j++) {
       const ull n = d + j;
       if (n < it.d_hi && n >= 2 && (!it.mod9 || ((KEEP9 >> (u32)(n % 9u)) & 1u))) mask |= 1u << j;
-      vs[j] = n + 1;
-      ss[j] = 0;
-      const bool keep = ((mask >> j) & 1u) && first_pairs<M, STATS>(vs[j], ss[j], n, G, w_thr_st, s_pow3, X);
-      qmask |= keep ? 1u << j : 0u;
     }
     seeds = __reduce_add_sync(FULL, __popc(mask));
-    pos = tail + queue_rank2(qmask, lane, &total);
+    total = 0;
 #pragma unroll
     for (u32 j = 0; j < 2; j++) {
-      if ((qmask >> j) & 1u) {
-        const ull n = d + j;
-        const u32 cand = vs[j] >= G ? 1u : 0u;
-        W.q[pos & (Q64 - 1)] = make_uint4((u32)vs[j], (u32)(vs[j] >> 32), (u32)n,
-                                          (u32)(n >> 32) | (slot << 16) | (cand << 21) | (ss[j] << 22));
-        pos++;
+      const ull n = d + j;
+      u64 v = n + 1;
+      u32 st = 0;
+      const bool keep = ((mask >> j) & 1u) && first_pairs<M, STATS>(v, st, n, G, w_thr_st, s_pow3, X);
+      const u32 bk = __ballot_sync(FULL, keep);
+      if (keep) {
+        const u32 cand = v >= G ? 1u : 0u;
+        W.q[(tail + total + __popc(bk & lanemask_lt())) & (Q64 - 1)] =
+            make_uint4((u32)v, (u32)(v >> 32), (u32)n, (u32)(n >> 32) | (slot << 16) | (cand << 21) | (st << 22));
       }
+      total += __popc(bk);
     }
   }
   __syncwarp();

@@ -112,7 +112,7 @@ struct collatz_ctx {
   cudaStream_t own_stream = nullptr, stream = nullptr, copy_stream = nullptr;
   cz::CaseTables ct;
   std::map<uint32_t, cz::RangeTables> rt;
-  int cases_variant = 4, range_variant = 4;
+  int cases_variant = 4, range_variant = 0;
   // 64-bit range kernel: its variant, and the limb-width cutoff -- launches whose seeds
   // all have at most range64_bits bits run it, the others run the four-limb kernel
   int range64_variant = 0;

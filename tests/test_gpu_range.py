@@ -76,7 +76,7 @@ def test_range_variants_match_oracle(verifier, variant):
             o = O.range_verify(*q, method=1, nthreads=NT)
             _cmp(m, o)
     finally:
-        v.set_variant(1, 4)  # the defaults
+        v.set_variant(1, 0)  # the defaults
         v.set_variant(cb.MODE_RANGE64_BITS, cb.RANGE64_BITS_DEFAULT)
 
 
@@ -265,7 +265,7 @@ def test_window_variant_equals_plain(verifier, off, size, k):
         v.set_variant(1, 2)
         p = v.verify_range(off, size, k)
     finally:
-        v.set_variant(1, 4)  # the defaults
+        v.set_variant(1, 0)  # the defaults
         v.set_variant(cb.MODE_RANGE64_BITS, cb.RANGE64_BITS_DEFAULT)
     assert (w.seeds_checked, w.failures, w.widened, w.errors) == (p.seeds_checked, p.failures, p.widened, p.errors)
     assert (w.max_stopping_time, w.max_stopping_time_seed) == (p.max_stopping_time, p.max_stopping_time_seed)
@@ -288,7 +288,7 @@ def test_narrow_variant_equals_plain(verifier, off, size, k):
         v.set_variant(1, 2)
         p = v.verify_range(off, size, k)
     finally:
-        v.set_variant(1, 4)  # the defaults
+        v.set_variant(1, 0)  # the defaults
         v.set_variant(cb.MODE_RANGE64_BITS, cb.RANGE64_BITS_DEFAULT)
     assert (w.seeds_checked, w.failures, w.widened, w.errors) == (p.seeds_checked, p.failures, p.widened, p.errors)
     assert (w.max_stopping_time, w.max_stopping_time_seed) == (p.max_stopping_time, p.max_stopping_time_seed)
