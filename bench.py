@@ -56,12 +56,12 @@ OPS_JUMP, OPS_ODD, OPS_EVEN = 16, 14, 12
 #   frontier: 2^36 launch at 2^60, k = 34 (dram bytes per 2^34 block: each
 #             block streams the 5 mod-9 classes it keeps of the 2.43 GB table).
 NCU_CAPTURES = {
-    "block": {"src": "fbc65cb3163b5004", "dram_bytes": 4.886784e6 + 0.195584e6, "per": "launch",
-              "issue_slots_busy": 0.7565, "alu_pipe_busy": 0.6515},
-    "frontier": {"src": "fbc65cb3163b5004", "dram_bytes": (5.424081664e9 + 8.218368e6) / 4, "per": "2^34 block",
-                 "issue_slots_busy": 0.7686, "alu_pipe_busy": 0.6483},
+    "block": {"src": "06391b6039936ead", "dram_bytes": 5.126912e6 + 0.332032e6, "per": "launch",
+              "issue_slots_busy": 0.8029, "alu_pipe_busy": 0.6963, "kernel": "k_range64 (64-bit values)"},
+    "frontier": {"src": "06391b6039936ead", "dram_bytes": (5.425077760e9 + 8.011264e6) / 4, "per": "2^34 block",
+                 "issue_slots_busy": 0.7614, "alu_pipe_busy": 0.6795, "kernel": "k_range (four limbs)"},
 }
-KERNEL_SOURCES = ("range.cu", "common.cuh", "kernels.h", "tables.h", "tables.cu")
+KERNEL_SOURCES = ("range.cu", "range64.cu", "range_shared.cuh", "common.cuh", "kernels.h", "tables.h", "tables.cu")
 # CPU sample of the block workload, the same for the reference arm's steps and
 # the cpu_baseline leg: 2^32 seeds at 2^40 + i 2^32 with the k = 24 sieve.
 CPU_SAMPLE_LOG2 = 32
@@ -326,7 +326,7 @@ def run_cases() -> dict:
                                        "semantics cu:185-411 on one thread)"}}
 
 
-def run_reference_gpu_program(reps: int = 2) -> dict:
+def run_reference_gpu_program(reps: int = 3) -> dict:
     """The reference program itself -- collatz_cudav7.cu compiled unchanged
     for sm_100a (MAXBITS = 45, the source's own value; built from the
     reference's sources by oracle/build_ref_gpu.sh) -- against this
@@ -515,8 +515,8 @@ def roofline(workload: str, base: int, k: int, survivors: int, mean_ms: float, s
     if valid:
         # every issued instruction (work distribution included), where achieved/peak counts only
         # the algorithmic operations
-        d["ncu"] = {"issue_slots_busy": cap["issue_slots_busy"], "alu_pipe_busy": cap["alu_pipe_busy"],
-                    "kernel_sources": cap["src"],
+        d["ncu"] = {"kernel": cap["kernel"], "issue_slots_busy": cap["issue_slots_busy"],
+                    "alu_pipe_busy": cap["alu_pipe_busy"], "kernel_sources": cap["src"],
                     "metrics": "sm__inst_issued.avg.pct_of_peak_sustained_active, "
                                "sm__pipe_alu_cycles_active.avg.pct_of_peak_sustained_active"}
     return d
