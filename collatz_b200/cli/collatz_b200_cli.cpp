@@ -7,7 +7,9 @@
 // prints every seed whose trajectory reaches 2^100 on stdout in the
 // reference's format (cu:298) and the reference's summary line on stderr
 // (cu:181-182), followed by one "# results {...}" JSON line with the outputs
-// the reference does not compute.  N defaults to 45 (MAXBITS, cu:43) or the
+// the reference does not compute, the device time (device_ms) and the wall
+// time of the run after the context and its tables exist (run_ms).  N
+// defaults to 45 (MAXBITS, cu:43) or the
 // COLLATZ_MAXBITS environment variable.
 //
 //   collatz_b200 --cases FILE [--journal JOURNAL] [N]
@@ -20,6 +22,7 @@
 //
 // Step 1 (search1, cu:497-563) runs on the GPU; --host-step1 runs it on the
 // host threads instead (same outputs).
+#include <chrono>
 #include <cinttypes>
 #include <fstream>
 #include <cstdio>
@@ -103,12 +106,14 @@ int main(int argc, char** argv) {
   r.overflow_seeds = ov.data();
   r.overflow_cap = cap;
   uint32_t n_run = 1;
+  const auto t_run = std::chrono::steady_clock::now();  // after the context and tables exist
   if (cases_file.empty()) {
     rc = collatz_run_case(ctx, &cases[0], &r);
   } else {
     rc = collatz_run_cases(ctx, cases.data(), (uint32_t)cases.size(), journal.empty() ? nullptr : journal.c_str(),
                            nullptr, &r, &n_run);
   }
+  const double run_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_run).count();
   if (rc && rc != COLLATZ_E_DEVICE) {
     std::fprintf(stderr, "collatz_run_case: %s: %s\n", collatz_status_string(rc), collatz_last_error(ctx));
     collatz_destroy(ctx);
@@ -123,11 +128,11 @@ int main(int argc, char** argv) {
                "# results {\"seeds_checked\": %" PRIu64 ", \"pairs\": %" PRIu64 ", \"cpu_pairs\": %" PRIu64
                ", \"overflow\": %" PRIu64
                ", \"max_excursion\": \"%s\", \"max_excursion_seed\": \"%s\", \"max_stopping_time\": %" PRIu64
-               ", \"max_stopping_time_seed\": \"%s\", \"errors\": %u, \"device_ms\": %.3f, \"cases\": %zu"
-               ", \"cases_run\": %u}\n",
+               ", \"max_stopping_time_seed\": \"%s\", \"errors\": %u, \"device_ms\": %.3f, \"run_ms\": %.3f"
+               ", \"cases\": %zu, \"cases_run\": %u}\n",
                r.seeds_checked, r.pairs, r.cpu_pairs, r.n_overflow, u128s(r.max_excursion, 4).c_str(),
                u128s(r.max_excursion_seed, 4).c_str(), r.max_stopping_time, u128s(r.max_stopping_time_seed, 4).c_str(),
-               r.errors, r.device_ms, cases.size(), n_run);
+               r.errors, r.device_ms, run_ms, cases.size(), n_run);
   collatz_destroy(ctx);
   return r.errors ? 4 : 0;
 }

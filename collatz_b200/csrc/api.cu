@@ -1360,59 +1360,36 @@ extern "C" int collatz_trajectory(collatz_ctx* c, const uint32_t* seeds, uint32_
   std::lock_guard<std::recursive_mutex> g(c->mu);
   DeviceScope dev_scope(c->device);
   CK(c, dev_scope.err);
-  static const int classes[5] = {4, 6, 8, 12, 16};
-  std::vector<std::vector<uint32_t>> lists(5);
-  for (uint32_t i = 0; i < n; i++) {
-    uint32_t bl = 0;
-    for (int j = 7; j >= 0; j--)
-      if (seeds[8ull * i + j]) {
-        bl = 32u * j + (32u - __builtin_clz(seeds[8ull * i + j]));
-        break;
-      }
-    int cl = bl <= 96 ? 0 : bl <= 160 ? 1 : bl <= 224 ? 2 : bl <= 352 ? 3 : 4;
-    lists[cl].push_back(i);
-  }
+  // seed ids sorted by limb class, then one launch for every class
+  uint32_t cnt[5] = {0, 0, 0, 0, 0};
+  std::vector<uint8_t> cls(n);
+  for (uint32_t i = 0; i < n; i++) cnt[cls[i] = (uint8_t)traj_class(seeds + 8ull * i)]++;
+  TrajAllArgs a;
+  a.cstart[0] = 0;
+  for (int j = 0; j < 5; j++) a.cstart[j + 1] = a.cstart[j] + cnt[j];
+  CK(c, c->h_pairs.ensure(4ull * n));
+  uint32_t* idx = c->h_pairs.as<uint32_t>();
+  uint32_t fill[5];
+  for (int j = 0; j < 5; j++) fill[j] = a.cstart[j];
+  for (uint32_t i = 0; i < n; i++) idx[fill[cls[i]]++] = i;
   CK(c, c->t_seeds.ensure(32ull * n));
   CK(c, c->t_st.ensure(8ull * n));
   CK(c, c->t_exc.ensure(64ull * n));
   CK(c, c->t_status.ensure(4ull * n));
   CK(c, c->t_idx[0].ensure(4ull * n));
-  CK(c, c->t_idx[1].ensure(4ull * n));
   CK(c, c->t_cnt.ensure(16));
   CK(c, cudaMemcpyAsync(c->t_seeds.p, seeds, 32ull * n, cudaMemcpyHostToDevice, c->stream));
-  std::vector<uint32_t> carry;
-  for (int ci = 0; ci < 5; ci++) {
-    std::vector<uint32_t>& L = lists[ci];
-    L.insert(L.end(), carry.begin(), carry.end());
-    carry.clear();
-    if (L.empty()) continue;
-    CK(c, cudaMemcpyAsync(c->t_idx[0].p, L.data(), 4ull * L.size(), cudaMemcpyHostToDevice, c->stream));
-    CK(c, cudaMemsetAsync(c->t_cnt.p, 0, 16, c->stream));
-    TrajArgs a;
-    a.seeds = c->t_seeds.as<uint32_t>();
-    a.nseeds = n;
-    a.index = c->t_idx[0].as<uint32_t>();
-    a.nindex = (uint32_t)L.size();
-    a.nindex_dev = nullptr;
-    a.st = c->t_st.as<unsigned long long>();
-    a.exc = c->t_exc.as<uint32_t>();
-    a.status = c->t_status.as<uint32_t>();
-    a.next = ci < 4 ? c->t_idx[1].as<uint32_t>() : nullptr;
-    a.next_count = c->t_cnt.as<uint32_t>();
-    a.cursor = c->t_cnt.as<uint32_t>() + 1;
-    a.iter_cap = c->iter_cap;
-    const uint32_t grid = std::min<uint32_t>((uint32_t)(L.size() + 127) / 128, (uint32_t)c->sm_count * 8);
-    CK(c, launch_traj(a, classes[ci], grid, c->stream));
-    if (ci < 4) {
-      uint32_t cnt = 0;
-      CK(c, cudaMemcpyAsync(&cnt, c->t_cnt.p, 4, cudaMemcpyDeviceToHost, c->stream));
-      CK(c, cudaStreamSynchronize(c->stream));
-      if (cnt) {
-        carry.resize(cnt);
-        CK(c, cudaMemcpy(carry.data(), c->t_idx[1].p, 4ull * cnt, cudaMemcpyDeviceToHost));
-      }
-    }
-  }
+  CK(c, cudaMemcpyAsync(c->t_idx[0].p, idx, 4ull * n, cudaMemcpyHostToDevice, c->stream));
+  CK(c, cudaMemsetAsync(c->t_cnt.p, 0, 16, c->stream));
+  a.seeds = c->t_seeds.as<uint32_t>();
+  a.index = c->t_idx[0].as<uint32_t>();
+  a.st = c->t_st.as<unsigned long long>();
+  a.exc = c->t_exc.as<uint32_t>();
+  a.status = c->t_status.as<uint32_t>();
+  a.cursor = c->t_cnt.as<uint32_t>();
+  a.iter_cap = c->iter_cap;
+  const uint32_t grid = std::min<uint32_t>((n + 127) / 128, (uint32_t)c->sm_count * 8);
+  CK(c, launch_traj_all(a, grid, c->stream));
   CK(c, cudaMemcpyAsync(st, c->t_st.p, 8ull * n, cudaMemcpyDeviceToHost, c->stream));
   CK(c, cudaMemcpyAsync(exc, c->t_exc.p, 64ull * n, cudaMemcpyDeviceToHost, c->stream));
   CK(c, cudaMemcpyAsync(status, c->t_status.p, 4ull * n, cudaMemcpyDeviceToHost, c->stream));

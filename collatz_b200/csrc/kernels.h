@@ -175,4 +175,32 @@ struct TrajArgs {
 };
 cudaError_t launch_traj(const TrajArgs& a, int limbs, uint32_t grid, cudaStream_t st);
 
+// All limb classes in one launch (traj.cu): index = the seed ids sorted by
+// limb class (4, 6, 8, 12, 16 limbs; class j at [cstart[j], cstart[j + 1])),
+// one cursor (zero before the launch); a seed that needs more limbs is run
+// again by the same thread with the next width.
+struct TrajAllArgs {
+  const uint32_t* seeds;       // nseeds x 8 limbs
+  const uint32_t* index;       // cstart[5] entries
+  uint32_t cstart[6];
+  unsigned long long* st;      // out: stopping time
+  uint32_t* exc;               // out: 16 limbs each
+  uint32_t* status;            // out: 0 ok, 1 trivial, 2 overflow, 3 iteration cap
+  uint32_t* cursor;            // scratch
+  uint32_t iter_cap;
+};
+cudaError_t launch_traj_all(const TrajAllArgs& a, uint32_t grid, cudaStream_t st);
+// Limb class of a seed of at most 256 bits (8 little-endian limbs): 0..4 for
+// 4, 6, 8, 12, 16 limbs, leaving room for the value to grow before it is
+// handed on.
+inline uint32_t traj_class(const uint32_t* w) {
+  uint32_t bl = 0;
+  for (int j = 7; j >= 0; j--)
+    if (w[j]) {
+      bl = 32u * j + (32u - __builtin_clz(w[j]));
+      break;
+    }
+  return bl <= 96 ? 0 : bl <= 160 ? 1 : bl <= 224 ? 2 : bl <= 352 ? 3 : 4;
+}
+
 }  // namespace cz

@@ -315,6 +315,8 @@ __device__ __forceinline__ bool expand64(Warp64& W, const RangeArgs& A, const ui
 
 template <int R, int MINB, int J, int JW, int C, int M, bool STATS>
 __global__ void __launch_bounds__(R64_WARPS * 32, MINB) k_range64(const RangeArgs A) {
+  // a queued seed's steps: k <= 34, C windows of JW steps, M run pairs of at most 7 + 31 steps
+  static_assert(34 + C * JW + M * 38 <= ST_ENTRY_MAX, "the step count of a queue entry has 10 bits");
   extern __shared__ __align__(16) unsigned char range64_smem[];
   Warp64* S = reinterpret_cast<Warp64*>(range64_smem);
   __shared__ unsigned long long s_p3[41];

@@ -38,6 +38,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <functional>
 #include <mutex>
 #include <thread>
 #include <unordered_map>
@@ -61,8 +62,6 @@ constexpr uint32_t MAX_BATCH_SEEDS = 1u << 22;
 // up to 45 (9 residues of q mod 9 x 5 kept classes) for the whole blocks in
 // between; more is allocated on demand.
 constexpr size_t SEGS_PER_REQ = 64;
-constexpr int NCLASS = 5;
-constexpr int CLASS_LIMBS[NCLASS] = {4, 6, 8, 12, 16};
 
 // host-time buckets of the worker threads
 enum { T_ADMIT, T_BUILD, T_COMPLETE, T_IDLE, T_N };
@@ -103,17 +102,75 @@ struct Batch {
 
 double since(Clock::time_point t0) { return std::chrono::duration<double>(Clock::now() - t0).count(); }
 
-uint32_t seed_class(const uint32_t* w) {
-  uint32_t bl = 0;
-  for (int j = 7; j >= 0; j--)
-    if (w[j]) {
-      bl = 32u * j + (32u - __builtin_clz(w[j]));
-      break;
+// A fixed set of host threads for the query path's copies (gathering query
+// seeds into the pinned batch, scattering results into the callers'
+// buffers).  run(parts, fn) calls fn(p) for every p in [0, parts) on the pool
+// and on the calling thread, and returns when all have finished.  One caller
+// at a time (the query thread).
+struct CopyPool {
+  std::vector<std::thread> th;
+  std::mutex mu;
+  std::condition_variable cv, cv_done;
+  std::function<void(int)> job;
+  std::atomic<int> next{0}, done{0};
+  int parts = 0;
+  uint64_t gen = 0;
+  bool stop = false;
+
+  void work() {
+    for (int p; (p = next.fetch_add(1)) < parts;) {
+      job(p);
+      if (done.fetch_add(1) + 1 == parts) {
+        std::lock_guard<std::mutex> g(mu);
+        cv_done.notify_all();
+      }
     }
-  // the same classes as collatz_trajectory: a class of L limbs takes seeds
-  // that leave room for the value to grow before it is handed on
-  return bl <= 96 ? 0 : bl <= 160 ? 1 : bl <= 224 ? 2 : bl <= 352 ? 3 : 4;
-}
+  }
+  void start(int n) {
+    for (int i = 0; i < n; i++)
+      th.emplace_back([this] {
+        uint64_t seen = 0;
+        for (;;) {
+          {
+            std::unique_lock<std::mutex> g(mu);
+            cv.wait(g, [&] { return stop || gen != seen; });
+            if (stop) return;
+            seen = gen;
+          }
+          work();
+        }
+      });
+  }
+  void run(int nparts, const std::function<void(int)>& fn) {
+    if (nparts <= 1 || th.empty()) {
+      for (int p = 0; p < nparts; p++) fn(p);
+      return;
+    }
+    {
+      std::lock_guard<std::mutex> g(mu);
+      job = fn;
+      parts = nparts;
+      next = 0;
+      done = 0;
+      gen++;
+    }
+    cv.notify_all();
+    work();
+    std::unique_lock<std::mutex> g(mu);
+    cv_done.wait(g, [&] { return done.load() >= parts; });
+  }
+  void shutdown() {
+    {
+      std::lock_guard<std::mutex> g(mu);
+      stop = true;
+    }
+    cv.notify_all();
+    for (std::thread& t : th) t.join();
+    th.clear();
+  }
+};
+
+constexpr uint64_t COPY_PART_SEEDS = 1u << 14;  // seeds per part of a parallel copy
 
 }  // namespace
 
@@ -123,7 +180,6 @@ struct collatz_server {
   cudaStream_t sa = nullptr, sb = nullptr;
   cudaMemPool_t pool = nullptr;
   Clock::time_point t0;
-  uint32_t grid = 0;
   size_t total_mem = 0;
 
   // guarded by mu
@@ -157,6 +213,7 @@ struct collatz_server {
   std::deque<int> batch_order;
 
   std::thread thr_range, thr_query;
+  CopyPool copy_pool;
 };
 
 namespace {
@@ -435,6 +492,55 @@ void admit_queries(collatz_server* s) {
   }
 }
 
+// Seeds of the requests of B whose batch positions overlap [lo, hi): calls
+// fn(request, first seed of the request in range, seeds in range).
+template <class F>
+void for_range(const Batch& B, uint64_t lo, uint64_t hi, F fn) {
+  size_t a = 0, b = B.reqs.size();
+  while (b - a > 1) {  // the last request starting at or before lo
+    const size_t m = (a + b) / 2;
+    if (B.reqs[m]->batch_off <= lo) a = m; else b = m;
+  }
+  for (size_t i = a; i < B.reqs.size() && B.reqs[i]->batch_off < hi; i++) {
+    Req* r = B.reqs[i];
+    const uint64_t r0 = std::max<uint64_t>(lo, r->batch_off), r1 = std::min<uint64_t>(hi, r->batch_off + r->q.nseeds);
+    if (r1 > r0) fn(r, r0 - r->batch_off, r1 - r0);
+  }
+}
+
+// Copies the batch's seeds into hs (pinned), sorts their ids by limb class
+// into hi and sets cstart; in parts on the copy pool for large batches.
+void gather_batch(collatz_server* s, Batch& B, uint32_t* hs, uint32_t* hi, uint32_t* cstart) {
+  const uint64_t n = B.n;
+  B.cls.resize(n);
+  const int parts = (int)std::max<uint64_t>(1, std::min<uint64_t>((n + COPY_PART_SEEDS - 1) / COPY_PART_SEEDS, 64));
+  std::vector<uint32_t> cnt((size_t)parts * 5, 0);
+  auto lo_of = [&](int p) { return n * (uint64_t)p / (uint64_t)parts; };
+  s->copy_pool.run(parts, [&](int p) {
+    const uint64_t lo = lo_of(p), hi_ = lo_of(p + 1);
+    for_range(B, lo, hi_, [&](Req* r, uint64_t first, uint64_t m) {
+      std::memcpy(hs + 8ull * (r->batch_off + first), r->q.seeds + 8ull * first, 32ull * m);
+    });
+    uint32_t* c = &cnt[(size_t)p * 5];
+    for (uint64_t i = lo; i < hi_; i++) c[B.cls[i] = (uint8_t)traj_class(hs + 8 * i)]++;
+  });
+  // class-major positions: class j, then part p within it
+  std::vector<uint32_t> fill((size_t)parts * 5);
+  uint32_t off = 0;
+  for (int j = 0; j < 5; j++) {
+    cstart[j] = off;
+    for (int p = 0; p < parts; p++) {
+      fill[(size_t)p * 5 + j] = off;
+      off += cnt[(size_t)p * 5 + j];
+    }
+  }
+  cstart[5] = off;
+  s->copy_pool.run(parts, [&](int p) {
+    uint32_t* f = &fill[(size_t)p * 5];
+    for (uint64_t i = lo_of(p); i < lo_of(p + 1); i++) hi[f[B.cls[i]]++] = (uint32_t)i;
+  });
+}
+
 // Builds and enqueues one trajectory batch.  Returns 1 if one was launched,
 // 0 if there are no queries waiting, negative on error.
 int launch_batch(collatz_server* s, int bi) {
@@ -455,34 +561,21 @@ int launch_batch(collatz_server* s, int bi) {
   // host: seeds into pinned memory, class lists (region j holds class j's
   // own seeds followed by room for every seed of the narrower classes)
   cudaError_t e = B.h_seeds.ensure(32 * n);
-  if (!e) e = B.h_idx.ensure(4 * NCLASS * n);
+  if (!e) e = B.h_idx.ensure(4 * n);
   if (!e) e = B.h_cnt.ensure(64);
   if (!e) e = B.h_st.ensure(8 * n);
   if (!e) e = B.h_exc.ensure(64 * n);
   if (!e) e = B.h_status.ensure(4 * n);
   if (e) return set_cuda_error(c, e, "server batch buffers");
   uint32_t* hs = B.h_seeds.as<uint32_t>();
-  for (Req* r : B.reqs) std::memcpy(hs + 8ull * r->batch_off, r->q.seeds, 32ull * r->q.nseeds);
-  uint32_t len[NCLASS] = {0, 0, 0, 0, 0};
-  B.cls.resize(n);
-  for (uint64_t i = 0; i < n; i++) len[B.cls[i] = (uint8_t)seed_class(hs + 8 * i)]++;
-  uint64_t base[NCLASS], cap[NCLASS], before = 0, off = 0;
-  for (int j = 0; j < NCLASS; j++) {
-    base[j] = off;
-    cap[j] = len[j] + before;
-    before += len[j];
-    off += cap[j];
-  }
   uint32_t* hi = B.h_idx.as<uint32_t>();
-  uint64_t fill[NCLASS];
-  for (int j = 0; j < NCLASS; j++) fill[j] = base[j];
-  for (uint64_t i = 0; i < n; i++) hi[fill[B.cls[i]]++] = (uint32_t)i;
+  TrajAllArgs a;
+  gather_batch(s, B, hs, hi, a.cstart);
   uint32_t* hc = B.h_cnt.as<uint32_t>();
   for (int j = 0; j < 16; j++) hc[j] = 0;
-  for (int j = 0; j < NCLASS; j++) hc[j] = len[j];  // [0..4] list lengths, [8..12] cursors
   // device: one block from the server's pool, freed in stream order
   const uint64_t o_st = 32 * n, o_exc = o_st + 8 * n, o_status = o_exc + 64 * n, o_idx = o_status + 4 * n,
-                 o_cnt = (o_idx + 4 * off + 255) & ~255ull, bytes = o_cnt + 64;
+                 o_cnt = (o_idx + 4 * n + 255) & ~255ull, bytes = o_cnt + 64;
   cudaStream_t st = s->sb;
   void* block = nullptr;
   e = cudaMallocFromPoolAsync(&block, bytes, s->pool, st);
@@ -495,29 +588,19 @@ int launch_batch(collatz_server* s, int bi) {
   }
   char* d = static_cast<char*>(block);
   e = cudaMemcpyAsync(d, hs, 32 * n, cudaMemcpyHostToDevice, st);
-  if (!e) e = cudaMemcpyAsync(d + o_idx, hi, 4 * off, cudaMemcpyHostToDevice, st);
+  if (!e) e = cudaMemcpyAsync(d + o_idx, hi, 4 * n, cudaMemcpyHostToDevice, st);
   if (!e) e = cudaMemcpyAsync(d + o_cnt, hc, 64, cudaMemcpyHostToDevice, st);
-  uint32_t* cnt = reinterpret_cast<uint32_t*>(d + o_cnt);
-  uint32_t* idx = reinterpret_cast<uint32_t*>(d + o_idx);
-  uint64_t reach = 0;  // seeds that may arrive in class j
-  for (int j = 0; j < NCLASS && !e; j++) {
-    reach += len[j];
-    if (reach == 0) continue;
-    TrajArgs a;
+  if (!e) {
+    // every limb class in one launch: a seed that needs more limbs is re-run by its thread
     a.seeds = reinterpret_cast<const uint32_t*>(d);
-    a.nseeds = (uint32_t)n;
-    a.index = idx + base[j];
-    a.nindex = (uint32_t)cap[j];
-    a.nindex_dev = cnt + j;
+    a.index = reinterpret_cast<const uint32_t*>(d + o_idx);
     a.st = reinterpret_cast<unsigned long long*>(d + o_st);
     a.exc = reinterpret_cast<uint32_t*>(d + o_exc);
     a.status = reinterpret_cast<uint32_t*>(d + o_status);
-    a.next = (j + 1 < NCLASS) ? idx + base[j + 1] : nullptr;
-    a.next_count = (j + 1 < NCLASS) ? cnt + j + 1 : cnt + 15;
-    a.cursor = cnt + 8 + j;
+    a.cursor = reinterpret_cast<uint32_t*>(d + o_cnt);
     a.iter_cap = c->iter_cap;
-    const uint32_t grid = (uint32_t)std::min<uint64_t>((reach + 127) / 128, (uint64_t)c->sm_count * 8);
-    e = launch_traj(a, CLASS_LIMBS[j], grid, st);
+    const uint32_t grid = (uint32_t)std::min<uint64_t>((n + 127) / 128, (uint64_t)c->sm_count * 8);
+    e = launch_traj_all(a, grid, st);
   }
   if (!e) e = cudaMemcpyAsync(B.h_st.p, d + o_st, 8 * n, cudaMemcpyDeviceToHost, st);
   if (!e) e = cudaMemcpyAsync(B.h_exc.p, d + o_exc, 64 * n, cudaMemcpyDeviceToHost, st);
@@ -535,11 +618,19 @@ int launch_batch(collatz_server* s, int bi) {
 
 void complete_batch(collatz_server* s, int bi) {
   Batch& B = s->batches[bi];
+  // results into the callers' buffers, in parts on the copy pool for large batches
+  const uint64_t n = B.n;
+  const int parts = (int)std::max<uint64_t>(1, std::min<uint64_t>((n + COPY_PART_SEEDS - 1) / COPY_PART_SEEDS, 64));
+  s->copy_pool.run(parts, [&](int p) {
+    for_range(B, n * (uint64_t)p / (uint64_t)parts, n * (uint64_t)(p + 1) / (uint64_t)parts,
+              [&](Req* r, uint64_t first, uint64_t m) {
+                const uint64_t o = r->batch_off + first;
+                std::memcpy(r->q.stopping_time + first, B.h_st.as<uint64_t>() + o, 8 * m);
+                std::memcpy(r->q.excursion + 16 * first, B.h_exc.as<uint32_t>() + 16 * o, 64 * m);
+                std::memcpy(r->q.status + first, B.h_status.as<uint32_t>() + o, 4 * m);
+              });
+  });
   for (Req* r : B.reqs) {
-    const uint64_t o = r->batch_off, m = r->q.nseeds;
-    std::memcpy(r->q.stopping_time, B.h_st.as<uint64_t>() + o, 8 * m);
-    std::memcpy(r->q.excursion, B.h_exc.as<uint32_t>() + 16 * o, 64 * m);
-    std::memcpy(r->q.status, B.h_status.as<uint32_t>() + o, 4 * m);
     s->active[1]--;
     publish(s, r, COLLATZ_OK);
   }
@@ -689,6 +780,7 @@ int query_pass(collatz_server* s, double* t, Clock::time_point tp, bool& busy_de
 
 void destroy(collatz_server* s) {
   if (!s) return;
+  s->copy_pool.shutdown();
   if (s->ctx) {
     cudaSetDevice(s->ctx->device);
     if (s->sa) cudaStreamSynchronize(s->sa);
@@ -793,16 +885,13 @@ extern "C" int collatz_server_start(const collatz_config* cfg, const collatz_ser
   for (Batch& B : s->batches) {
     if ((e = cudaEventCreateWithFlags(&B.done, cudaEventDisableTiming))) return fail(e, "event");
     if ((e = B.h_seeds.ensure(32 * nb))) return fail(e, "batch");
-    if ((e = B.h_idx.ensure(4 * NCLASS * nb))) return fail(e, "batch");
+    if ((e = B.h_idx.ensure(4 * nb))) return fail(e, "batch");
     if ((e = B.h_cnt.ensure(64))) return fail(e, "batch");
     if ((e = B.h_st.ensure(8 * nb))) return fail(e, "batch");
     if ((e = B.h_exc.ensure(64 * nb))) return fail(e, "batch");
     if ((e = B.h_status.ensure(4 * nb))) return fail(e, "batch");
     B.cls.reserve(nb);
   }
-  int bps = 0;
-  if (range_occupancy(c->range_variant, &bps) != cudaSuccess || bps <= 0) bps = 1;
-  s->grid = (uint32_t)(bps * c->sm_count);
   size_t fr = 0;
   if ((e = cudaMemGetInfo(&fr, &s->total_mem))) return fail(e, "cudaMemGetInfo");
   {
@@ -810,6 +899,8 @@ extern "C" int collatz_server_start(const collatz_config* cfg, const collatz_ser
     refresh_budget(s);
   }
   for (uint32_t i = s->cfg.max_active; i-- > 0;) s->free_slots.push_back(i);
+  // helpers for the query path's host copies: up to 7, half the host's threads at most
+  s->copy_pool.start((int)std::min(7u, std::max(1u, std::thread::hardware_concurrency() / 2) - 1u));
   s->t0 = Clock::now();
   s->thr_range = std::thread([s] { worker(s, true, [s](double* t, Clock::time_point tp, bool& b) {
                                        return range_pass(s, t, tp, b);
