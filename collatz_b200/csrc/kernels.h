@@ -159,22 +159,6 @@ cudaError_t launch_range_wide(const WidenEntry* list, const uint32_t* count, uin
                               uint32_t iter_cap, cudaStream_t st, bool negative = false);
 
 // ---------------- trajectory queries (traj.cu) ----------------
-struct TrajArgs {
-  const uint32_t* seeds;       // nseeds x 8 limbs
-  uint32_t nseeds;
-  const uint32_t* index;       // optional: seeds to process (nullptr = all)
-  uint32_t nindex;             // capacity of index
-  const uint32_t* nindex_dev;  // optional: index length on the device (<= nindex)
-  unsigned long long* st;      // out: stopping time
-  uint32_t* exc;               // out: 16 limbs each
-  uint32_t* status;            // out: 0 ok, 1 trivial, 2 overflow, 3 iteration cap
-  uint32_t* next;              // seeds that need more limbs
-  uint32_t* next_count;
-  uint32_t* cursor;            // scratch
-  uint32_t iter_cap;
-};
-cudaError_t launch_traj(const TrajArgs& a, int limbs, uint32_t grid, cudaStream_t st);
-
 // All limb classes in one launch (traj.cu): index = the seed ids sorted by
 // limb class (4, 6, 8, 12, 16 limbs; class j at [cstart[j], cstart[j + 1])),
 // one cursor (zero before the launch); a seed that needs more limbs is run

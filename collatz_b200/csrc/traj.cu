@@ -4,8 +4,9 @@
 //
 // One seed per lane with per-lane dynamic fetch, so the warp stays busy
 // while seeds of very different lengths finish.  The host sorts seeds by
-// bit length into limb classes (L = 4, 6, 8, 12, 16); a seed whose value
-// could leave L limbs is queued for the next class.
+// bit length into limb classes (L = 4, 6, 8, 12, 16) and one launch serves
+// every class; a seed whose value could leave L limbs is run again by its
+// thread with the next width.
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -19,112 +20,13 @@ __device__ __forceinline__ void load_seed(const u32* __restrict__ s, Limbs<L>& n
   for (int j = 0; j < L; j++) n.w[j] = (j < 8) ? s[j < 8 ? j : 0] : 0u;
 }
 
-template <int L, int ITERS>
-__global__ void __launch_bounds__(128) k_traj(const TrajArgs A) {
-  __shared__ u32 s_pow3[9];
-  if (threadIdx.x < 9) {
-    u32 p = 1;
-    for (u32 i = 0; i < threadIdx.x; i++) p *= 3;
-    s_pow3[threadIdx.x] = p;
-  }
-  __syncthreads();
-  const u32 count = A.index ? (A.nindex_dev ? min(*A.nindex_dev, A.nindex) : A.nindex) : A.nseeds;
-  u32 slot = atomicAdd(A.cursor, 1u);
-  bool active = false;
-  Limbs<L> v, N, E;
-  unsigned long long st = 0;
-  u32 it = 0, sid = 0;
-
-  auto start = [&]() {
-    while (slot < count) {
-      sid = A.index ? A.index[slot] : slot;
-      load_seed<L>(A.seeds + 8ull * sid, N);
-      bool small = N.w[0] < 2u;
-#pragma unroll
-      for (int j = 1; j < L; j++) small = small & (N.w[j] == 0u);
-      if (!small) {
-        v = N;
-        inc_l<L>(v);
-        E = N;
-        st = 0;
-        it = 0;
-        active = true;
-        return;
-      }
-      A.st[sid] = 0;  // n = 0, 1: no stopping time
-#pragma unroll
-      for (int j = 0; j < 16; j++) A.exc[16ull * sid + j] = (j < L) ? N.w[j < L ? j : 0] : 0u;
-      A.status[sid] = 1;
-      slot = atomicAdd(A.cursor, 1u);
-    }
-  };
-  start();
-
-  while (__any_sync(FULL, active)) {
-    if (active) {
-#pragma unroll 1
-      for (int r = 0; r < ITERS; r++) {
-        int fin = 0;  // 1 done, 2 needs more limbs, 3 iteration cap
-        if (v.w[L - 1] >= (1u << 19)) {
-          fin = 2;
-        } else if (++it > A.iter_cap) {
-          fin = 3;
-        } else {
-          const u32 a = ctz32(v.w[0] | (1u << 8));
-          odd_run_l<L>(v, a, s_pow3[a]);
-          st += a;
-          Limbs<L> x = v;
-          dec_l<L>(x);
-          if (limbs_lt<L>(E, x)) E = x;
-          const u32 b = ctz32(x.w[0] | 0x80000000u);
-          Limbs<L> w = x;
-          shr_l<L>(w, b);
-          if (b != 0 && limbs_lt<L>(w, N)) {
-            u32 s = 1;
-            for (; s < b; s++) {
-              Limbs<L> y = x;
-              shr_l<L>(y, s);
-              if (limbs_lt<L>(y, N)) break;
-            }
-            st += s;
-            fin = 1;
-          } else {
-            st += b;
-            v = w;
-            inc_l<L>(v);
-          }
-        }
-        if (fin) {
-          if (fin == 1) {
-            A.st[sid] = st;
-#pragma unroll
-            for (int j = 0; j < 16; j++) A.exc[16ull * sid + j] = (j < L) ? E.w[j < L ? j : 0] : 0u;
-            A.status[sid] = 0;
-          } else if (fin == 2 && A.next) {
-            A.next[atomicAdd(A.next_count, 1u)] = sid;
-          } else {
-            A.st[sid] = 0;
-#pragma unroll
-            for (int j = 0; j < 16; j++) A.exc[16ull * sid + j] = 0u;
-            A.status[sid] = (fin == 2) ? 2u : 3u;
-          }
-          active = false;
-          slot = atomicAdd(A.cursor, 1u);
-          start();
-          break;
-        }
-      }
-    }
-  }
-}
-
 // ------------------------------------------------------------------
 // All limb classes in one launch.  index holds the seed ids sorted by class
 // (class j at [cstart[j], cstart[j + 1]); classes of 4, 6, 8, 12, 16 limbs);
 // every lane takes the next slot from one cursor and runs that seed with its
 // class's width.  A seed whose value could leave L limbs is run again from
 // the start with the next width, by the same thread; past 16 limbs its status
-// is 2.  Results are those of the per-class chain of launch_traj.
+// is 2.
 // ------------------------------------------------------------------
 template <int L>
 struct WiderLimbs {
@@ -223,18 +125,6 @@ __global__ void __launch_bounds__(128) k_traj_all(const TrajAllArgs A) {
 
 cudaError_t launch_traj_all(const TrajAllArgs& a, u32 grid, cudaStream_t st) {
   k_traj_all<<<grid, 128, 0, st>>>(a);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_traj(const TrajArgs& a, int limbs, u32 grid, cudaStream_t st) {
-  switch (limbs) {
-    case 4: k_traj<4, 8><<<grid, 128, 0, st>>>(a); break;
-    case 6: k_traj<6, 8><<<grid, 128, 0, st>>>(a); break;
-    case 8: k_traj<8, 8><<<grid, 128, 0, st>>>(a); break;
-    case 12: k_traj<12, 4><<<grid, 128, 0, st>>>(a); break;
-    case 16: k_traj<16, 4><<<grid, 128, 0, st>>>(a); break;
-    default: return cudaErrorInvalidValue;
-  }
   return cudaGetLastError();
 }
 
