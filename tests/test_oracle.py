@@ -309,3 +309,29 @@ def test_split_rejects_bad_cut():
     for n, tup, cut in ((26, (3, 2, 2, 9, 1, 0), 1), (26, (3, 2, 2, 9, 1, 0), 17), (15, (3, 2, 2, 9, 1, 0), 4)):
         with pytest.raises(cb.CollatzError):
             cb.split_cases(n, tup, cut)
+
+
+@pytest.mark.parametrize("j", [8, 10, 11])
+def test_jump_table_bounds(j):
+    """The range kernels' j-step windows rest on 0 <= T^i(r) < 2^(j-i) 3^(f_i)
+    for every r < 2^j and 1 <= i <= j (f_i: odd steps among the first i), so
+    that for x = a 2^j + r, a g(r) <= T^i(x) < (a + 1) h(r) with g, h the least
+    and largest of the j multipliers 2^(j-i) 3^(f_i).  Also checks that the
+    table entry fits its fields: T^j(r) in 18 bits, f_j in 4, bit lengths of g
+    and h in 5."""
+    for r in range(1 << j):
+        x, f, ms = r, 0, []
+        for i in range(1, j + 1):
+            if x & 1:
+                x, f = (3 * x + 1) // 2, f + 1
+            else:
+                x //= 2
+            m = (1 << (j - i)) * 3 ** f
+            assert 0 <= x < m
+            ms.append(m)
+        assert x < 1 << 18 and f < 16 and max(ms).bit_length() < 32
+        for a in (1, 2, 3, 1 << 40, (1 << 40) + 12345):
+            y = a * (1 << j) + r
+            for i in range(1, j + 1):
+                y = (3 * y + 1) // 2 if y & 1 else y // 2
+                assert a * min(ms) <= y < (a + 1) * max(ms)
