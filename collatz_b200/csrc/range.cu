@@ -101,7 +101,7 @@ __device__ __forceinline__ bool first_pairs4(u32& V0, u32& V1, u32& V2, u32& V3,
   return true;
 }
 
-template <bool STATS, bool NEG, bool WIN, int M, class WT>
+template <bool STATS, bool NEG, int JW, int M, class WT>
 __device__ __forceinline__ bool expand_one(WT& W, const RangeArgs& A, const uint4* __restrict__ T, u32 lane, u32 k,
                                            u32 k9, const unsigned long long* s_p3, const u32* s_win, u32 head,
                                            u32& tail, bool& exhausted, u32& w_thr_st, u32& w_req, u64& w_gate,
@@ -227,30 +227,30 @@ __device__ __forceinline__ bool expand_one(WT& W, const RangeArgs& A, const uint
             V3 += q2 * p1 + (u32)(ee >> 32);
           }
           s0 = k;
-          if (WIN && !NEG) {
-            // 8 more steps at once when they can neither descend nor reach the
-            // excursion threshold: x = T^k(n) = a 2^8 + r gives T^i(x) = a 2^(8-i) 3^f_i +
-            // T^i(r) for i <= 8, so a g(r) <= T^i(x) < (a + 1) h(r) (g, h: the least and
-            // largest 2^(8-i) 3^f_i); bit lengths test both bounds
+          if (JW && !NEG) {
+            // JW more steps at once when they can neither descend nor reach the
+            // excursion threshold: x = T^k(n) = a 2^JW + r gives T^i(x) = a 2^(JW-i) 3^f_i +
+            // T^i(r) for i <= JW, so a g(r) <= T^i(x) < (a + 1) h(r) (g, h: the least and
+            // largest 2^(JW-i) 3^f_i); bit lengths test both bounds
             const u32 x0 = V0 - 1, x1 = V1 - (V0 == 0), x2 = V2 - ((V0 | V1) == 0), x3 = V3 - ((V0 | V1 | V2) == 0);
-            const u32 e8 = s_win[x0 & 255u];
+            const u32 te = s_win[x0 & ((1u << JW) - 1u)];
             const u32 xb = x3 ? 128u - __clz(x3) : (x2 ? 96u - __clz(x2) : (x1 ? 64u - __clz(x1) : 32u - __clz(x0)));
-            const u32 glen = (e8 >> 20) & 31u, hlen = (e8 >> 25) & 31u;
-            if ((xb + glen >= nbl + 10u) & (xb + hlen < w_thr_bl + 8u) & (xb <= 100u)) {
+            const u32 glen = (te >> 22) & 31u, hlen = te >> 27;
+            if ((xb + glen >= nbl + (u32)JW + 2u) & (xb + hlen < w_thr_bl + (u32)JW) & (xb <= 100u)) {
               u32 y0 = x0, y1 = x1, y2 = x2, y3 = x3;
-              odd_run4(y0, y1, y2, y3, 8u, (u32)s_p3[(e8 >> 16) & 15u]);  // (x >> 8) 3^f_8
-              // + T^8(r) + 1 (back to v space)
+              odd_run4(y0, y1, y2, y3, (u32)JW, (u32)s_p3[(te >> 18) & 15u]);  // (x >> JW) 3^f_JW
+              // + T^JW(r) + 1 (back to v space)
               asm("add.cc.u32 %0, %0, %4;\n\t"
                   "addc.cc.u32 %1, %1, 0;\n\t"
                   "addc.cc.u32 %2, %2, 0;\n\t"
                   "addc.u32 %3, %3, 0;"
                   : "+r"(y0), "+r"(y1), "+r"(y2), "+r"(y3)
-                  : "r"((e8 & 0xFFFFu) + 1u));
+                  : "r"((te & 0x3FFFFu) + 1u));
               V0 = y0;
               V1 = y1;
               V2 = y2;
               V3 = y3;
-              s0 = k + 8u;
+              s0 = k + (u32)JW;
               if (STATS) X.c_win++;
             }
           }
@@ -356,7 +356,7 @@ __device__ __noinline__ u32 drop_dominated(RangeWarp& W, u32 lane, u32 pend, u32
   return pend;
 }
 
-template <int R, int MINB, bool STATS = false, bool NEG = false, bool WIN = false, bool N64 = false, int M = 0>
+template <int R, int MINB, bool STATS = false, bool NEG = false, int JW = 0, bool N64 = false, int M = 0>
 __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) {
   // diagnostics (STATS variant only): run pairs, excursion slow paths, replays, jumps, pops,
   // expansions, passes, offers; clock64 cycles per phase (lane 0)
@@ -367,25 +367,8 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
   RangeWarp* S = reinterpret_cast<RangeWarp*>(range_smem);
   __shared__ unsigned long long s_p3[41];
   __shared__ u32 s_pow3[9], s_keep9[9];
-  __shared__ u32 s_win[WIN ? 256 : 1];  // per r < 2^8: T^8(r) | f_8 << 16 | bitlen(g) << 20 | bitlen(h) << 25
-  if (WIN) {
-    for (u32 r = threadIdx.x; r < 256u; r += blockDim.x) {
-      u32 x = r, f = 0, g = 0xFFFFFFFFu, h = 0;
-      for (u32 i = 1; i <= 8u; i++) {
-        if (x & 1u) {
-          x = (3u * x + 1u) >> 1;
-          f++;
-        } else {
-          x >>= 1;
-        }
-        u32 t = 1u << (8u - i);
-        for (u32 j = 0; j < f; j++) t *= 3u;
-        g = min(g, t);
-        h = max(h, t);
-      }
-      s_win[r] = x | (f << 16) | ((32u - __clz(g)) << 20) | ((32u - __clz(h)) << 25);
-    }
-  }
+  __shared__ u32 s_win[JW ? (1u << JW) : 1];  // the JW-step table (build_step_table)
+  if (JW) build_step_table(s_win, (u32)JW);
   const u32 lane = lane_id();
   RangeWarp& W = S[threadIdx.x >> 5];
   if (threadIdx.x < 41) {
@@ -540,7 +523,7 @@ __global__ void __launch_bounds__(RWARPS * 32, MINB) k_range(const RangeArgs A) 
     }
     // ---- refill: keep 32 R seeds queued (each lane pops at most R per pass) ----
     while (tail - head < 32u * R && !exhausted) {
-      if (!expand_one<STATS, NEG, WIN, M>(W, A, T, lane, k, k9, s_p3, s_win, head, tail, exhausted, w_thr_st, w_req,
+      if (!expand_one<STATS, NEG, JW, M>(W, A, T, lane, k, k9, s_p3, s_win, head, tail, exhausted, w_thr_st, w_req,
                                        w_gate, X))
         break;
     }
@@ -907,17 +890,18 @@ int range_variants() { return 8; }
 constexpr size_t RANGE_SMEM = sizeof(RangeWarp) * RWARPS;
 
 cudaError_t launch_range_stats(const RangeArgs& a, u32 grid, cudaStream_t st) {
-  k_range<2, 3, true, false, true, false, 3><<<grid, RWARPS * 32, RANGE_SMEM, st>>>(a);
+  k_range<2, 3, true, false, 8, false, 3><<<grid, RWARPS * 32, RANGE_SMEM, st>>>(a);
   return cudaGetLastError();
 }
 
-// (run pairs per pass, minimum resident blocks per SM, 8-step window after the k-step jump,
-// 64-bit body while the warp's values are below 2^59, run pairs per seed taken at expansion)
-// Measured on B200, 2^36 seeds at 2^60 + 3 2^34 with k = 34: 8.20 ms (variant 0), 8.49 (1),
-// 10.15 (2), 8.82 (3), 9.63 (4: the window alone), 8.9-9.2 (5, 6), 8.30 (7).
+// (run pairs per pass, minimum resident blocks per SM, length JW of the jump-table window
+// after the k-step jump (0: none), 64-bit body while the warp's values are below 2^59, run
+// pairs per seed taken at expansion).  Measured on B200, 2^36 seeds at 2^60 + 3 2^34 with
+// k = 34: 8.19 ms (variant 0), 8.43 (1), 10.13 (2), 9.08 (3), 9.63 (4), 9.07 (5), 8.63 (6),
+// 9.26 (7); a table of 2^10 or 2^11 entries costs this kernel a resident block per SM.
 #define CZ_RANGE_VARIANTS(X)                                                                   \
-  X(0, 2, 4, 1, 0, 3) X(1, 2, 4, 1, 0, 4) X(2, 2, 4, 0, 0, 0) X(3, 2, 4, 1, 0, 5) X(4, 2, 4, 1, 0, 0) \
-  X(5, 2, 3, 1, 0, 3) X(6, 2, 4, 1, 1, 3) X(7, 1, 4, 1, 0, 3)
+  X(0, 2, 4, 8, 0, 3) X(1, 2, 4, 8, 0, 4) X(2, 2, 4, 0, 0, 0) X(3, 2, 4, 11, 0, 3) X(4, 2, 4, 8, 0, 0) \
+  X(5, 2, 4, 10, 0, 3) X(6, 2, 4, 8, 1, 3) X(7, 2, 4, 11, 0, 4)
 
 cudaError_t launch_range(const RangeArgs& a, int variant, u32 grid, cudaStream_t st) {
   switch (variant) {
@@ -960,7 +944,7 @@ cudaError_t range_init() {
   CZ_RANGE_VARIANTS(X)
 #undef X
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_range<2, 3, true, false, true, false, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_range<2, 3, true, false, 8, false, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)RANGE_SMEM);
   return e;
 }

@@ -55,29 +55,6 @@ __device__ __forceinline__ u64 gate64_of(u64 window) { return (window >> 32) ? ~
 
 __device__ __forceinline__ u32 bitlen64(u64 x) { return x ? 64u - __clzll(x) : 0u; }
 
-// Table of J steps for residues r < 2^J (J <= 11): T^J(r) [17:0] | f_J [21:18]
-// | bitlen(g) [26:22] | bitlen(h) [31:27], g and h the least and largest of
-// 2^(J-i) 3^(f_i) over 1 <= i <= J.  For x = a 2^J + r, T^i(x) = a 2^(J-i) 3^(f_i)
-// + T^i(r) with 0 <= T^i(r) < 2^(J-i) 3^(f_i), so a g <= T^i(x) < (a + 1) h.
-__device__ __forceinline__ void build_step_table(u32* t, u32 J) {
-  for (u32 r = threadIdx.x; r < (1u << J); r += blockDim.x) {
-    u32 x = r, f = 0, g = 0xFFFFFFFFu, h = 0;
-    for (u32 i = 1; i <= J; i++) {
-      if (x & 1u) {
-        x = x + (x >> 1) + 1u;  // (3x + 1) / 2
-        f++;
-      } else {
-        x >>= 1;
-      }
-      u32 m = 1u << (J - i);
-      for (u32 j = 0; j < f; j++) m *= 3u;
-      g = min(g, m);
-      h = max(h, m);
-    }
-    t[r] = x | (f << 18) | ((32u - __clz(g)) << 22) | ((32u - __clz(h)) << 27);
-  }
-}
-
 // Drops pending offers that another pending lane of the same request beats
 // (larger, or equal with a smaller seed), so that one offer per request and
 // kind remains; all lanes call it together.
