@@ -140,43 +140,6 @@ __device__ __forceinline__ bool first_pairs(u64& v, u32& st, u64 n, u64 G, u32 t
   return true;
 }
 
-// Up to M run pairs of two seeds per lane taken at expansion, side by side
-// (the same rules as first_pairs, which takes one seed).  live[j]: seed j may
-// still take pairs; done[j] becomes true when seed j finished here.  Every
-// lane of the warp calls this.
-template <int M, bool STATS>
-__device__ __forceinline__ void pairs_side_by_side(u64* v, u32* st, const u64* n, bool* live, bool* done, u64 G,
-                                                   u32 thr_st, const u32* s_pow3, Stats64& X) {
-#pragma unroll
-  for (int m = 0; m < M; m++) {
-    if (!__any_sync(FULL, live[0] | live[1])) break;
-#pragma unroll
-    for (int j = 0; j < 2; j++) {
-      if (live[j]) {
-        const u32 a = ctz32((u32)v[j] | 0x80u);
-        const u64 x = (v[j] >> a) * s_pow3[a] - 1;
-        if (x + 1 >= G) {  // an excursion candidate: the loop takes this pair
-          live[j] = false;
-        } else {
-          const u32 b = ctz32((u32)x | 0x80000000u);
-          const u64 w = x >> b;
-          const u32 st2 = st[j] + a + b;
-          if (w < n[j]) {  // descends in this pair (b = 0 leaves x, which is above n)
-            live[j] = false;
-            done[j] = st2 < thr_st;  // else sigma may reach the maximum: the loop takes it
-            if (STATS) X.xfin += done[j];
-          } else {
-            v[j] = w + 1;
-            st[j] = st2;
-            live[j] = v[j] < FAST_LIMIT;
-            if (STATS) X.xpairs++;
-          }
-        }
-      }
-    }
-  }
-}
-
 // Expands the staged item into the warp's queue from position tail (see
 // expand_one in range.cu for the rules; this is its 64-bit form).  Seeds are
 // below 2^52, so the block q is below 2^(52-k) and n = q 2^k + r is one
@@ -255,16 +218,12 @@ __device__ __forceinline__ bool expand64(Warp64& W, const RangeArgs& A, const ui
       for (u32 j = 0; j < RANGE_ITEM / 32; j++)
         if (it.sbase + j * 32 + lane < it.send) mask |= 1u << j;
     }
-    // both entries' start states (the k-step jump, up to C windows of JW steps), then up to
-    // M run pairs for the two seeds side by side (two independent chains per lane), then one
-    // ballot per entry places the lanes' seeds in the queue
+    // each entry in turn: its seed's start state (the k-step jump, up to C windows of JW
+    // steps, up to M run pairs), then one ballot places the lanes' seeds in the queue
     seeds = __reduce_add_sync(FULL, __popc(mask));
     total = 0;
-    u64 vs[2], ns[2];
-    u32 ss[2];
-    bool live[2], done[2];
 #pragma unroll
-    for (u32 j = 0; j < 2; j++) {
+    for (u32 j = 0; j < RANGE_ITEM / 32; j++) {
       const u32 f = (e[j].y >> 8) & 0xFFu, emax = e[j].y >> 24;
       const u64 n = qk | e[j].x | ((u64)(e[j].y & 0xFFu) << 32);
       u64 v = n + 1;
@@ -283,22 +242,12 @@ __device__ __forceinline__ bool expand64(Warp64& W, const RangeArgs& A, const ui
         }
       }
       if (STATS && ((mask >> j) & 1u) && st == 0) X.replay++;
-      vs[j] = v;
-      ns[j] = n;
-      ss[j] = st;
-      live[j] = ((mask >> j) & 1u) && v < FAST_LIMIT;
-      done[j] = false;
-    }
-    pairs_side_by_side<M, STATS>(vs, ss, ns, live, done, G, w_thr_st, s_pow3, X);
-#pragma unroll
-    for (u32 j = 0; j < 2; j++) {
-      const bool keep = ((mask >> j) & 1u) && !done[j];
+      const bool keep = ((mask >> j) & 1u) && first_pairs<M, STATS>(v, st, n, G, w_thr_st, s_pow3, X);
       const u32 bk = __ballot_sync(FULL, keep);
       if (keep) {
-        const u32 cand = vs[j] >= G ? 1u : 0u;
+        const u32 cand = v >= G ? 1u : 0u;
         W.q[(tail + total + __popc(bk & lanemask_lt())) & (Q64 - 1)] =
-            make_uint4((u32)vs[j], (u32)(vs[j] >> 32), (u32)ns[j],
-                       (u32)(ns[j] >> 32) | (slot << 16) | (cand << 21) | (ss[j] << 22));
+            make_uint4((u32)v, (u32)(v >> 32), (u32)n, (u32)(n >> 32) | (slot << 16) | (cand << 21) | (st << 22));
       }
       total += __popc(bk);
     }
