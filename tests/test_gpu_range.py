@@ -293,3 +293,27 @@ def test_narrow_variant_equals_plain(verifier, off, size, k):
     assert (w.seeds_checked, w.failures, w.widened, w.errors) == (p.seeds_checked, p.failures, p.widened, p.errors)
     assert (w.max_stopping_time, w.max_stopping_time_seed) == (p.max_stopping_time, p.max_stopping_time_seed)
     assert (w.max_excursion, w.max_excursion_seed) == (p.max_excursion, p.max_excursion_seed)
+
+
+@pytest.mark.parametrize("width", [0, 48])
+def test_range_edges_both_kernels(verifier, width):
+    """Empty and one-seed ranges, a range of the smallest kept seeds, and a range
+    straddling 2^48 (its launch has 49-bit seeds, so it runs four limbs even
+    with the 64-bit kernel enabled) give the oracle's results with the limb
+    width at 0 (four limbs only) and at 48."""
+    import collatz_b200 as cb
+    from oracle import oracle as O
+    v = verifier(26)
+    v.set_variant(cb.MODE_RANGE64_BITS, width)
+    try:
+        for off, size, k in [(1 << 40, 0, 24), ((1 << 40) + 27, 1, 24), ((1 << 40) + 28, 1, 24), (2, 1, 16),
+                             (0, 10, 16), ((1 << 48) - (1 << 20), 1 << 21, 24)]:
+            g = v.verify_range(off, size, k)
+            o = O.range_verify(off, size, k, True, method=1, nthreads=NT)
+            assert g.errors == 0 and g.failures == 0
+            assert g.seeds_checked == o.seeds, (off, size)
+            if o.seeds:
+                assert (g.max_stopping_time, g.max_stopping_time_seed) == (o.max_st, o.max_st_seed)
+                assert (g.max_excursion, g.max_excursion_seed) == (o.max_exc, o.max_exc_seed)
+    finally:
+        v.set_variant(cb.MODE_RANGE64_BITS, cb.RANGE64_BITS_DEFAULT)
