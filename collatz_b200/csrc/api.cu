@@ -1141,15 +1141,18 @@ static RangeArgs range_args(collatz_ctx* c, const RangeTables& T, uint32_t k, bo
 }
 
 cudaError_t cz::range_kernel_launch(collatz_ctx* c, const RangeArgs& a, bool stats, cudaStream_t s) {
-  int bps = 0;
   if (!a.negative && a.seed_bits && a.seed_bits <= std::min(c->range64_bits, range64_max_seed_bits())) {
-    if (range64_occupancy(c->range64_variant, &bps) != cudaSuccess || bps <= 0) bps = 1;
+    const int v = c->range64_variant;
+    int& bps = c->occ_range64[v & 7];
+    if (bps <= 0 && (range64_occupancy(v, &bps) != cudaSuccess || bps <= 0)) bps = 1;
     const uint32_t grid = (uint32_t)(bps * c->sm_count);
-    return stats ? launch_range64_stats(a, c->range64_variant, grid, s)
-                 : launch_range64(a, c->range64_variant, grid, s);
+    return stats ? launch_range64_stats(a, v, grid, s) : launch_range64(a, v, grid, s);
   }
-  const uint32_t grid = (uint32_t)grid_for(c, 1, c->range_variant);
-  return (stats && !a.negative) ? launch_range_stats(a, grid, s) : launch_range(a, c->range_variant, grid, s);
+  const int v = c->range_variant;
+  int& bps = c->occ_range[v & 7];
+  if (bps <= 0 && (range_occupancy(v, &bps) != cudaSuccess || bps <= 0)) bps = 1;
+  const uint32_t grid = (uint32_t)(bps * c->sm_count);
+  return (stats && !a.negative) ? launch_range_stats(a, grid, s) : launch_range(a, v, grid, s);
 }
 
 // One range launch on stream s: record and counter reset, k_range, the

@@ -117,6 +117,8 @@ struct collatz_ctx {
   // all have at most range64_bits bits run it, the others run the four-limb kernel
   int range64_variant = 0;
   uint32_t range64_bits = 48;
+  // resident blocks per SM of each range-kernel variant (0: not asked yet)
+  int occ_range[8] = {}, occ_range64[8] = {};
   uint32_t iter_cap = 1u << 16;
   // scratch for the synchronous calls
   cz::DevBuf d_rec, d_counter, d_overflow, d_ovcount, d_pairs[2], d_segs, d_widen, d_widen2, d_wcount;

@@ -9,7 +9,9 @@
 //                    that need less than an equal share take what they need,
 //                    the rest of the slice budget goes to the larger ones),
 //                    followed by the 192- and 256-bit widening passes and a
-//                    copy of the request records.  Two slices are kept in
+//                    copy of the request records; a prologue kernel zeroes the
+//                    slice's counters and the records of newly admitted
+//                    requests.  Two slices are kept in
 //                    flight, so the next one is queued behind the running one
 //                    and the device does not wait for the host.  A request's
 //                    record lives in one device slot for its whole life, so
@@ -17,12 +19,12 @@
 //                    in a single launch.
 //   query thread  -- trajectory batches (higher-priority stream).  Admitted
 //                    queries are concatenated into one batch: seeds are sorted
-//                    by bit length into limb classes on the host, and the chain
-//                    of class kernels hands seeds that need wider values to the
-//                    next class on the device (the counts stay on the device).
-//                    Two batches are kept in flight.  The host copies of a
-//                    batch (gathering seeds, scattering results into the
-//                    callers' buffers) run on this thread, off the range path.
+//                    by bit length into limb classes on the host, and one
+//                    launch serves every class (a seed that needs wider values
+//                    is run again by its thread).  Two batches are kept in
+//                    flight.  The host copies of a batch (gathering seeds,
+//                    scattering results into the callers' buffers) run on this
+//                    thread and a small pool of helpers, off the range path.
 // Admission (arrival order within each kind) needs a free request slot and
 // free device memory: cudaMemGetInfo's free bytes plus this server's idle
 // pool memory, minus the bytes promised to admitted queries that have not
@@ -91,8 +93,21 @@ struct Slice {
   bool busy = false;
 };
 
+// Byte layout of a trajectory batch of n seeds in its device block:
+//   [0, 32n) seeds (8 words each) | [32n, 36n) class lists | o_cnt: 16 cursor
+//   words | o_out: stopping times (8n), excursions (64n), statuses (4n).
+struct BatchLayout {
+  uint64_t o_idx, o_cnt, in_bytes, o_out, r_st, r_exc, r_status, out_bytes;
+  explicit BatchLayout(uint64_t n)
+      : o_idx(32 * n), o_cnt((36 * n + 255) & ~255ull), in_bytes(o_cnt + 64), o_out(o_cnt + 256),
+        r_st(0), r_exc(8 * n), r_status(72 * n), out_bytes(76 * n) {}
+};
+
 struct Batch {
-  HostBuf h_seeds, h_idx, h_cnt, h_st, h_exc, h_status;
+  // h_in mirrors the input part of the batch's device block (seeds, class
+  // lists, cursors) and h_out its output part (stopping times, excursions,
+  // statuses), so that each direction is one copy
+  HostBuf h_in, h_out;
   std::vector<Req*> reqs;
   std::vector<uint8_t> cls;
   uint32_t n = 0;
@@ -101,6 +116,22 @@ struct Batch {
 };
 
 double since(Clock::time_point t0) { return std::chrono::duration<double>(Clock::now() - t0).count(); }
+
+// A slice's prologue: zeroes its item cursor and widen counters and the
+// records of the requests admitted since the previous slice (one launch in
+// place of a memset per request).
+__global__ void k_slice_prologue(unsigned long long* cursor, uint32_t* wcount, ReqRec* recs, const uint32_t* slots,
+                                 uint32_t nslots) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0) {
+    *cursor = 0;
+    wcount[0] = 0;
+    wcount[1] = 0;
+  }
+  constexpr uint32_t W = sizeof(ReqRec) / 8;  // 17 words of 8 bytes
+  for (uint32_t i = t; i < nslots * W; i += gridDim.x * blockDim.x)
+    reinterpret_cast<unsigned long long*>(recs + slots[i / W])[i % W] = 0ull;
+}
 
 // A fixed set of host threads for the query path's copies (gathering query
 // seeds into the pinned batch, scattering results into the callers'
@@ -204,6 +235,7 @@ struct collatz_server {
   // range thread only
   std::vector<Req*> ranges;  // admitted range requests not yet complete
   std::vector<uint32_t> free_slots;
+  std::vector<uint32_t> fresh_slots;  // records of admitted requests, zeroed by the next slice's prologue
   DevBuf d_recs;
   Slice slices[SLICE_DEPTH];
   std::deque<int> slice_order;
@@ -325,15 +357,11 @@ void admit_ranges(collatz_server* s) {
       publish(s, r, rc);
       continue;
     }
+    // the record is zeroed by the prologue of the next slice, which runs before any slice
+    // that holds this request (slices run in order on one stream)
     r->slot = s->free_slots.back();
-    cudaError_t e = cudaMemsetAsync(s->d_recs.as<ReqRec>() + r->slot, 0, sizeof(ReqRec), s->sa);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      s->active[0]--;
-      publish(s, r, COLLATZ_E_CUDA);
-      continue;
-    }
     s->free_slots.pop_back();
+    s->fresh_slots.push_back(r->slot);
     s->ranges.push_back(r);
   }
 }
@@ -403,13 +431,18 @@ int launch_slice(collatz_server* s, int si) {
   int rc = get_range_tables(c, k, &T, neg);
   if (rc) return rc;
   const size_t sb = sizeof(RangeSeg) * segs.size(), fb = sizeof(uint32_t) * scouts.size();
+  const size_t zb = sizeof(uint32_t) * s->fresh_slots.size();
   const size_t rb = sizeof(ReqRec) * s->cfg.max_active;
-  cudaError_t e = S.d_segs.ensure(sb + fb);  // the segments, then the scouts' segment indices
-  if (!e) e = S.h_segs.ensure(sb + fb);
+  // one upload: the segments, the scouts' segment indices, the records to zero
+  cudaError_t e = S.d_segs.ensure(sb + fb + zb);
+  if (!e) e = S.h_segs.ensure(sb + fb + zb);
   if (!e) e = S.h_recs.ensure(rb);
   if (e) return set_cuda_error(c, e, "server slice buffers");
   std::memcpy(S.h_segs.p, segs.data(), sb);
   if (fb) std::memcpy(static_cast<char*>(S.h_segs.p) + sb, scouts.data(), fb);
+  if (zb) std::memcpy(static_cast<char*>(S.h_segs.p) + sb + fb, s->fresh_slots.data(), zb);
+  const uint32_t nfresh = (uint32_t)s->fresh_slots.size();
+  s->fresh_slots.clear();
   RangeArgs a;
   a.table = T->dev.table;
   a.k = k;
@@ -426,11 +459,16 @@ int launch_slice(collatz_server* s, int si) {
   a.negative = neg ? 1u : 0u;
   a.seed_bits = seed_bits;
   cudaStream_t st = s->sa;
-  e = cudaMemcpyAsync(S.d_segs.p, S.h_segs.p, sb + fb, cudaMemcpyHostToDevice, st);
-  if (!e) e = cudaMemsetAsync(S.d_cursor.p, 0, sizeof(unsigned long long), st);
-  if (!e) e = cudaMemsetAsync(S.d_wcount.p, 0, 2 * sizeof(uint32_t), st);
+  e = cudaMemcpyAsync(S.d_segs.p, S.h_segs.p, sb + fb + zb, cudaMemcpyHostToDevice, st);
+  if (!e) {
+    const uint32_t words = nfresh * (uint32_t)(sizeof(ReqRec) / 8);
+    k_slice_prologue<<<std::max(1u, std::min(64u, (words + 255) / 256)), 256, 0, st>>>(
+        S.d_cursor.as<unsigned long long>(), S.d_wcount.as<uint32_t>(), s->d_recs.as<ReqRec>(),
+        reinterpret_cast<const uint32_t*>(static_cast<const char*>(S.d_segs.p) + sb + fb), nfresh);
+    e = cudaGetLastError();
+  }
   if (!e) e = cudaEventRecord(S.t0, st);
-  // threshold scouts for the requests that start here (their records were zeroed at admission)
+  // threshold scouts for the requests that start here (their records were zeroed by the prologue)
   if (!e && fb)
     e = launch_range_scout(a, reinterpret_cast<const uint32_t*>(static_cast<const char*>(S.d_segs.p) + sb),
                            (uint32_t)scouts.size(), st);
@@ -480,7 +518,7 @@ void admit_queries(collatz_server* s) {
   for (;;) {
     Req* r = front(s, s->pend_query, TRAJ_BYTES_PER_SEED);
     if (!r) return;
-    const uint64_t need = TRAJ_BYTES_PER_SEED * r->q.nseeds + 256;
+    const uint64_t need = TRAJ_BYTES_PER_SEED * r->q.nseeds + 768;  // covers BatchLayout's padding
     if (!take_active(s, 1)) return;
     if (!take_budget(s, need)) {
       s->active[1]--;
@@ -560,22 +598,16 @@ int launch_batch(collatz_server* s, int bi) {
   B.n = (uint32_t)n;
   // host: seeds into pinned memory, class lists (region j holds class j's
   // own seeds followed by room for every seed of the narrower classes)
-  cudaError_t e = B.h_seeds.ensure(32 * n);
-  if (!e) e = B.h_idx.ensure(4 * n);
-  if (!e) e = B.h_cnt.ensure(64);
-  if (!e) e = B.h_st.ensure(8 * n);
-  if (!e) e = B.h_exc.ensure(64 * n);
-  if (!e) e = B.h_status.ensure(4 * n);
+  const BatchLayout L(n);
+  cudaError_t e = B.h_in.ensure(L.in_bytes);
+  if (!e) e = B.h_out.ensure(L.out_bytes);
   if (e) return set_cuda_error(c, e, "server batch buffers");
-  uint32_t* hs = B.h_seeds.as<uint32_t>();
-  uint32_t* hi = B.h_idx.as<uint32_t>();
+  char* h = B.h_in.as<char>();
   TrajAllArgs a;
-  gather_batch(s, B, hs, hi, a.cstart);
-  uint32_t* hc = B.h_cnt.as<uint32_t>();
-  for (int j = 0; j < 16; j++) hc[j] = 0;
+  gather_batch(s, B, reinterpret_cast<uint32_t*>(h), reinterpret_cast<uint32_t*>(h + L.o_idx), a.cstart);
+  std::memset(h + L.o_cnt, 0, 64);
   // device: one block from the server's pool, freed in stream order
-  const uint64_t o_st = 32 * n, o_exc = o_st + 8 * n, o_status = o_exc + 64 * n, o_idx = o_status + 4 * n,
-                 o_cnt = (o_idx + 4 * n + 255) & ~255ull, bytes = o_cnt + 64;
+  const uint64_t bytes = L.o_out + L.out_bytes;
   cudaStream_t st = s->sb;
   void* block = nullptr;
   e = cudaMallocFromPoolAsync(&block, bytes, s->pool, st);
@@ -587,24 +619,20 @@ int launch_batch(collatz_server* s, int bi) {
     s->promised -= std::min(s->promised, promised);
   }
   char* d = static_cast<char*>(block);
-  e = cudaMemcpyAsync(d, hs, 32 * n, cudaMemcpyHostToDevice, st);
-  if (!e) e = cudaMemcpyAsync(d + o_idx, hi, 4 * n, cudaMemcpyHostToDevice, st);
-  if (!e) e = cudaMemcpyAsync(d + o_cnt, hc, 64, cudaMemcpyHostToDevice, st);
+  e = cudaMemcpyAsync(d, h, L.in_bytes, cudaMemcpyHostToDevice, st);
   if (!e) {
     // every limb class in one launch: a seed that needs more limbs is re-run by its thread
     a.seeds = reinterpret_cast<const uint32_t*>(d);
-    a.index = reinterpret_cast<const uint32_t*>(d + o_idx);
-    a.st = reinterpret_cast<unsigned long long*>(d + o_st);
-    a.exc = reinterpret_cast<uint32_t*>(d + o_exc);
-    a.status = reinterpret_cast<uint32_t*>(d + o_status);
-    a.cursor = reinterpret_cast<uint32_t*>(d + o_cnt);
+    a.index = reinterpret_cast<const uint32_t*>(d + L.o_idx);
+    a.st = reinterpret_cast<unsigned long long*>(d + L.o_out + L.r_st);
+    a.exc = reinterpret_cast<uint32_t*>(d + L.o_out + L.r_exc);
+    a.status = reinterpret_cast<uint32_t*>(d + L.o_out + L.r_status);
+    a.cursor = reinterpret_cast<uint32_t*>(d + L.o_cnt);
     a.iter_cap = c->iter_cap;
     const uint32_t grid = (uint32_t)std::min<uint64_t>((n + 127) / 128, (uint64_t)c->sm_count * 8);
     e = launch_traj_all(a, grid, st);
   }
-  if (!e) e = cudaMemcpyAsync(B.h_st.p, d + o_st, 8 * n, cudaMemcpyDeviceToHost, st);
-  if (!e) e = cudaMemcpyAsync(B.h_exc.p, d + o_exc, 64 * n, cudaMemcpyDeviceToHost, st);
-  if (!e) e = cudaMemcpyAsync(B.h_status.p, d + o_status, 4 * n, cudaMemcpyDeviceToHost, st);
+  if (!e) e = cudaMemcpyAsync(B.h_out.p, d + L.o_out, L.out_bytes, cudaMemcpyDeviceToHost, st);
   const cudaError_t ef = cudaFreeAsync(block, st);
   if (!e) e = ef;
   if (!e) e = cudaEventRecord(B.done, st);
@@ -620,14 +648,19 @@ void complete_batch(collatz_server* s, int bi) {
   Batch& B = s->batches[bi];
   // results into the callers' buffers, in parts on the copy pool for large batches
   const uint64_t n = B.n;
+  const BatchLayout L(n);
+  const char* h = B.h_out.as<char>();
+  const uint64_t* h_st = reinterpret_cast<const uint64_t*>(h + L.r_st);
+  const uint32_t* h_exc = reinterpret_cast<const uint32_t*>(h + L.r_exc);
+  const uint32_t* h_status = reinterpret_cast<const uint32_t*>(h + L.r_status);
   const int parts = (int)std::max<uint64_t>(1, std::min<uint64_t>((n + COPY_PART_SEEDS - 1) / COPY_PART_SEEDS, 64));
   s->copy_pool.run(parts, [&](int p) {
     for_range(B, n * (uint64_t)p / (uint64_t)parts, n * (uint64_t)(p + 1) / (uint64_t)parts,
               [&](Req* r, uint64_t first, uint64_t m) {
                 const uint64_t o = r->batch_off + first;
-                std::memcpy(r->q.stopping_time + first, B.h_st.as<uint64_t>() + o, 8 * m);
-                std::memcpy(r->q.excursion + 16 * first, B.h_exc.as<uint32_t>() + 16 * o, 64 * m);
-                std::memcpy(r->q.status + first, B.h_status.as<uint32_t>() + o, 4 * m);
+                std::memcpy(r->q.stopping_time + first, h_st + o, 8 * m);
+                std::memcpy(r->q.excursion + 16 * first, h_exc + 16 * o, 64 * m);
+                std::memcpy(r->q.status + first, h_status + o, 4 * m);
               });
   });
   for (Req* r : B.reqs) {
@@ -797,12 +830,8 @@ void destroy(collatz_server* s) {
       if (S.done) cudaEventDestroy(S.done);
     }
     for (Batch& B : s->batches) {
-      B.h_seeds.release();
-      B.h_idx.release();
-      B.h_cnt.release();
-      B.h_st.release();
-      B.h_exc.release();
-      B.h_status.release();
+      B.h_in.release();
+      B.h_out.release();
       if (B.done) cudaEventDestroy(B.done);
     }
     s->d_recs.release();
@@ -884,12 +913,8 @@ extern "C" int collatz_server_start(const collatz_config* cfg, const collatz_ser
   const uint64_t nb = s->cfg.traj_batch_seeds;
   for (Batch& B : s->batches) {
     if ((e = cudaEventCreateWithFlags(&B.done, cudaEventDisableTiming))) return fail(e, "event");
-    if ((e = B.h_seeds.ensure(32 * nb))) return fail(e, "batch");
-    if ((e = B.h_idx.ensure(4 * nb))) return fail(e, "batch");
-    if ((e = B.h_cnt.ensure(64))) return fail(e, "batch");
-    if ((e = B.h_st.ensure(8 * nb))) return fail(e, "batch");
-    if ((e = B.h_exc.ensure(64 * nb))) return fail(e, "batch");
-    if ((e = B.h_status.ensure(4 * nb))) return fail(e, "batch");
+    if ((e = B.h_in.ensure(BatchLayout(nb).in_bytes))) return fail(e, "batch");
+    if ((e = B.h_out.ensure(BatchLayout(nb).out_bytes))) return fail(e, "batch");
     B.cls.reserve(nb);
   }
   size_t fr = 0;
