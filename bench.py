@@ -372,7 +372,7 @@ def run_reference_gpu_program(reps: int = 3) -> dict:
 
 
 def run_served(v, capacity: float, load: float = 0.7, duration: float = 1.0, seed: int = 5,
-               slice_items: int = 1 << 19, plain_sample: int = 600) -> dict:
+               slice_items: int = 1 << 19, plain_sample: int = 600, trace: str | None = None) -> dict:
     """Served configuration: Poisson arrivals at `load` x capacity (range seeds
     per second), 70 % range verifications (sizes log-uniform 2^16..2^32,
     offsets uniform [2^40, 2^64), unaligned) and 30 % trajectory queries
@@ -431,6 +431,11 @@ def run_served(v, capacity: float, load: float = 0.7, duration: float = 1.0, see
         tickets[i] = srv.submit_range(*arg) if kind == "range" else srv.submit_trajectory_array(arg)
     wt.join()
     wall = max(r.done_s for r in resps) - min(r.submit_s for r in resps)
+    if trace:  # per request: kind (0 range, 1 query), seeds, planned arrival, submit, admit, done (s)
+        s0 = resps[0].submit_s
+        np.save(trace, np.array([(0 if k == "range" else 1, a[1] if k == "range" else len(a), arrivals[i],
+                                  r.submit_s - s0, r.admit_s - s0, r.done_s - s0)
+                                 for i, ((k, a), r) in enumerate(zip(reqs, resps))], dtype=np.float64))
     info = srv.info()
     srv.stop()
     lat = np.array([r.latency_s for r in resps]) * 1e3
@@ -445,11 +450,16 @@ def run_served(v, capacity: float, load: float = 0.7, duration: float = 1.0, see
     sub = [reqs[i] for i in pick]
     t1 = time.perf_counter()
     exact = True
+    t_kind = {"range": 0.0, "traj": 0.0}
     for (kind, arg), r in zip(sub, [resps[i] for i in pick]):
+        tk = time.perf_counter()
         if kind == "range":
-            exact &= _range_key(v.verify_range(*arg)) == _range_key(r.range)
+            got = v.verify_range(*arg)
+            t_kind[kind] += time.perf_counter() - tk
+            exact &= _range_key(got) == _range_key(r.range)
         else:
             status, st, exc = v.trajectory_array(arg)
+            t_kind[kind] += time.perf_counter() - tk
             exact &= bool((status == r.traj_status).all() and (st == r.traj_stopping_time).all()
                           and (exc == r.traj_excursion).all())
     t_plain = time.perf_counter() - t1
@@ -471,6 +481,7 @@ def run_served(v, capacity: float, load: float = 0.7, duration: float = 1.0, see
             "plain_seeds_per_s_same_stream": sub_seeds / t_plain,
             "plain_sample": f"{len(sub)} requests, every {stride}th of the stream, one at a time "
                             "(verify_range / trajectory)",
+            "plain_s": {"range": t_kind["range"], "traj": t_kind["traj"], "all": t_plain},
             "host_s": {"admit": info["host_admit_s"], "build_slices": info["host_slice_s"],
                        "build_batches": info["host_batch_s"], "complete": info["host_complete_s"],
                        "idle": info["host_idle_s"], "wall": wall},

@@ -25,11 +25,14 @@
 //                    flight.  The host copies of a batch (gathering seeds,
 //                    scattering results into the callers' buffers) run on this
 //                    thread and a small pool of helpers, off the range path.
-// Admission (arrival order within each kind) needs a free request slot and
-// free device memory: cudaMemGetInfo's free bytes plus this server's idle
-// pool memory, minus the bytes promised to admitted queries that have not
-// allocated yet, minus hbm_reserve.  A query needs 128 bytes per seed; a
-// range request needs its record slot only.  A request that could not fit
+// Admission (arrival order within each kind) needs a free request slot and,
+// for a query, free device memory: cudaMemGetInfo's free bytes plus this
+// server's idle pool memory, minus the bytes promised to admitted queries
+// that have not allocated yet, minus hbm_reserve.  A budget thread re-reads
+// these every 50 ms (and when a query does not fit), so admission itself
+// makes no CUDA call: cudaMemGetInfo has taken hundreds of milliseconds under
+// load.  A query needs 128 bytes per seed; a range request needs its record
+// slot only.  A request that could not fit
 // even on an otherwise empty device is refused (COLLATZ_E_ADMISSION); one
 // that does not fit now waits.
 #include <cuda_runtime.h>
@@ -226,11 +229,14 @@ struct collatz_server {
 
   std::atomic<uint32_t> active[2] = {{0}, {0}};  // admitted, not yet complete: [0] ranges, [1] queries
 
-  // admission budget (guarded by mb)
+  // query admission budget (guarded by mb), re-read by the budget thread
   std::mutex mb;
+  std::condition_variable cv_budget;
   int64_t budget = 0;
   uint64_t promised = 0;  // admitted query bytes not yet allocated
-  Clock::time_point budget_read{};
+  uint64_t launched = 0;  // query bytes moved from promised to the pool, in total
+  bool want_budget = false, budget_stop = false;
+  std::thread thr_budget;
 
   // range thread only
   std::vector<Req*> ranges;  // admitted range requests not yet complete
@@ -260,37 +266,64 @@ void publish(collatz_server* s, Req* r, int status) {
   s->cv_done.notify_all();
 }
 
-// Re-reads the device's free memory into the admission budget (caller holds
-// mb): free bytes plus this server's idle pool memory, minus the bytes
-// promised to admitted queries that have not allocated yet, minus
-// hbm_reserve.  Between reads each admission takes its bytes from the
-// budget and frees are not credited, so the budget never over-states what is
-// free.  The read is far slower than an admission, so it happens when a
-// request does not fit (at most every millisecond) and every 100 ms.
+// Re-reads the device's free memory into the admission budget (called
+// without mb held; the CUDA calls run outside it): free bytes plus this
+// server's idle pool memory, minus the bytes promised to admitted queries
+// that have not allocated yet, minus hbm_reserve, minus the bytes that
+// reached the pool while the read ran (they may be missing from it).
+// Between reads each admission takes its bytes from the budget and frees are
+// not credited, so the budget never over-states what is free.
 void refresh_budget(collatz_server* s) {
-  size_t fr = 0, tot = 0;
-  s->budget_read = Clock::now();
-  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
-    cudaGetLastError();
-    s->budget = -1;
-    return;
+  uint64_t launched0 = 0;
+  {
+    std::lock_guard<std::mutex> g(s->mb);
+    launched0 = s->launched;
   }
+  size_t fr = 0, tot = 0;
+  const bool ok = cudaMemGetInfo(&fr, &tot) == cudaSuccess;
+  if (!ok) cudaGetLastError();
   uint64_t reserved = 0, used = 0;
   cudaMemPoolGetAttribute(s->pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
   cudaMemPoolGetAttribute(s->pool, cudaMemPoolAttrUsedMemCurrent, &used);
-  s->budget = (int64_t)fr + (int64_t)(reserved - used) - (int64_t)s->promised - (int64_t)s->cfg.hbm_reserve;
+  uint64_t promised = 0;
+  {
+    std::lock_guard<std::mutex> g(s->mb);
+    promised = s->promised;
+    s->budget = ok ? (int64_t)fr + (int64_t)(reserved - used) - (int64_t)promised -
+                         (int64_t)(s->launched - launched0) - (int64_t)s->cfg.hbm_reserve
+                   : -1;
+  }
   std::lock_guard<std::mutex> g(s->mu);
   s->info.hbm_free = fr;
-  s->info.hbm_admitted = s->promised + used;
+  s->info.hbm_admitted = promised + used;
 }
 
-// Takes need bytes from the budget if they fit.
+// Budget thread: re-reads the budget every 50 ms, or at most every
+// millisecond while a query waits for memory, and wakes the query thread.
+void budget_loop(collatz_server* s) {
+  cudaSetDevice(s->ctx->device);
+  std::unique_lock<std::mutex> g(s->mb);
+  while (!s->budget_stop) {
+    s->cv_budget.wait_for(g, std::chrono::milliseconds(50), [s] { return s->want_budget || s->budget_stop; });
+    if (s->budget_stop) break;
+    s->want_budget = false;
+    g.unlock();
+    refresh_budget(s);
+    s->cv_query.notify_one();
+    std::this_thread::sleep_for(std::chrono::milliseconds(1));
+    g.lock();
+  }
+}
+
+// Takes need bytes from the budget if they fit; else asks the budget thread
+// for a fresh read.
 bool take_budget(collatz_server* s, uint64_t need) {
   std::lock_guard<std::mutex> g(s->mb);
-  const auto age = Clock::now() - s->budget_read;
-  if (age > std::chrono::milliseconds(100) || (s->budget < (int64_t)need && age > std::chrono::milliseconds(1)))
-    refresh_budget(s);
-  if (s->budget < (int64_t)need) return false;
+  if (s->budget < (int64_t)need) {
+    s->want_budget = true;
+    s->cv_budget.notify_one();
+    return false;
+  }
   s->budget -= (int64_t)need;
   s->promised += need;
   return true;
@@ -342,10 +375,6 @@ void admit_ranges(collatz_server* s) {
     Req* r = front(s, s->pend_range, 0);
     if (!r || s->free_slots.empty()) return;
     if (!take_active(s, 0)) return;
-    if (!take_budget(s, 0)) {
-      s->active[0]--;
-      return;
-    }
     pop_admitted(s, s->pend_range, r);
     r->k = r->q.range.k ? r->q.range.k : c->cfg.range_k;
     r->neg = (r->q.range.flags & COLLATZ_RANGE_NEGATIVE) != 0;
@@ -617,6 +646,7 @@ int launch_batch(collatz_server* s, int bi) {
     for (Req* r : B.reqs) promised += r->dev_bytes;
     std::lock_guard<std::mutex> g(s->mb);
     s->promised -= std::min(s->promised, promised);
+    s->launched += promised;
   }
   char* d = static_cast<char*>(block);
   e = cudaMemcpyAsync(d, h, L.in_bytes, cudaMemcpyHostToDevice, st);
@@ -744,7 +774,7 @@ void worker(collatz_server* s, bool range_side, Work work) {
       fail_worker(s, range_side, rc);
       return;
     }
-    if (!rc && busy_device) {  // nothing happened: wait for the device or a new request
+    if (!rc) {  // nothing happened: wait for the device, a new request or a budget read
       const Clock::time_point tw = Clock::now();
       std::unique_lock<std::mutex> g(s->mu);
       cv.wait_for(g, std::chrono::microseconds(50));
@@ -917,12 +947,21 @@ extern "C" int collatz_server_start(const collatz_config* cfg, const collatz_ser
     if ((e = B.h_out.ensure(BatchLayout(nb).out_bytes))) return fail(e, "batch");
     B.cls.reserve(nb);
   }
+  // the query pool grown to two full batches now (growing it under load took milliseconds)
+  {
+    const BatchLayout L(nb);
+    void* blk[BATCH_DEPTH] = {};
+    for (void*& b : blk)
+      if (!e) e = cudaMallocFromPoolAsync(&b, L.o_out + L.out_bytes, s->pool, s->sb);
+    for (void* b : blk)
+      if (b) cudaFreeAsync(b, s->sb);
+    const cudaError_t es = cudaStreamSynchronize(s->sb);
+    if (!e) e = es;
+    if (e) return fail(e, "query pool");
+  }
   size_t fr = 0;
   if ((e = cudaMemGetInfo(&fr, &s->total_mem))) return fail(e, "cudaMemGetInfo");
-  {
-    std::lock_guard<std::mutex> g(s->mb);
-    refresh_budget(s);
-  }
+  refresh_budget(s);
   for (uint32_t i = s->cfg.max_active; i-- > 0;) s->free_slots.push_back(i);
   // helpers for the query path's host copies: up to 7, half the host's threads at most
   s->copy_pool.start((int)std::min(7u, std::max(1u, std::thread::hardware_concurrency() / 2) - 1u));
@@ -933,6 +972,7 @@ extern "C" int collatz_server_start(const collatz_config* cfg, const collatz_ser
   s->thr_query = std::thread([s] { worker(s, false, [s](double* t, Clock::time_point tp, bool& b) {
                                        return query_pass(s, t, tp, b);
                                      }); });
+  s->thr_budget = std::thread([s] { budget_loop(s); });
   *out = s;
   return COLLATZ_OK;
 }
@@ -1024,6 +1064,12 @@ extern "C" int collatz_server_stop(collatz_server* s) {
   s->cv_query.notify_all();
   if (s->thr_range.joinable()) s->thr_range.join();
   if (s->thr_query.joinable()) s->thr_query.join();
+  {
+    std::lock_guard<std::mutex> g(s->mb);
+    s->budget_stop = true;
+  }
+  s->cv_budget.notify_all();
+  if (s->thr_budget.joinable()) s->thr_budget.join();
   destroy(s);
   return COLLATZ_OK;
 }
