@@ -56,10 +56,10 @@ OPS_JUMP, OPS_ODD, OPS_EVEN = 16, 14, 12
 #   frontier: 2^36 launch at 2^60, k = 34 (dram bytes per 2^34 block: each
 #             block streams the 5 mod-9 classes it keeps of the 2.43 GB table).
 NCU_CAPTURES = {
-    "block": {"src": "2d2a66f2a3382cee", "dram_bytes": 5.119744e6 + 0.314880e6, "per": "launch",
-              "issue_slots_busy": 0.8031, "alu_pipe_busy": 0.6965, "kernel": "k_range64 (64-bit values)"},
-    "frontier": {"src": "2d2a66f2a3382cee", "dram_bytes": (5.424407552e9 + 9.482752e6) / 4, "per": "2^34 block",
-                 "issue_slots_busy": 0.7583, "alu_pipe_busy": 0.6764, "kernel": "k_range (four limbs)"},
+    "block": {"src": "4fb5c600c49019d1", "dram_bytes": 5.220864e6 + 0.423936e6, "per": "launch",
+              "issue_slots_busy": 0.7960, "alu_pipe_busy": 0.6853, "kernel": "k_range64 (64-bit values)"},
+    "frontier": {"src": "4fb5c600c49019d1", "dram_bytes": (5.423305e9 + 9.317888e6) / 4, "per": "2^34 block",
+                 "issue_slots_busy": 0.7581, "alu_pipe_busy": 0.6762, "kernel": "k_range (four limbs)"},
 }
 KERNEL_SOURCES = ("range.cu", "range64.cu", "range_shared.cuh", "common.cuh", "kernels.h", "tables.h", "tables.cu")
 # CPU sample of the block workload, the same for the reference arm's steps and

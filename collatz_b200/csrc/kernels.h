@@ -139,6 +139,8 @@ cudaError_t range_occupancy(int variant, int* blocks_per_sm);
 // run pairs per pass, resident blocks per SM and the in-loop table steps J
 // (0: none; 8, 10, 11).
 int range64_variants();
+// Hash of the 64-bit kernel's variant table (part of the autotuner's cache key).
+uint32_t range64_variant_rev();
 uint32_t range64_max_seed_bits();
 cudaError_t range64_init();  // once per device, before the first launch
 cudaError_t launch_range64(const RangeArgs& a, int variant, uint32_t grid, cudaStream_t st);

@@ -13,6 +13,13 @@
 //     (128 bits) until it comes back below -- lane by lane, so the other
 //     lanes keep the 64-bit pair -- and a value that could leave 2^128 sends
 //     the seed to the widen list (re-run from scratch with 6 and 8 limbs);
+//   * at expansion every seed takes up to M run pairs in its lane; the seeds
+//     still running are then packed into lanes and take up to M2 more, so
+//     that the warp does not step every entry's pairs for the few that need
+//     them; the rest go to the queue;
+//   * the run loop takes one warp vote per step for all of its rare events (a
+//     value at or above 2^59, an excursion candidate, a finish that may
+//     offer) when V is set;
 //   * with J > 0, a lane whose value is far from its seed and from the
 //     excursion threshold takes J steps at once from a 2^J-entry table in
 //     shared memory (rs:111-123 and rs:321-341 give the jump-table form,
@@ -140,12 +147,43 @@ __device__ __forceinline__ bool first_pairs(u64& v, u32& st, u64 n, u64 G, u32 t
   return true;
 }
 
+// Second stage of the run pairs taken at expansion: the seeds that the first
+// stage kept sit in W.q[tail, tail + total); each takes up to M2 more pairs
+// (the same rules as first_pairs, so the two stages give exactly what
+// first_pairs<M + M2> gives) and those still running are written back,
+// compacted, from tail.  Packing the survivors into lanes first keeps the
+// warp from stepping every entry's M + M2 pairs for the few that need them.
+// Returns the number kept.  Warp-uniform.
+template <int M2, bool STATS>
+__device__ __forceinline__ u32 second_pairs(Warp64& W, u32 lane, u32 tail, u32 total, u32 slot, u64 G, u32 thr_st,
+                                            const u32* s_pow3, Stats64& X) {
+  u32 kept = 0;
+  for (u32 base = 0; base < total; base += 32) {
+    const bool has = base + lane < total;
+    const uint4 e = has ? W.q[(tail + base + lane) & (Q64 - 1)] : make_uint4(0u, 0u, 0u, 0u);
+    __syncwarp();  // every entry of this round is read before any is overwritten
+    u64 v = ((u64)e.y << 32) | e.x;
+    const u64 n = ((u64)(e.w & 0xFFFFu) << 32) | e.z;
+    u32 st = e.w >> 22;
+    const bool keep = has && first_pairs<M2, STATS>(v, st, n, G, thr_st, s_pow3, X);
+    const u32 bk = __ballot_sync(FULL, keep);
+    if (keep) {  // kept <= base: the slot written was read in this round or an earlier one
+      const u32 cand = v >= G ? 1u : 0u;
+      W.q[(tail + kept + __popc(bk & lanemask_lt())) & (Q64 - 1)] =
+          make_uint4((u32)v, (u32)(v >> 32), (u32)n, (u32)(n >> 32) | (slot << 16) | (cand << 21) | (st << 22));
+    }
+    kept += __popc(bk);
+    __syncwarp();
+  }
+  return kept;
+}
+
 // Expands the staged item into the warp's queue from position tail (see
 // expand_one in range.cu for the rules; this is its 64-bit form).  Seeds are
 // below 2^52, so the block q is below 2^(52-k) and n = q 2^k + r is one
 // 64-bit word; the jump q 3^f + c is taken when it fits 63 bits, else the
 // seed replays its first k steps from v = n + 1.  Warp-uniform.
-template <int JW, int C, int M, bool STATS>
+template <int JW, int C, int M, int M2, bool STATS>
 __device__ __forceinline__ bool expand64(Warp64& W, const RangeArgs& A, const uint4* __restrict__ T, u32 lane, u32 k,
                                          u32 k9, const unsigned long long* s_p3, const u32* s_pow3, const u32* s_win,
                                          u32 head, u32& tail, bool& exhausted, u32& w_thr_st, u32& w_req, u64& w_gate,
@@ -277,6 +315,7 @@ __device__ __forceinline__ bool expand64(Warp64& W, const RangeArgs& A, const ui
     }
   }
   __syncwarp();
+  if (M2 > 0) total = second_pairs<M2, STATS>(W, lane, tail, total, slot, G, w_thr_st, s_pow3, X);
   if (lane == 0) {
     W.ring[slot] = make_uint4(rq, w_thr_st, (u32)G, (u32)(G >> 32));
     W.ring_end[slot] = tail + total;
@@ -290,10 +329,10 @@ __device__ __forceinline__ bool expand64(Warp64& W, const RangeArgs& A, const ui
   return true;
 }
 
-template <int R, int MINB, int J, int JW, int C, int M, bool STATS>
+template <int R, int MINB, int J, int JW, int C, int M, int M2, bool V, bool STATS>
 __global__ void __launch_bounds__(R64_WARPS * 32, MINB) k_range64(const RangeArgs A) {
   // a queued seed's steps: k <= 34, C windows of JW steps, M run pairs of at most 7 + 31 steps
-  static_assert(34 + C * JW + M * 38 <= ST_ENTRY_MAX, "the step count of a queue entry has 10 bits");
+  static_assert(34 + C * JW + (M + M2) * 38 <= ST_ENTRY_MAX, "the step count of a queue entry has 10 bits");
   extern __shared__ __align__(16) unsigned char range64_smem[];
   Warp64* S = reinterpret_cast<Warp64*>(range64_smem);
   __shared__ unsigned long long s_p3[41];
@@ -388,7 +427,7 @@ __global__ void __launch_bounds__(R64_WARPS * 32, MINB) k_range64(const RangeArg
     }
     // ---- refill: keep 32 R seeds queued (each lane takes at most R per pass) ----
     while (tail - head < 32u * R && !exhausted) {
-      if (!expand64<JW, C, M, STATS>(W, A, T, lane, k, k9, s_p3, s_pow3, s_win, head, tail, exhausted, w_thr_st, w_req,
+      if (!expand64<JW, C, M, M2, STATS>(W, A, T, lane, k, k9, s_p3, s_pow3, s_win, head, tail, exhausted, w_thr_st, w_req,
                            w_gate, X))
         break;
     }
@@ -458,134 +497,142 @@ __global__ void __launch_bounds__(R64_WARPS * 32, MINB) k_range64(const RangeArg
       bool fin = false;
       u32 b = 0;
       const bool slow = active & !jstep & ((vh != 0) | (v >= FAST_LIMIT));
-      if (__any_sync(FULL, slow)) {
-        if (slow) {
-          // four-limb run pair for a value at or above 2^59
-          u32 v0 = (u32)v, v1 = (u32)(v >> 32), v2 = (u32)vh, v3 = (u32)(vh >> 32);
-          const u32 a = ctz32(v0 | 0x80u);
-          odd_run4(v0, v1, v2, v3, a, pow3_le7(a));
-          st += a;
-          if (STATS) X.pairs++;
-          bool gone = false;
-          // excursion / overflow gate: a value of 2^64 or more is always a candidate
-          if (((v2 | v3) != 0) | ((((u64)v1 << 32) | v0) >= G)) {
-            if (v3 >= OVF3) {
-              // the next odd run could leave 128 bits: re-run this seed with wider limbs
-              widen_seed(A, req, (u32)n, (u32)(n >> 32), 0u);
-              active = false;
-              gone = true;
-            } else {
-              if (STATS) X.slow_e++;
-              u32 xv[4];
-              value_of<false>(v0, v1, v2, v3, xv);
-              bool tk = !evalid;
-              if (evalid)
-                tk = lt96c(W.e[0][lane], W.e[1][lane], W.e[2][lane], xv[0], xv[1], xv[2]) ? (W.e[3][lane] <= xv[3])
-                                                                                            : (W.e[3][lane] < xv[3]);
-              if (tk) {
-                W.e[0][lane] = xv[0];
-                W.e[1][lane] = xv[1];
-                W.e[2][lane] = xv[2];
-                W.e[3][lane] = xv[3];
-                evalid = true;
-              }
-            }
+      // four-limb run pair for a value at or above 2^59
+      auto slow_pair = [&]() {
+        u32 v0 = (u32)v, v1 = (u32)(v >> 32), v2 = (u32)vh, v3 = (u32)(vh >> 32);
+        const u32 a = ctz32(v0 | 0x80u);
+        odd_run4(v0, v1, v2, v3, a, pow3_le7(a));
+        st += a;
+        if (STATS) X.pairs++;
+        // excursion / overflow gate: a value of 2^64 or more is always a candidate
+        if (((v2 | v3) != 0) | ((((u64)v1 << 32) | v0) >= G)) {
+          if (v3 >= OVF3) {
+            // the next odd run could leave 128 bits: re-run this seed with wider limbs
+            widen_seed(A, req, (u32)n, (u32)(n >> 32), 0u);
+            active = false;
+            return;
           }
-          if (!gone) {
-            v0 -= 1;  // v0 == 0 gives b == 0 below, and the borrow cancels against the +1
-            b = ctz32(v0 | 0x80000000u);
-            const u32 w0 = __funnelshift_r(v0, v1, b), w1 = __funnelshift_r(v1, v2, b);
-            const u32 w2 = __funnelshift_r(v2, v3, b), w3 = v3 >> b;
-            st += b;
-            fin = (((w3 | w2) == 0) & (b != 0) & ((((u64)w1 << 32) | w0) < n)) | (st > ST_CAP);
-            if (fin) {
-              v = ((u64)v1 << 32) | v0;  // the value before the even run
-              vh = ((u64)v3 << 32) | v2;
-            } else {
-              u32 y0 = w0 + 1, y1 = w1, y2 = w2, y3 = w3;
-              add_carry3(y1, y2, y3, (y0 == 0) & (b != 0));
-              v = ((u64)y1 << 32) | y0;
-              vh = ((u64)y3 << 32) | y2;
-            }
+          if (STATS) X.slow_e++;
+          u32 xv[4];
+          value_of<false>(v0, v1, v2, v3, xv);
+          bool tk = !evalid;
+          if (evalid)
+            tk = lt96c(W.e[0][lane], W.e[1][lane], W.e[2][lane], xv[0], xv[1], xv[2]) ? (W.e[3][lane] <= xv[3])
+                                                                                        : (W.e[3][lane] < xv[3]);
+          if (tk) {
+            W.e[0][lane] = xv[0];
+            W.e[1][lane] = xv[1];
+            W.e[2][lane] = xv[2];
+            W.e[3][lane] = xv[3];
+            evalid = true;
           }
         }
+        v0 -= 1;  // v0 == 0 gives b == 0 below, and the borrow cancels against the +1
+        b = ctz32(v0 | 0x80000000u);
+        const u32 w0 = __funnelshift_r(v0, v1, b), w1 = __funnelshift_r(v1, v2, b);
+        const u32 w2 = __funnelshift_r(v2, v3, b), w3 = v3 >> b;
+        st += b;
+        fin = (((w3 | w2) == 0) & (b != 0) & ((((u64)w1 << 32) | w0) < n)) | (st > ST_CAP);
+        if (fin) {
+          v = ((u64)v1 << 32) | v0;  // the value before the even run
+          vh = ((u64)v3 << 32) | v2;
+        } else {
+          u32 y0 = w0 + 1, y1 = w1, y2 = w2, y3 = w3;
+          add_carry3(y1, y2, y3, (y0 == 0) & (b != 0));
+          v = ((u64)y1 << 32) | y0;
+          vh = ((u64)y3 << 32) | y2;
+        }
+      };
+      // an excursion candidate x of a 64-bit pair: keep it when it is the seed's largest value
+      auto take_candidate = [&](u64 x) {
+        if (STATS) X.slow_e++;
+        const u64 ex = ((u64)W.e[1][lane] << 32) | W.e[0][lane];
+        if (!evalid || (W.e[2][lane] == 0 && W.e[3][lane] == 0 && x > ex)) {
+          W.e[0][lane] = (u32)x;
+          W.e[1][lane] = (u32)(x >> 32);
+          W.e[2][lane] = 0;
+          W.e[3][lane] = 0;
+          evalid = true;
+        }
+      };
+      // a finish that may change a maximum or is an error; every other finish only frees the lane
+      auto finish = [&]() {
+        if (st > ST_CAP) {
+          atomicOr(&A.recs[req].errors, ERR_ITER_CAP);
+          atomicAdd(&A.recs[req].failures, 1ull);
+          return;
+        }
+        // the seed fell below its start inside the last even run; st is an upper bound of sigma
+        if (st >= thr_st) {
+          // x = (vh:v), the value before that run.  i* = least i with x >> i < n: with
+          // d = bitlen(x) - bitlen(n), i* is d when x >> d < n, else d + 1 (d <= b <= 31).
+          const int d = (int)(vh ? 128u - __clzll(vh) : bitlen64(v)) - (int)bitlen64(n);
+          u32 istar = 1;
+          if (d >= 1) {
+            const u64 ylo = (v >> d) | (vh << (64 - d)), yhi = vh >> d;
+            istar = ((yhi == 0) & (ylo < n)) ? (u32)d : (u32)d + 1u;
+          }
+          st = st - b + istar;
+          if (st >= thr_st) {
+            W.c[0][lane] = st;
+            pend |= 1u;
+          }
+        }
+        if (evalid) {
+          pend |= 2u;
+          W.pe[0][lane] = W.e[0][lane];
+          W.pe[1][lane] = W.e[1][lane];
+          W.pe[2][lane] = W.e[2][lane];
+          W.pe[3][lane] = W.e[3][lane];
+        }
+        if (pend) {
+          W.c[1][lane] = (u32)n;
+          W.c[2][lane] = (u32)(n >> 32);
+          W.c[3][lane] = 0;
+          W.c[4][lane] = req;
+        }
+      };
+      // V: the 64-bit pair first, then one vote for every rare event of the step (a value at
+      // or above 2^59, an excursion candidate, a finish that may offer); else a vote each,
+      // the four-limb pair before the 64-bit one
+      if (!V && __any_sync(FULL, slow)) {
+        if (slow) slow_pair();
       }
-      {
-        // 64-bit run pair (every lane computes it; active fast lanes keep the result): the
-        // odd run (at most 7 steps) multiplies by less than 2^5, so the value stays below 2^64
-        const bool fast = active & !slow & !jstep;
-        const u32 a = ctz32((u32)v | 0x80u);
-        const u64 x = (v >> a) * s_pow3[a] - 1;  // the value after the odd run
-        const u32 bb = ctz32((u32)x | 0x80000000u);
-        const u64 w = x >> bb;
-        const u32 st2 = st + a + bb;
-        // a run of bb = 0 leaves x, which exceeds the value before the odd run (>= n)
-        const bool ff = fast & ((w < n) | (st2 > ST_CAP));
-        const bool cand = fast & (x + 1 >= G);
-        if (STATS && fast) {
-          X.pairs++;
-          X.fast++;
+      // 64-bit run pair (every lane computes it; active fast lanes keep the result): the
+      // odd run (at most 7 steps) multiplies by less than 2^5, so the value stays below 2^64
+      const bool fast = active & !slow & !jstep;
+      const u32 a = ctz32((u32)v | 0x80u);
+      const u64 x = (v >> a) * s_pow3[a] - 1;  // the value after the odd run
+      const u32 bb = ctz32((u32)x | 0x80000000u);
+      const u64 w = x >> bb;
+      const u32 st2 = st + a + bb;
+      // a run of bb = 0 leaves x, which exceeds the value before the odd run (>= n)
+      const bool ff = fast & ((w < n) | (st2 > ST_CAP));
+      const bool cand = fast & (x + 1 >= G);
+      if (STATS && fast) {
+        X.pairs++;
+        X.fast++;
+      }
+      if (fast) {
+        st = st2;
+        b = bb;
+        fin = ff;
+        v = ff ? x : w + 1;  // the finish reads the value before the even run
+      }
+      if (V) {
+        const bool rare = slow | cand | (fin & ((st > ST_CAP) | (st >= thr_st) | evalid));
+        if (__any_sync(FULL, rare)) {
+          if (slow) slow_pair();
+          if (cand) take_candidate(x);
+          if (fin & ((st > ST_CAP) | (st >= thr_st) | evalid)) finish();
         }
-        if (fast) {
-          st = st2;
-          b = bb;
-          fin = ff;
-          v = ff ? x : w + 1;  // the finish reads the value before the even run
-        }
+      } else {
         if (__any_sync(FULL, cand)) {
-          // an excursion candidate (rare): keep x when it is the seed's largest value
-          if (cand) {
-            if (STATS) X.slow_e++;
-            const u64 ex = ((u64)W.e[1][lane] << 32) | W.e[0][lane];
-            if (!evalid || (W.e[2][lane] == 0 && W.e[3][lane] == 0 && x > ex)) {
-              W.e[0][lane] = (u32)x;
-              W.e[1][lane] = (u32)(x >> 32);
-              W.e[2][lane] = 0;
-              W.e[3][lane] = 0;
-              evalid = true;
-            }
-          }
+          if (cand) take_candidate(x);
         }
-      }
-      // a finish that may change a maximum or is an error (rare); every other finish only
-      // frees the lane
-      const bool need = fin & ((st > ST_CAP) | (st >= thr_st) | evalid);
-      if (__any_sync(FULL, need)) {
-        if (need) {
-          if (st > ST_CAP) {
-            atomicOr(&A.recs[req].errors, ERR_ITER_CAP);
-            atomicAdd(&A.recs[req].failures, 1ull);
-          } else {
-            // the seed fell below its start inside the last even run; st is an upper bound of sigma
-            if (st >= thr_st) {
-              // x = (vh:v), the value before that run.  i* = least i with x >> i < n: with
-              // d = bitlen(x) - bitlen(n), i* is d when x >> d < n, else d + 1 (d <= b <= 31).
-              const int d = (int)(vh ? 128u - __clzll(vh) : bitlen64(v)) - (int)bitlen64(n);
-              u32 istar = 1;
-              if (d >= 1) {
-                const u64 ylo = (v >> d) | (vh << (64 - d)), yhi = vh >> d;
-                istar = ((yhi == 0) & (ylo < n)) ? (u32)d : (u32)d + 1u;
-              }
-              st = st - b + istar;
-              if (st >= thr_st) {
-                W.c[0][lane] = st;
-                pend |= 1u;
-              }
-            }
-            if (evalid) {
-              pend |= 2u;
-              W.pe[0][lane] = W.e[0][lane];
-              W.pe[1][lane] = W.e[1][lane];
-              W.pe[2][lane] = W.e[2][lane];
-              W.pe[3][lane] = W.e[3][lane];
-            }
-            if (pend) {
-              W.c[1][lane] = (u32)n;
-              W.c[2][lane] = (u32)(n >> 32);
-              W.c[3][lane] = 0;
-              W.c[4][lane] = req;
-            }
-          }
+        const bool need = fin & ((st > ST_CAP) | (st >= thr_st) | evalid);
+        if (__any_sync(FULL, need)) {
+          if (need) finish();
         }
       }
       active = active & !fin;
@@ -624,26 +671,42 @@ __global__ void __launch_bounds__(R64_WARPS * 32, MINB) k_range64(const RangeArg
 // ------------------------------------------------------------------
 constexpr size_t RANGE64_SMEM = sizeof(Warp64) * R64_WARPS;
 
-// (run pairs per pass, minimum resident blocks per SM, in-loop table steps J, expansion
-// window length JW, windows per seed C, run pairs per seed at expansion M).  Measured on
-// B200, 2^36 seeds at 2^40 with k = 24: 11.66 ms (variant 0), 11.68 (1), 11.84 (2), 11.78
-// (3), 12.21 (4: three windows), 16.72 (5: one 8-step window, no pairs at expansion),
-// 14.24 (6: in-loop 8-step table), 12.09 (7: one run pair per pass); the four-limb
-// kernel takes 17.62 ms.
-#define CZ_RANGE64_VARIANTS(X)                                                                        \
-  X(0, 2, 4, 0, 11, 1, 5) X(1, 2, 4, 0, 10, 1, 5) X(2, 2, 4, 0, 8, 1, 5) X(3, 2, 4, 0, 10, 1, 4)          \
-  X(4, 2, 4, 0, 10, 3, 4) X(5, 2, 4, 0, 8, 1, 0) X(6, 2, 4, 8, 11, 1, 5) X(7, 1, 4, 0, 11, 1, 5)
+// (run pairs per pass R, minimum resident blocks per SM, in-loop table steps J, expansion
+// window length JW, windows per seed C, run pairs per seed at expansion M, then M2 more for
+// the seeds the first M left running, packed into lanes; V: one vote per run-loop step for
+// every rare event).  Measured on B200, 2^36 seeds at 2^40 with k = 24 (and 2^34 at 2^47):
+// 11.25 ms (3.08) for variant 0, 11.25 (3.05) for 1, 11.32 (3.08) for 2, 11.29 (3.09) for
+// 3, 11.60 (3.18) for 4, 11.77 (3.18) for 5 (the form without the second stage or the
+// single vote), 11.56 (3.13) for 6, 11.97 (3.23) for 7; 3 + 3 + 3 pairs in three stages took
+// 12.06 ms, 2 + 4 took 12.21, and the lanes' two entries stepped in lockstep 12.15.
+#define CZ_RANGE64_VARIANTS(X)                                                                          \
+  X(0, 2, 4, 0, 11, 1, 3, 4, true) X(1, 2, 4, 0, 10, 1, 3, 4, true) X(2, 2, 4, 0, 11, 1, 3, 3, true)      \
+  X(3, 2, 4, 0, 11, 1, 3, 5, true) X(4, 2, 4, 0, 11, 1, 5, 0, true) X(5, 2, 4, 0, 11, 1, 5, 0, false)     \
+  X(6, 2, 4, 0, 11, 1, 4, 3, true) X(7, 2, 3, 0, 11, 1, 3, 4, true)
 
 int range64_variants() { return 8; }
+
+// FNV-1a of the variant table's parameters: part of the autotuner's cache key, so that a
+// choice cached for another table is not applied to this one.
+uint32_t range64_variant_rev() {
+  static const int p[] = {
+#define X(id, rm, mb, j, jw, cw, m, m2, vo) id, rm, mb, j, jw, cw, m, m2, (int)(vo),
+      CZ_RANGE64_VARIANTS(X)
+#undef X
+  };
+  uint32_t h = 2166136261u;
+  for (int x : p) h = (h ^ (uint32_t)x) * 16777619u;
+  return h;
+}
 
 uint32_t range64_max_seed_bits() { return SEED_BITS_64; }
 
 cudaError_t launch_range64(const RangeArgs& a, int variant, u32 grid, cudaStream_t st) {
   if (a.negative || a.seed_bits > SEED_BITS_64) return cudaErrorInvalidValue;
   switch (variant) {
-#define X(id, rm, mb, j, jw, cw, m)                                                         \
+#define X(id, rm, mb, j, jw, cw, m, m2, vo)                                                         \
   case id:                                                                       \
-    k_range64<rm, mb, j, jw, cw, m, false><<<grid, R64_WARPS * 32, RANGE64_SMEM, st>>>(a);  \
+    k_range64<rm, mb, j, jw, cw, m, m2, vo, false><<<grid, R64_WARPS * 32, RANGE64_SMEM, st>>>(a);  \
     break;
     CZ_RANGE64_VARIANTS(X)
 #undef X
@@ -655,9 +718,9 @@ cudaError_t launch_range64(const RangeArgs& a, int variant, u32 grid, cudaStream
 cudaError_t launch_range64_stats(const RangeArgs& a, int variant, u32 grid, cudaStream_t st) {
   if (a.negative || a.seed_bits > SEED_BITS_64) return cudaErrorInvalidValue;
   switch (variant) {
-#define X(id, rm, mb, j, jw, cw, m)                                                        \
+#define X(id, rm, mb, j, jw, cw, m, m2, vo)                                                        \
   case id:                                                                      \
-    k_range64<rm, mb, j, jw, cw, m, true><<<grid, R64_WARPS * 32, RANGE64_SMEM, st>>>(a);  \
+    k_range64<rm, mb, j, jw, cw, m, m2, vo, true><<<grid, R64_WARPS * 32, RANGE64_SMEM, st>>>(a);  \
     break;
     CZ_RANGE64_VARIANTS(X)
 #undef X
@@ -668,9 +731,9 @@ cudaError_t launch_range64_stats(const RangeArgs& a, int variant, u32 grid, cuda
 
 cudaError_t range64_occupancy(int variant, int* bps) {
   switch (variant) {
-#define X(id, rm, mb, j, jw, cw, m) \
+#define X(id, rm, mb, j, jw, cw, m, m2, vo) \
   case id:               \
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_range64<rm, mb, j, jw, cw, m, false>, R64_WARPS * 32, RANGE64_SMEM);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_range64<rm, mb, j, jw, cw, m, m2, vo, false>, R64_WARPS * 32, RANGE64_SMEM);
     CZ_RANGE64_VARIANTS(X)
 #undef X
     default: return cudaErrorInvalidValue;
@@ -680,12 +743,12 @@ cudaError_t range64_occupancy(int variant, int* bps) {
 // Opts every 64-bit range kernel into RANGE64_SMEM of dynamic shared memory.
 cudaError_t range64_init() {
   cudaError_t e = cudaSuccess;
-#define X(id, rm, mb, j, jw, cw, m)                                                                                            \
+#define X(id, rm, mb, j, jw, cw, m, m2, vo)                                                                                            \
   if (e == cudaSuccess)                                                                                             \
-    e = cudaFuncSetAttribute(k_range64<rm, mb, j, jw, cw, m, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,              \
+    e = cudaFuncSetAttribute(k_range64<rm, mb, j, jw, cw, m, m2, vo, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,              \
                              (int)RANGE64_SMEM);                                                                    \
   if (e == cudaSuccess)                                                                                             \
-    e = cudaFuncSetAttribute(k_range64<rm, mb, j, jw, cw, m, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,               \
+    e = cudaFuncSetAttribute(k_range64<rm, mb, j, jw, cw, m, m2, vo, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,               \
                              (int)RANGE64_SMEM);
   CZ_RANGE64_VARIANTS(X)
 #undef X

@@ -39,7 +39,8 @@ std::string device_key(const collatz_ctx* c) {
     if (ch == ' ' || ch == '\t') ch = '_';
   std::ostringstream k;
   k << name << ":sm" << p.multiProcessorCount << ":cc" << p.major << "." << p.minor << ":abi"
-    << COLLATZ_ABI_VERSION << ":v" << range_variants() << "." << cases_variants() << "." << range64_variants();
+    << COLLATZ_ABI_VERSION << ":v" << range_variants() << "." << cases_variants() << "." << range64_variants()
+    << "." << std::hex << range64_variant_rev();
   return k.str();
 }
 
