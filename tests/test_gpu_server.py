@@ -118,3 +118,34 @@ def test_submit_validation():
         assert e.value.status == cb.E_LIMIT
         with pytest.raises(cb.CollatzError):
             srv.wait(12345, timeout=0.1)
+
+
+def test_queries_wait_for_memory_and_complete(verifier):
+    """An hbm_reserve that leaves room for a fraction of the queued queries:
+    admission runs out of budget, waits for the budget thread's next read of
+    free memory (batches that finished have given their memory back), and
+    every query completes with the results of the query run alone."""
+    import numpy as np
+    import collatz_b200 as cb
+    v = verifier(26)
+    with cb.Server(26) as probe:
+        free = probe.info()["hbm_free"]
+    rng = np.random.default_rng(7)
+    qs = []
+    for _ in range(400):  # 2.1 MB of admission budget each, 840 MB in all
+        s = rng.integers(0, 1 << 32, size=(1 << 14, 8), dtype=np.uint64).astype(np.uint32)
+        s[:, 4:] = 0
+        s[:, 3] |= np.uint32(1 << 31)
+        qs.append(s)
+    with cb.Server(26, hbm_reserve=free - (100 << 20)) as srv:
+        tickets = [srv.submit_trajectory_array(s) for s in qs]
+        resps = [srv.wait(t, timeout=120) for t in tickets]
+        info = srv.info()
+    assert info["refused"] == 0
+    for s, r in zip(qs[::20], resps[::20]):
+        assert r.status == 0
+        status, st, exc = v.trajectory_array(s)
+        assert (status == r.traj_status).all()
+        assert (st == r.traj_stopping_time).all()
+        assert (exc == r.traj_excursion).all()
+    assert all(r.status == 0 for r in resps)
