@@ -1,7 +1,8 @@
 // server.cu -- serving mode: continuous batching of range verifications and
 // trajectory queries on one device (collatz_server_* in include/collatz.h).
 //
-// The server owns a context (sieve tables resident in HBM) and two worker
+// The server owns a context (sieve tables resident in HBM), a budget thread
+// (the admission budget's reads of free device memory, below) and two worker
 // threads, each with its own stream:
 //   range thread  -- slices.  A slice is one launch of the persistent range
 //                    kernel over a work list cut from the admitted range
