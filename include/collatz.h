@@ -285,8 +285,9 @@ int collatz_trajectory(collatz_ctx *ctx, const uint32_t *seeds, uint32_t n, uint
 /* Serving (new entry mode): continuous batching of range requests and */
 /* trajectory queries on one device.                                   */
 /* ------------------------------------------------------------------ */
-/* A scheduler thread admits requests in arrival order while request
- * slots and free device memory allow (cudaMemGetInfo minus hbm_reserve),
+/* Worker threads admit requests in arrival order while request slots
+ * and, for trajectory queries, free device memory allow (cudaMemGetInfo
+ * minus hbm_reserve, read every 50 ms by a budget thread),
  * cuts the admitted range requests into slices of work items that share
  * one persistent range launch (small requests take what they need, the
  * rest of the slice goes to the large ones), runs trajectory queries as
@@ -333,7 +334,7 @@ typedef struct {
   uint64_t range_slices, traj_batches;
   uint64_t range_seeds_checked, traj_seeds;
   uint32_t active, pending;
-  uint64_t hbm_free;           /* cudaMemGetInfo free bytes at the last admission pass */
+  uint64_t hbm_free;           /* cudaMemGetInfo free bytes at the last budget read */
   uint64_t hbm_admitted;       /* device bytes held by admitted requests */
   double device_busy_s;        /* summed device time of range slices */
   /* scheduler thread: loop iterations and host seconds spent admitting,
