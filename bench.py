@@ -340,35 +340,45 @@ def run_reference_gpu_program(reps: int = 3) -> dict:
         return {"unavailable": "oracle/_ref/ref_gpu_N45 or the CLI is not built (the reference sources were "
                                "absent at build time)"}
     line1, empty = "27 10 8 183 0 0\n", "0 5 0 1 0 0\n"
+    best = {}
+    info = {}
 
-    def run(cmd, text):
-        best, summ, res = None, None, None
-        for _ in range(reps):
-            t0 = time.perf_counter()
-            p = subprocess.run(cmd, input=text, capture_output=True, text=True, timeout=300)
-            dt = time.perf_counter() - t0
-            if p.returncode:
-                raise RuntimeError(f"{os.path.basename(cmd[0])} rc={p.returncode}: {p.stderr[-200:]}")
-            lines = p.stderr.splitlines()
-            summ = next((ln for ln in lines if ln.startswith("Number of kernel launches")), None)
-            res = next((json.loads(ln[len("# results "):]) for ln in lines if ln.startswith("# results ")), res)
-            best = dt if best is None else min(best, dt)
-        return best, summ, res
+    def run(key, cmd, text):
+        t0 = time.perf_counter()
+        p = subprocess.run(cmd, input=text, capture_output=True, text=True, timeout=300)
+        dt = time.perf_counter() - t0
+        if p.returncode:
+            raise RuntimeError(f"{os.path.basename(cmd[0])} rc={p.returncode}: {p.stderr[-200:]}")
+        lines = p.stderr.splitlines()
+        info[key] = (next((ln for ln in lines if ln.startswith("Number of kernel launches")), None),
+                     next((json.loads(ln[len("# results "):]) for ln in lines if ln.startswith("# results ")),
+                          None))
+        best[key] = min(best.get(key, dt), dt)
 
-    r_line, r_sum, _ = run([ref], line1)
-    c_line, c_sum, c_res = run([cli, "45"], line1)
-    r_empty, _, _ = run([ref], empty)
-    c_empty, _, _ = run([cli, "45"], empty)
+    # interleaved, so that a slow stretch of the host hits every program and input alike
+    for _ in range(reps):
+        run("r_line", [ref], line1)
+        run("r_empty", [ref], empty)
+        run("c_line", [cli, "45"], line1)
+        run("c_empty", [cli, "45"], empty)
+    r_sum, c_sum, c_res = info["r_line"][0], info["c_line"][0], info["c_line"][1]
+
+    def diff(a, b):
+        d = best[a] - best[b]
+        return d if d >= 0 else None
+
     return {"input": "27 10 8 183 0 0 (cases_tiny line 1, N = 45; the reference's own default run)",
             "reference_program": "oracle/_ref/ref_gpu_N45 (collatz_cudav7.cu, nvcc -O3 sm_100a, unchanged)",
             "reference_summary": r_sum, "cli_summary": c_sum, "same_summary_line": r_sum == c_sum,
-            "reference_s": r_line, "cli_s": c_line, "reference_startup_s": r_empty, "cli_startup_s": c_empty,
-            "reference_run_s": r_line - r_empty, "cli_run_s": c_line - c_empty,
+            "reference_s": best["r_line"], "cli_s": best["c_line"], "reference_startup_s": best["r_empty"],
+            "cli_startup_s": best["c_empty"], "reference_run_s": diff("r_line", "r_empty"),
+            "cli_run_s": diff("c_line", "c_empty"),
             "cli_run_ms_inside": (c_res or {}).get("run_ms"), "cli_device_ms": (c_res or {}).get("device_ms"),
-            "note": f"wall time of whole processes, best of {reps}; *_run_s = line 1 minus the start-up-only "
-                    "input (0 5 0 1 0 0, no Step-1 leaves): both are dominated by CUDA context creation, which "
-                    "varies by a second from process to process; the reference's start-up includes its CPU "
-                    "table precompute. cli_run_ms_inside: the CLI's own timer around the run after set-up."}
+            "note": f"wall time of whole processes, best of {reps}, the four runs interleaved; *_run_s = line 1 "
+                    "minus the start-up-only input (0 5 0 1 0 0, no Step-1 leaves), null when the start-up "
+                    "spread (CUDA context creation varies by up to a second from process to process) exceeds "
+                    "the run; the reference's start-up includes its CPU table precompute. cli_run_ms_inside: "
+                    "the CLI's own timer around the run after set-up."}
 
 
 def run_served(v, capacity: float, load: float = 0.7, duration: float = 1.0, seed: int = 5,
