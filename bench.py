@@ -47,31 +47,37 @@ UNIT = "seeds/s"
 # ctz, table, overflow test) and, per even run, 2L + 4 (decrement, ctz, L
 # shifts, increment with carry, descent test).
 OPS_JUMP, OPS_ODD, OPS_EVEN = 16, 14, 12
-# Counters of one k_range launch taken with ncu, valid only for the kernel
-# sources they were captured from: `src` is kernel_source_hash() at capture
-# time, and a line reports them only while the sources still hash to it.
-#   block:    2^33 launch at 2^40, k = 24 (dram bytes per launch do not grow
-#             with the block: the 4.6 MB survivor table is read from DRAM once
-#             and from L2 after that);
-#   frontier: 2^36 launch at 2^60, k = 34 (dram bytes per 2^34 block: each
-#             block streams the 5 mod-9 classes it keeps of the 2.43 GB table).
+# Counters of one range-kernel launch taken with ncu, valid only for the
+# sources of the kernel they were captured from: `src` is
+# kernel_source_hash(workload) at capture time (the kernel's own file and the
+# headers and table code it shares), and a line reports them only while those
+# sources still hash to it.
+#   block:    k_range64, 2^33 launch at 2^40, k = 24 (dram bytes per launch do
+#             not grow with the block: the 4.6 MB survivor table is read from
+#             DRAM once and from L2 after that);
+#   frontier: k_range, 2^36 launch at 2^60, k = 34 (dram bytes per 2^34 block:
+#             each block streams the 5 mod-9 classes it keeps of the 2.43 GB
+#             table).
 NCU_CAPTURES = {
-    "block": {"src": "4fb5c600c49019d1", "dram_bytes": 5.220864e6 + 0.423936e6, "per": "launch",
-              "issue_slots_busy": 0.7960, "alu_pipe_busy": 0.6853, "kernel": "k_range64 (64-bit values)"},
-    "frontier": {"src": "4fb5c600c49019d1", "dram_bytes": (5.423305e9 + 9.317888e6) / 4, "per": "2^34 block",
+    "block": {"src": "212c53bc6b1ae53d", "dram_bytes": 5.210368e6 + 0.406272e6, "per": "launch",
+              "issue_slots_busy": 0.7923, "alu_pipe_busy": 0.6873, "kernel": "k_range64 (64-bit values)"},
+    "frontier": {"src": "756669d9f18f48b4", "dram_bytes": (5.423305e9 + 9.317888e6) / 4, "per": "2^34 block",
                  "issue_slots_busy": 0.7581, "alu_pipe_busy": 0.6762, "kernel": "k_range (four limbs)"},
 }
-KERNEL_SOURCES = ("range.cu", "range64.cu", "range_shared.cuh", "common.cuh", "kernels.h", "tables.h", "tables.cu")
+SHARED_KERNEL_SOURCES = ("range_shared.cuh", "common.cuh", "kernels.h", "tables.h", "tables.cu")
+KERNEL_SOURCES = {"block": ("range64.cu",) + SHARED_KERNEL_SOURCES,
+                  "frontier": ("range.cu",) + SHARED_KERNEL_SOURCES}
 # CPU sample of the block workload, the same for the reference arm's steps and
 # the cpu_baseline leg: 2^32 seeds at 2^40 + i 2^32 with the k = 24 sieve.
 CPU_SAMPLE_LOG2 = 32
 
 
-def kernel_source_hash() -> str:
-    """sha256 (first 16 hex digits) of the range kernel's sources."""
+def kernel_source_hash(workload: str) -> str:
+    """sha256 (first 16 hex digits) of the sources of the range kernel that
+    runs the workload."""
     import hashlib
     h = hashlib.sha256()
-    for name in KERNEL_SOURCES:
+    for name in KERNEL_SOURCES[workload]:
         with open(os.path.join(ROOT, "collatz_b200", "csrc", name), "rb") as f:
             h.update(f.read())
     return h.hexdigest()[:16]
@@ -516,7 +522,7 @@ def roofline(workload: str, base: int, k: int, survivors: int, mean_ms: float, s
     peak = ipk[1]["ops_per_clk_sm"] * sm_count * sm_mhz * 1e6 / 1e12
     issue_peak = sm_count * 128 * sm_mhz * 1e6 / 1e12
     cap = NCU_CAPTURES[workload]
-    src = kernel_source_hash()
+    src = kernel_source_hash(workload)
     valid = cap["src"] == src
     traffic = None
     if valid:

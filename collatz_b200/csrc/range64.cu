@@ -20,6 +20,9 @@
 //   * the run loop takes one warp vote per step for all of its rare events (a
 //     value at or above 2^59, an excursion candidate, a finish that may
 //     offer) when V is set;
+//   * idle lanes take queued seeds at the first step of each pass of R steps,
+//     and at the later steps only when at least PT lanes are idle: a pop costs
+//     the warp the same instructions for one idle lane as for 32;
 //   * with J > 0, a lane whose value is far from its seed and from the
 //     excursion threshold takes J steps at once from a 2^J-entry table in
 //     shared memory (rs:111-123 and rs:321-341 give the jump-table form,
@@ -183,7 +186,7 @@ __device__ __forceinline__ u32 second_pairs(Warp64& W, u32 lane, u32 tail, u32 t
 // below 2^52, so the block q is below 2^(52-k) and n = q 2^k + r is one
 // 64-bit word; the jump q 3^f + c is taken when it fits 63 bits, else the
 // seed replays its first k steps from v = n + 1.  Warp-uniform.
-template <int JW, int C, int M, int M2, bool STATS>
+template <int JW, int C, int M, int M2, bool NQ, bool STATS>
 __device__ __forceinline__ bool expand64(Warp64& W, const RangeArgs& A, const uint4* __restrict__ T, u32 lane, u32 k,
                                          u32 k9, const unsigned long long* s_p3, const u32* s_pow3, const u32* s_win,
                                          u32 head, u32& tail, bool& exhausted, u32& w_thr_st, u32& w_req, u64& w_gate,
@@ -270,7 +273,16 @@ __device__ __forceinline__ bool expand64(Warp64& W, const RangeArgs& A, const ui
       // threshold, else replay the first k steps exactly
       if (((mask >> j) & 1u) && nbl + 1 + emax < w_thr_bl) {
         const u64 p = s_p3[f];
-        const u64 lo = q * p, hi = __umul64hi(q, p);
+        u64 lo, hi;
+        if (NQ && (q >> 32) == 0) {  // warp-uniform: q 2^32-narrow, two wide multiply-adds
+          const u64 t = (u64)(u32)q * (u32)p;
+          const u64 u = (u64)(u32)q * (u32)(p >> 32) + (t >> 32);
+          lo = (u << 32) | (u32)t;
+          hi = u >> 32;
+        } else {
+          lo = q * p;
+          hi = __umul64hi(q, p);
+        }
         const u64 vv = lo + (((u64)e[j].w << 32) | e[j].z);
         if ((hi == 0) & (vv >= lo) & (vv < (1ull << 63))) {
           v = vv;
@@ -329,10 +341,11 @@ __device__ __forceinline__ bool expand64(Warp64& W, const RangeArgs& A, const ui
   return true;
 }
 
-template <int R, int MINB, int J, int JW, int C, int M, int M2, bool V, bool STATS>
+template <int R, int MINB, int J, int JW, int C, int M, int M2, bool V, int PT, bool NQ, bool STATS>
 __global__ void __launch_bounds__(R64_WARPS * 32, MINB) k_range64(const RangeArgs A) {
   // a queued seed's steps: k <= 34, C windows of JW steps, M run pairs of at most 7 + 31 steps
   static_assert(34 + C * JW + (M + M2) * 38 <= ST_ENTRY_MAX, "the step count of a queue entry has 10 bits");
+  static_assert(Q64 >= 32 * R + RANGE_ITEM, "a refill may leave 32 R - 1 seeds queued and add one item");
   extern __shared__ __align__(16) unsigned char range64_smem[];
   Warp64* S = reinterpret_cast<Warp64*>(range64_smem);
   __shared__ unsigned long long s_p3[41];
@@ -427,7 +440,7 @@ __global__ void __launch_bounds__(R64_WARPS * 32, MINB) k_range64(const RangeArg
     }
     // ---- refill: keep 32 R seeds queued (each lane takes at most R per pass) ----
     while (tail - head < 32u * R && !exhausted) {
-      if (!expand64<JW, C, M, M2, STATS>(W, A, T, lane, k, k9, s_p3, s_pow3, s_win, head, tail, exhausted, w_thr_st, w_req,
+      if (!expand64<JW, C, M, M2, NQ, STATS>(W, A, T, lane, k, k9, s_p3, s_pow3, s_win, head, tail, exhausted, w_thr_st, w_req,
                            w_gate, X))
         break;
     }
@@ -448,7 +461,9 @@ __global__ void __launch_bounds__(R64_WARPS * 32, MINB) k_range64(const RangeArg
       {
         const bool idle = !active && !pend;
         const u32 want = __ballot_sync(FULL, idle);
-        if (want) {
+        // the first step of a pass refills every idle lane; the later ones only when at
+        // least PT lanes are idle (PT <= 1: whenever one is)
+        if (want && (r == 0 || PT <= 1 || __popc(want) >= PT)) {
           const u32 avail = tail - head;
           const u32 rank = __popc(want & lanemask_lt());
           const bool take = idle && rank < avail;
@@ -674,15 +689,21 @@ constexpr size_t RANGE64_SMEM = sizeof(Warp64) * R64_WARPS;
 // (run pairs per pass R, minimum resident blocks per SM, in-loop table steps J, expansion
 // window length JW, windows per seed C, run pairs per seed at expansion M, then M2 more for
 // the seeds the first M left running, packed into lanes; V: one vote per run-loop step for
-// every rare event).  Measured on B200, 2^36 seeds at 2^40 with k = 24 (and 2^34 at 2^47):
-// 11.25 ms (3.08) for variant 0, 11.25 (3.05) for 1, 11.32 (3.08) for 2, 11.29 (3.09) for
-// 3, 11.60 (3.18) for 4, 11.77 (3.18) for 5 (the form without the second stage or the
-// single vote), 11.56 (3.13) for 6, 11.97 (3.23) for 7; 3 + 3 + 3 pairs in three stages took
-// 12.06 ms, 2 + 4 took 12.21, and the lanes' two entries stepped in lockstep 12.15.
-#define CZ_RANGE64_VARIANTS(X)                                                                          \
-  X(0, 2, 4, 0, 11, 1, 3, 4, true) X(1, 2, 4, 0, 10, 1, 3, 4, true) X(2, 2, 4, 0, 11, 1, 3, 3, true)      \
-  X(3, 2, 4, 0, 11, 1, 3, 5, true) X(4, 2, 4, 0, 11, 1, 5, 0, true) X(5, 2, 4, 0, 11, 1, 5, 0, false)     \
-  X(6, 2, 4, 0, 11, 1, 4, 3, true) X(7, 2, 3, 0, 11, 1, 3, 4, true)
+// every rare event; PT: after the first step of a pass, idle lanes take queued seeds only
+// when at least PT of them are idle; NQ: the k-step jump multiplies a block number q below
+// 2^32 with two wide multiply-adds).  Measured on B200, 2^36 seeds at 2^40 with k = 24
+// (2^34 at 2^47; the 2^38 block at 2^40), best of three, side by side in one process:
+// 11.11 ms (3.07; 43.54) for variant 0, 11.09 (3.02; 43.60) for 1, 11.25 (3.09; 44.15) for
+// 2 (the previous default: a pop at every step), 11.14 (3.06; 43.72) for 3, 11.18 (3.04;
+// 43.90) for 6; pop thresholds of 8, 16 and 24 gave 43.57, 43.55 and 43.54 ms on the block.
+// Earlier, with PT = 1 and no NQ: 11.60 (3.18) for 4, 11.77 (3.18) for 5 (the form without
+// the second stage or the single vote), 11.97 (3.23) for 7; 3 + 3 + 3 pairs in three stages
+// took 12.06 ms, 2 + 4 took 12.21, and the lanes' two entries stepped in lockstep 12.15.
+#define CZ_RANGE64_VARIANTS(X)                                                                                   \
+  X(0, 2, 4, 0, 11, 1, 3, 4, true, 12, true) X(1, 2, 4, 0, 10, 1, 3, 4, true, 12, true)                          \
+  X(2, 2, 4, 0, 11, 1, 3, 4, true, 1, false) X(3, 2, 4, 0, 11, 1, 3, 5, true, 12, true)                          \
+  X(4, 2, 4, 0, 11, 1, 5, 0, true, 1, false) X(5, 2, 4, 0, 11, 1, 5, 0, false, 1, false)                         \
+  X(6, 2, 4, 0, 11, 1, 3, 4, true, 33, false) X(7, 2, 3, 0, 11, 1, 3, 4, true, 1, false)
 
 int range64_variants() { return 8; }
 
@@ -690,7 +711,7 @@ int range64_variants() { return 8; }
 // choice cached for another table is not applied to this one.
 uint32_t range64_variant_rev() {
   static const int p[] = {
-#define X(id, rm, mb, j, jw, cw, m, m2, vo) id, rm, mb, j, jw, cw, m, m2, (int)(vo),
+#define X(id, rm, mb, j, jw, cw, m, m2, vo, pt, nq) id, rm, mb, j, jw, cw, m, m2, (int)(vo), pt, (int)(nq),
       CZ_RANGE64_VARIANTS(X)
 #undef X
   };
@@ -704,9 +725,9 @@ uint32_t range64_max_seed_bits() { return SEED_BITS_64; }
 cudaError_t launch_range64(const RangeArgs& a, int variant, u32 grid, cudaStream_t st) {
   if (a.negative || a.seed_bits > SEED_BITS_64) return cudaErrorInvalidValue;
   switch (variant) {
-#define X(id, rm, mb, j, jw, cw, m, m2, vo)                                                         \
+#define X(id, rm, mb, j, jw, cw, m, m2, vo, pt, nq)                                                         \
   case id:                                                                       \
-    k_range64<rm, mb, j, jw, cw, m, m2, vo, false><<<grid, R64_WARPS * 32, RANGE64_SMEM, st>>>(a);  \
+    k_range64<rm, mb, j, jw, cw, m, m2, vo, pt, nq, false><<<grid, R64_WARPS * 32, RANGE64_SMEM, st>>>(a);  \
     break;
     CZ_RANGE64_VARIANTS(X)
 #undef X
@@ -718,9 +739,9 @@ cudaError_t launch_range64(const RangeArgs& a, int variant, u32 grid, cudaStream
 cudaError_t launch_range64_stats(const RangeArgs& a, int variant, u32 grid, cudaStream_t st) {
   if (a.negative || a.seed_bits > SEED_BITS_64) return cudaErrorInvalidValue;
   switch (variant) {
-#define X(id, rm, mb, j, jw, cw, m, m2, vo)                                                        \
+#define X(id, rm, mb, j, jw, cw, m, m2, vo, pt, nq)                                                        \
   case id:                                                                      \
-    k_range64<rm, mb, j, jw, cw, m, m2, vo, true><<<grid, R64_WARPS * 32, RANGE64_SMEM, st>>>(a);  \
+    k_range64<rm, mb, j, jw, cw, m, m2, vo, pt, nq, true><<<grid, R64_WARPS * 32, RANGE64_SMEM, st>>>(a);  \
     break;
     CZ_RANGE64_VARIANTS(X)
 #undef X
@@ -731,9 +752,9 @@ cudaError_t launch_range64_stats(const RangeArgs& a, int variant, u32 grid, cuda
 
 cudaError_t range64_occupancy(int variant, int* bps) {
   switch (variant) {
-#define X(id, rm, mb, j, jw, cw, m, m2, vo) \
+#define X(id, rm, mb, j, jw, cw, m, m2, vo, pt, nq) \
   case id:               \
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_range64<rm, mb, j, jw, cw, m, m2, vo, false>, R64_WARPS * 32, RANGE64_SMEM);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_range64<rm, mb, j, jw, cw, m, m2, vo, pt, nq, false>, R64_WARPS * 32, RANGE64_SMEM);
     CZ_RANGE64_VARIANTS(X)
 #undef X
     default: return cudaErrorInvalidValue;
@@ -743,12 +764,12 @@ cudaError_t range64_occupancy(int variant, int* bps) {
 // Opts every 64-bit range kernel into RANGE64_SMEM of dynamic shared memory.
 cudaError_t range64_init() {
   cudaError_t e = cudaSuccess;
-#define X(id, rm, mb, j, jw, cw, m, m2, vo)                                                                                            \
+#define X(id, rm, mb, j, jw, cw, m, m2, vo, pt, nq)                                                                                            \
   if (e == cudaSuccess)                                                                                             \
-    e = cudaFuncSetAttribute(k_range64<rm, mb, j, jw, cw, m, m2, vo, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,              \
+    e = cudaFuncSetAttribute(k_range64<rm, mb, j, jw, cw, m, m2, vo, pt, nq, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,              \
                              (int)RANGE64_SMEM);                                                                    \
   if (e == cudaSuccess)                                                                                             \
-    e = cudaFuncSetAttribute(k_range64<rm, mb, j, jw, cw, m, m2, vo, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,               \
+    e = cudaFuncSetAttribute(k_range64<rm, mb, j, jw, cw, m, m2, vo, pt, nq, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,               \
                              (int)RANGE64_SMEM);
   CZ_RANGE64_VARIANTS(X)
 #undef X

@@ -88,7 +88,10 @@ VARIANT64_CASES = [CASES[i] for i in (0, 1, 3, 4, 5, 6)] + [
 ]
 
 
-@pytest.mark.parametrize("variant", range(8))
+RANGE64_VARIANTS = 8
+
+
+@pytest.mark.parametrize("variant", range(RANGE64_VARIANTS))
 def test_range64_variants_match_oracle(verifier, variant):
     """Every variant of the 64-bit range kernel (run pairs per pass, blocks per
     SM, in-loop table steps J, expansion windows of 8, 10 or 11 steps and run
@@ -96,7 +99,7 @@ def test_range64_variants_match_oracle(verifier, variant):
     batch, with the limb width at its maximum (48 bits)."""
     import collatz_b200 as cb
     from oracle import oracle as O
-    assert cb.lib().collatz_variant_count(cb.MODE_RANGE64) == 8
+    assert cb.lib().collatz_variant_count(cb.MODE_RANGE64) == RANGE64_VARIANTS
     v = verifier(26)
     v.set_variant(cb.MODE_RANGE64, variant)
     v.set_variant(cb.MODE_RANGE64_BITS, 48)
