@@ -362,8 +362,9 @@ int collatz_server_stop(collatz_server *s);
 /* Kernel choices for the autotuner (no counterpart in the reference).
  *   COLLATZ_MODE_CASES, COLLATZ_MODE_RANGE: variant (block shape, body) of
  *     the cases kernel and of the four-limb range kernel;
- *   COLLATZ_MODE_RANGE64: variant of the 64-bit range kernel (run pairs per
- *     pass, blocks per SM, in-loop table steps J of 0, 8, 10 or 11);
+ *   COLLATZ_MODE_RANGE64: variant of the 64-bit range kernel (jump-table
+ *     window of 10 or 11 steps, run pairs at expansion, warp votes per step,
+ *     queue-pop threshold, blocks per SM);
  *   COLLATZ_MODE_RANGE64_BITS: the limb width -- launches whose seeds all have
  *     at most this many bits (0..52) run the 64-bit kernel, the others the
  *     four-limb kernel (0: always four limbs).
